@@ -1,0 +1,430 @@
+"""Python binding of libcfdfs (the B200 fractional-step solver's C ABI).
+
+The solver itself is C++ host code plus sm_100a CUDA kernels inside
+``lib/libcfdfs.so``; this module only declares the C prototypes (ctypes) and
+offers a ``Solver`` class whose methods carry the names of the reference's
+device seam (fractionalStep/Cpp/blascoCodinaHuerta.cpp:365-377):
+``selectCUDAdevice``, ``initializeAndAllocateGPU``, ``calculateZ_CUSP``,
+``calculateMatrixAGPU``, ``step1GPUpart``, ``step2GPU``, ``step3GPU``,
+``calculate_KtimesAcc_prevGPU``, ``checkConvergenceGPU``,
+``checkConvergenceInTimeGPU`` and ``printMonitorDataGPU``.  Where the
+reference prints "ErrorNN" and waits on std::cin, these raise ``CfdError``.
+
+There is no CPU fallback: if the library cannot be loaded, or no GPU is
+present, construction fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+_PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(_PKG_DIR)
+LIB_PATH = os.path.join(ROOT, "lib", "libcfdfs.so")
+HEADER = os.path.join(os.path.dirname(ROOT), "include", "cfdfs.h")
+
+CFD_OK, CFD_E_CUDA, CFD_E_NOCONV, CFD_E_NONFINITE, CFD_E_TIMEOUT, CFD_E_BADARG, CFD_E_BADINPUT, CFD_E_IO, \
+    CFD_E_NOMEM = 0, -1, -2, -3, -4, -5, -6, -7, -8
+FP64, MIXED = 0, 1
+PC_JACOBI, PC_LEARNED = 0, 1
+
+VEC = dict(Un=0, Unp1=1, Unp1_prev=2, UnpHalf=3, UnpHalf_prev=4, Acc=5, Acc_prev=6, Pn=7, Pnp1=8,
+           Pnp1_prev=9, Pdot=10, MdInv=11, MdOrigInv=12, KtimesAcc_prev=13, R1=14, R2=15, R3=16, DIV=17)
+PRESSURE_SIZED = {"Pn", "Pnp1", "Pnp1_prev", "Pdot", "R2", "DIV"}
+MAT = dict(K=0, G=1, GT=2, Z=3)
+
+
+class CfdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"cfdfs error {code}: {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [("precision", C.c_int), ("precond", C.c_int), ("cg_rtol", C.c_double), ("cg_maxit", C.c_int),
+                ("cg_warm", C.c_int), ("ngp_override", C.c_int), ("inner_rtol", C.c_double),
+                ("max_outer", C.c_int)]
+
+
+class ProblemInfo(C.Structure):
+    _fields_ = [("NE", C.c_int), ("NCN", C.c_int), ("NN", C.c_int), ("NNp", C.c_int), ("NGP", C.c_int),
+                ("maxIter", C.c_int), ("nnzK", C.c_longlong), ("nnzG", C.c_longlong), ("nnzZ", C.c_longlong),
+                ("nBCnodes", C.c_int), ("monPoint", C.c_int), ("zeroPressureNode", C.c_int),
+                ("dt", C.c_double), ("t_ini", C.c_double), ("t_final", C.c_double), ("tolerance", C.c_double),
+                ("convergence", C.c_double), ("density", C.c_double), ("viscosity", C.c_double),
+                ("timeN", C.c_int), ("timeT", C.c_double)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("outer", C.c_int), ("relres", C.c_double), ("status", C.c_int),
+                ("fallback", C.c_int)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("steps", C.c_int), ("subiters", C.c_longlong), ("cg_iters", C.c_longlong), ("steady", C.c_int),
+                ("maxAcc", C.c_double), ("last_iter", C.c_int)]
+
+
+_lib = None
+_vp, _ip, _dp, _cp, _llp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_char_p, C.POINTER(C.c_longlong)
+
+_PROTOS = {
+    "cfd_abi_version": (C.c_int, []),
+    "cfd_default_options": (None, [C.POINTER(Options)]),
+    "cfd_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int]),
+    "cfd_destroy": (None, [_vp]),
+    "cfd_last_error": (C.c_char_p, [_vp]),
+    "cfd_set_options": (C.c_int, [_vp, C.POINTER(Options)]),
+    "cfd_load_inp": (C.c_int, [_vp, _cp]),
+    "cfd_load_mesh": (C.c_int, [_vp, C.POINTER(ProblemInfo), _dp, _ip, C.c_int, _dp, C.c_int, _ip, _dp]),
+    "cfd_info": (C.c_int, [_vp, C.POINTER(ProblemInfo)]),
+    "cfd_step0": (C.c_int, [_vp]),
+    "cfd_begin_step": (C.c_int, [_vp]),
+    "cfd_convect": (C.c_int, [_vp]),
+    "cfd_step1": (C.c_int, [_vp, C.c_int]),
+    "cfd_step2": (C.c_int, [_vp, C.c_int, C.POINTER(SolveStats)]),
+    "cfd_step3": (C.c_int, [_vp, C.c_int]),
+    "cfd_check_iter": (C.c_int, [_vp, C.c_double, _ip, _dp]),
+    "cfd_rotate": (C.c_int, [_vp]),
+    "cfd_k_times_acc": (C.c_int, [_vp]),
+    "cfd_check_steady": (C.c_int, [_vp, C.c_double, _dp, _ip]),
+    "cfd_end_step": (C.c_int, [_vp]),
+    "cfd_run": (C.c_int, [_vp, C.c_int, C.POINTER(RunStats)]),
+    "cfd_get_monitor": (C.c_int, [_vp, C.c_int, _dp]),
+    "cfd_download_state": (C.c_int, [_vp, _dp, _dp]),
+    "cfd_upload_state": (C.c_int, [_vp, _dp, _dp]),
+    "cfd_download_vector": (C.c_int, [_vp, C.c_int, _dp]),
+    "cfd_download_matrix": (C.c_int, [_vp, C.c_int, _llp, _ip, _ip, _dp]),
+    "cfd_pressure_solve": (C.c_int, [_vp, _dp, _dp, C.POINTER(SolveStats)]),
+    "cfd_write_tecplot": (C.c_int, [_vp, _cp, _cp]),
+    "cfd_read_restart": (C.c_int, [_vp, _cp]),
+    "cfd_set_bc_values": (C.c_int, [_vp, C.c_int, _ip, _dp]),
+    "cfd_unet_load": (C.c_int, [_vp, _cp]),
+    "cfd_stream": (C.c_void_p, [_vp]),
+    "cfd_launch_count": (C.c_longlong, [_vp]),
+    "cfd_profile": (C.c_int, [_vp, C.c_int]),
+    "cfd_profile_read": (C.c_int, [_vp, _dp]),
+    "cfd_selftest_wait_timeout": (C.c_int, [_vp, C.c_int]),
+    "cfdh_load": (C.c_int, [C.POINTER(C.c_void_p), _cp, C.c_char_p, C.c_int]),
+    "cfdh_free": (None, [_vp]),
+    "cfdh_sizes": (C.c_int, [_vp, _llp]),
+    "cfdh_get_ltog": (C.c_int, [_vp, _ip]),
+    "cfdh_get_coord": (C.c_int, [_vp, _dp]),
+    "cfdh_get_bcnodes": (C.c_int, [_vp, _ip]),
+    "cfdh_get_pattern": (C.c_int, [_vp, C.c_int, _ip, _ip]),
+    "cfdh_write_tecplot": (C.c_int, [_vp, _dp, _dp, _cp, _cp]),
+}
+
+
+def header_functions(path: str = HEADER) -> list[str]:
+    """Names of every function the public header declares."""
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(cfdh?_[a-z0-9_]+)\s*\(", txt)))
+
+
+def lib():
+    """Loads libcfdfs.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise CfdError(CFD_E_CUDA, f"{LIB_PATH} is missing; build it with __graft_entry__.build()")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def default_options() -> Options:
+    o = Options()
+    lib().cfd_default_options(C.byref(o))
+    return o
+
+
+class HostMesh:
+    """Deck + preprocessing on the host only (no GPU): cfdh_* entry points."""
+
+    def __init__(self, path: str):
+        L = lib()
+        h = C.c_void_p()
+        err = C.create_string_buffer(512)
+        rc = L.cfdh_load(C.byref(h), path.encode(), err, 512)
+        if rc != CFD_OK:
+            raise CfdError(rc, err.value.decode())
+        self.h, self.L = h, L
+        s = np.zeros(12, dtype=np.int64)
+        L.cfdh_sizes(h, _p(s, C.c_longlong))
+        (self.NE, self.NCN, self.NN, self.NNp, self.nnzK, self.nnzG, self.nnzZ, self.nbc, self.mon, self.zero_p,
+         self.NGP, self.max_iter) = [int(x) for x in s]
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cfdh_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def ltog(self):
+        a = np.zeros(self.NE * 27, dtype=np.int32)
+        self.L.cfdh_get_ltog(self.h, _p(a, C.c_int))
+        return a.reshape(self.NE, 27)
+
+    def coord(self):
+        a = np.zeros(self.NN * 3)
+        self.L.cfdh_get_coord(self.h, _p(a, C.c_double))
+        return a.reshape(self.NN, 3)
+
+    def bcnodes(self):
+        a = np.zeros(self.nbc * 2, dtype=np.int32)
+        self.L.cfdh_get_bcnodes(self.h, _p(a, C.c_int))
+        return a.reshape(self.nbc, 2)
+
+    def pattern(self, which: str):
+        w = {"K": 0, "G": 1, "GT": 2, "Z": 3}[which]
+        nrows = self.NNp if which in ("GT", "Z") else self.NN
+        nnz = {"K": self.nnzK, "G": self.nnzG, "GT": self.nnzG, "Z": self.nnzZ}[which]
+        rp = np.zeros(nrows + 1, dtype=np.int32)
+        col = np.zeros(nnz, dtype=np.int32)
+        self.L.cfdh_get_pattern(self.h, w, _p(rp, C.c_int), _p(col, C.c_int))
+        return rp, col
+
+    def write_tecplot(self, U, P, path: str, title: str):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        rc = self.L.cfdh_write_tecplot(self.h, _p(U, C.c_double), _p(P, C.c_double), path.encode(), title.encode())
+        if rc != CFD_OK:
+            raise CfdError(rc, "tecplot write failed")
+
+
+class Solver:
+    """One GPU solver context (cfd_ctx)."""
+
+    def __init__(self, device: int = 0, precision: int = FP64, cg_rtol: float = 1e-8, cg_maxit: int = 1000,
+                 cg_warm: int = 0, ngp: int = 0, inner_rtol: float = 1e-4, max_outer: int = 12,
+                 precond: int = PC_JACOBI):
+        L = lib()
+        h = C.c_void_p()
+        rc = L.cfd_create(C.byref(h), device)
+        if rc != CFD_OK:
+            raise CfdError(rc, "cfd_create failed (no usable CUDA device?)")
+        self.h, self.L = h, L
+        o = default_options()
+        o.precision, o.precond, o.cg_rtol, o.cg_maxit, o.cg_warm = precision, precond, cg_rtol, cg_maxit, cg_warm
+        o.ngp_override, o.inner_rtol, o.max_outer = ngp, inner_rtol, max_outer
+        self._check(L.cfd_set_options(h, C.byref(o)))
+        self.info = None
+
+    # ---- plumbing ----
+    def _check(self, rc: int):
+        if rc != CFD_OK:
+            raise CfdError(rc, self.L.cfd_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def refresh(self) -> ProblemInfo:
+        i = ProblemInfo()
+        self._check(self.L.cfd_info(self.h, C.byref(i)))
+        self.info = i
+        return i
+
+    # ---- set-up ----
+    def load(self, path: str):
+        """readInputFile + preprocessing + initializeAndAllocateGPU."""
+        self._check(self.L.cfd_load_inp(self.h, path.encode()))
+        return self.refresh()
+
+    def step0(self):
+        """step0 + calculateZ_CUSP on the device."""
+        self._check(self.L.cfd_step0(self.h))
+
+    # ---- reference-named stage calls ----
+    def begin_step(self):
+        self._check(self.L.cfd_begin_step(self.h))
+
+    def calculateMatrixAGPU(self):
+        self._check(self.L.cfd_convect(self.h))
+
+    def step1GPUpart(self, it: int):
+        self._check(self.L.cfd_step1(self.h, it))
+
+    def step2GPU(self, it: int) -> SolveStats:
+        st = SolveStats()
+        self._check(self.L.cfd_step2(self.h, it, C.byref(st)))
+        return st
+
+    def step3GPU(self, it: int):
+        self._check(self.L.cfd_step3(self.h, it))
+
+    def checkConvergenceGPU(self, tol: float | None = None):
+        tol = self.refresh().tolerance if tol is None else tol
+        conv = C.c_int(0)
+        norms = np.zeros(2)
+        self._check(self.L.cfd_check_iter(self.h, tol, C.byref(conv), _p(norms, C.c_double)))
+        return bool(conv.value), norms
+
+    def rotate(self):
+        self._check(self.L.cfd_rotate(self.h))
+
+    def calculate_KtimesAcc_prevGPU(self):
+        self._check(self.L.cfd_k_times_acc(self.h))
+
+    def checkConvergenceInTimeGPU(self, crit: float | None = None):
+        crit = self.refresh().convergence if crit is None else crit
+        m, s = C.c_double(0), C.c_int(0)
+        self._check(self.L.cfd_check_steady(self.h, crit, C.byref(m), C.byref(s)))
+        return bool(s.value), m.value
+
+    def end_step(self):
+        self._check(self.L.cfd_end_step(self.h))
+
+    def printMonitorDataGPU(self, it: int) -> str:
+        i = self.refresh()
+        m = self.monitor()
+        return "%6d  %6d  %10.5f  %12.5f  %12.5f  %12.5f  %12.5f" % (i.timeN, it, i.timeT, m[0], m[1], m[2], m[3])
+
+    # aliases with the reference's set-up names
+    def initializeAndAllocateGPU(self, path: str):
+        return self.load(path)
+
+    def calculateZ_CUSP(self):
+        return self.step0()
+
+    def run(self, nsteps: int = -1) -> RunStats:
+        st = RunStats()
+        self._check(self.L.cfd_run(self.h, nsteps, C.byref(st)))
+        return st
+
+    def time_step(self):
+        """One time step through the stage calls (timeLoop body)."""
+        i = self.refresh()
+        self.begin_step()
+        cg = []
+        it = 1
+        while it <= i.maxIter:
+            self.calculateMatrixAGPU()
+            self.step1GPUpart(it)
+            cg.append(self.step2GPU(it).iterations)
+            self.step3GPU(it)
+            conv, _ = self.checkConvergenceGPU(i.tolerance)
+            if conv:
+                break
+            self.rotate()
+            self.calculate_KtimesAcc_prevGPU()
+            it += 1
+        steady, max_acc = self.checkConvergenceInTimeGPU(i.convergence)
+        self.end_step()
+        return dict(iter=it, cg=cg, steady=steady, max_acc=max_acc)
+
+    # ---- state ----
+    def monitor(self, node: int = -1):
+        out = np.zeros(4)
+        self._check(self.L.cfd_get_monitor(self.h, node, _p(out, C.c_double)))
+        return out
+
+    def state(self):
+        i = self.info or self.refresh()
+        U, P = np.zeros(3 * i.NN), np.zeros(i.NNp)
+        self._check(self.L.cfd_download_state(self.h, _p(U, C.c_double), _p(P, C.c_double)))
+        return U, P
+
+    def set_state(self, U, P):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        self._check(self.L.cfd_upload_state(self.h, _p(U, C.c_double), _p(P, C.c_double)))
+
+    def vector(self, name: str):
+        i = self.info or self.refresh()
+        n = i.NNp if name in PRESSURE_SIZED else 3 * i.NN
+        out = np.zeros(n)
+        self._check(self.L.cfd_download_vector(self.h, VEC[name], _p(out, C.c_double)))
+        return out
+
+    def matrix(self, which: str):
+        """(rowptr, col, val); val is (nnz, 3) for G and GT."""
+        w = MAT[which]
+        i = self.info or self.refresh()
+        nnz = C.c_longlong(0)
+        self._check(self.L.cfd_download_matrix(self.h, w, C.byref(nnz), None, None, None))
+        nrows = i.NNp if which in ("GT", "Z") else i.NN
+        rp = np.zeros(nrows + 1, dtype=np.int32)
+        col = np.zeros(nnz.value, dtype=np.int32)
+        nv = 3 if which in ("G", "GT") else 1
+        val = np.zeros(nnz.value * nv)
+        self._check(self.L.cfd_download_matrix(self.h, w, C.byref(nnz), _p(rp, C.c_int), _p(col, C.c_int),
+                                               _p(val, C.c_double)))
+        return rp, col, (val.reshape(-1, 3) if nv == 3 else val)
+
+    def pressure_solve(self, rhs, x0=None):
+        i = self.info or self.refresh()
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.zeros(i.NNp) if x0 is None else np.array(x0, dtype=np.float64)
+        st = SolveStats()
+        rc = self.L.cfd_pressure_solve(self.h, _p(rhs, C.c_double), _p(x, C.c_double), C.byref(st))
+        if rc not in (CFD_OK, CFD_E_NOCONV):
+            self._check(rc)
+        return x, st
+
+    # ---- timing / counters ----
+    KCLASS = ["convect", "step1", "gt", "pcg64", "pcg32", "resid64", "step3", "spmv_k3", "pupdate", "other"]
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.L.cfd_stream(self.h) or 0)
+
+    def launch_count(self) -> int:
+        return int(self.L.cfd_launch_count(self.h))
+
+    def profile(self, on: bool):
+        self._check(self.L.cfd_profile(self.h, 1 if on else 0))
+
+    def profile_read(self) -> dict:
+        out = np.zeros(3 * len(self.KCLASS))
+        self._check(self.L.cfd_profile_read(self.h, _p(out, C.c_double)))
+        return {k: dict(launches=int(out[3 * i]), ms=float(out[3 * i + 1]), iters=int(out[3 * i + 2]))
+                for i, k in enumerate(self.KCLASS)}
+
+    def selftest_wait_timeout(self, ms: int) -> int:
+        return int(self.L.cfd_selftest_wait_timeout(self.h, ms))
+
+    def write_tecplot(self, path: str, title: str):
+        self._check(self.L.cfd_write_tecplot(self.h, path.encode(), title.encode()))
+
+    def read_restart(self, path: str):
+        self._check(self.L.cfd_read_restart(self.h, path.encode()))
+
+    def set_bc_values(self, nodes, uvw):
+        nodes = np.ascontiguousarray(nodes, dtype=np.int32)
+        uvw = np.ascontiguousarray(uvw, dtype=np.float64)
+        self._check(self.L.cfd_set_bc_values(self.h, len(nodes), _p(nodes, C.c_int), _p(uvw, C.c_double)))
+
+
+def selectCUDAdevice(device: int = -1) -> Solver:
+    """selectCUDAdevice (CUDAcodes.cu:126-154): a solver on the given device
+    (-1 = the last one, as the reference)."""
+    return Solver(device=device)

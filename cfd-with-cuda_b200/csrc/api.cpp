@@ -1,0 +1,1006 @@
+// libcfdfs C ABI: context, device buffers and the fractional-step driver.
+//
+// Replaces the device seam of the reference (blascoCodinaHuerta.cpp:365-377,
+// CUDAcodes.cu:126-1178).  One context owns one GPU stream and every device
+// buffer; nothing is allocated or freed inside the time loop (the reference
+// mallocs temporaries in step2GPU and checkConvergenceGPU on every call).
+// State rotation between sub-iterations and time steps swaps buffer
+// pointers instead of copying (blascoCodinaHuerta.cpp:2929-2932, 3070-3071).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/cfdfs.h"
+#include "cuda/kernels.h"
+#include "host/problem.h"
+
+namespace cfd {
+int make_basis(int ngp, Basis& B);
+int write_tecplot(const HostProblem& P, const double* U, const double* Pn, const std::string& path,
+                  const std::string& title);
+int read_restart(const HostProblem& P, const std::string& path, double* U, double* Pn);
+}  // namespace cfd
+
+using namespace cfd;
+
+namespace {
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    reset();
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    n = count;
+    return cudaSuccess;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+}  // namespace
+
+struct cfd_ctx {
+  int device = 0, num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cfd_options opt{};
+  std::string err;
+  HostProblem P;
+  bool loaded = false, assembled = false;
+
+  // mesh
+  DevBuf<int> ltog, bcnodes;
+  DevBuf<double> coord, bcvals;
+  DevBuf<Basis> basis;
+  DevBuf<unsigned char> bcmask;
+  // patterns
+  DevBuf<int> k_rp, k_col, g_rp, g_col, gt_rp, gt_col, gt_pos, z_rp, z_col;
+  // FP64 operators
+  DevBuf<double> kval, g1, g2, g3, gt1, gt2, gt3, zval, zdiag, zdinv, msum, minv_orig, minv_free;
+  // FP32 operators (CFD_MIXED)
+  DevBuf<float> kval32, g1_32, g2_32, g3_32, gt1_32, gt2_32, gt3_32, zval32, zdinv32;
+  // velocity-sized state, double4 per node
+  DevBuf<double4> vbuf[12];
+  double4 *un = nullptr, *unp1 = nullptr, *unp1_prev = nullptr, *unphalf = nullptr, *unphalf_prev = nullptr,
+          *acc = nullptr, *acc_prev = nullptr, *kacc = nullptr, *r1conv = nullptr, *dvec = nullptr, *r1dbg = nullptr,
+          *r3dbg = nullptr;
+  // pressure-sized state
+  DevBuf<double> pbuf[6];
+  double *pn = nullptr, *pnp1 = nullptr, *pnp1_prev = nullptr, *pdot = nullptr, *r2 = nullptr, *pzero = nullptr;
+  // Krylov work
+  DevBuf<double> cg_r, cg_z, cg_p, cg_q, cg_part, cg_res, ir_r, ir_part, ir_sum;
+  DevBuf<float> f_b, f_x, f_r, f_z, f_p, f_q;
+  DevBuf<unsigned> cg_bar;
+  DevBuf<int> cg_err;
+  int pcg_grid64 = 1, pcg_grid32 = 1, res_blocks = 1;
+  // reductions
+  DevBuf<double> upart, ppart, norms, blk;
+  int nub = 1, npb = 1;
+  double* h_small = nullptr;  // pinned scratch for small readbacks (64 doubles)
+
+  int timeN = 0;
+  double timeT = 0, maxAcc = 0;
+  double last_norms[5] = {0, 0, 0, 0, 0};
+  bool r_debug = true;
+
+  // launch counting and per-kernel-class event timing
+  long long launches = 0;
+  bool prof_on = false;
+  struct Pair {
+    int cls;
+    cudaEvent_t a, b;
+  };
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<Pair> pending;
+  double prof[CFD_K_COUNT][3] = {};
+  ~cfd_ctx() {
+    for (auto& p : pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    for (auto e : ev_pool) cudaEventDestroy(e);
+  }
+};
+
+namespace {
+
+int fail(cfd_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CU(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess)                                                                       \
+      return fail(c, e_ == cudaErrorMemoryAllocation ? CFD_E_NOMEM : CFD_E_CUDA, "%s: %s (%s:%d)", \
+                  #call, cudaGetErrorString(e_), __FILE__, __LINE__);                            \
+  } while (0)
+
+#define NEED(cond, msg)                                                        \
+  do {                                                                         \
+    if (!(cond)) return fail(c, CFD_E_BADARG, "%s", msg);                      \
+  } while (0)
+
+template <class T>
+cudaError_t upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
+  cudaError_t e = d.alloc(h.size());
+  if (e != cudaSuccess) return e;
+  if (h.empty()) return cudaSuccess;
+  return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+int set_device(cfd_ctx* c) {
+  CU(cudaSetDevice(c->device));
+  return CFD_OK;
+}
+
+cudaEvent_t take_event(cfd_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Converts finished event pairs into per-class totals (call after a sync).
+void harvest(cfd_ctx* c) {
+  for (auto& p : c->pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      c->prof[p.cls][0] += 1;
+      c->prof[p.cls][1] += ms;
+    }
+    c->ev_pool.push_back(p.a);
+    c->ev_pool.push_back(p.b);
+  }
+  c->pending.clear();
+}
+
+// Issues one kernel launch on the context stream, counting it and, when
+// profiling is on, bracketing it with CUDA events.
+template <class F>
+int klaunch(cfd_ctx* c, int cls, F&& f) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (c->prof_on) {
+    a = take_event(c);
+    b = take_event(c);
+    cudaEventRecord(a, c->stream);
+  }
+  cudaError_t e = f();
+  c->launches++;
+  if (c->prof_on) {
+    cudaEventRecord(b, c->stream);
+    c->pending.push_back({cls, a, b});
+  }
+  if (e != cudaSuccess)
+    return fail(c, e == cudaErrorMemoryAllocation ? CFD_E_NOMEM : CFD_E_CUDA, "kernel launch (class %d): %s", cls,
+                cudaGetErrorString(e));
+  return CFD_OK;
+}
+
+#define KL(cls, expr)                                           \
+  do {                                                          \
+    int rc_ = klaunch(c, cls, [&]() { return (expr); });        \
+    if (rc_) return rc_;                                        \
+  } while (0)
+
+// Allocates every device buffer and uploads mesh, patterns, BC data and the
+// initial condition (initializeAndAllocateGPU, CUDAcodes.cu:161-274, and
+// applyBC_initial, blascoCodinaHuerta.cpp:4062-4110).
+int upload_problem(cfd_ctx* c) {
+  HostProblem& P = c->P;
+  cudaStream_t s = c->stream;
+  if (c->opt.ngp_override) P.NGP = c->opt.ngp_override;
+  Basis hb;
+  if (make_basis(P.NGP, hb)) return fail(c, CFD_E_BADINPUT, "unsupported NGP %d", P.NGP);
+  CU(c->basis.alloc(1));
+  CU(cudaMemcpyAsync(c->basis.p, &hb, sizeof(Basis), cudaMemcpyHostToDevice, s));
+  CU(upload(c->ltog, P.ltog, s));
+  CU(upload(c->coord, P.coord, s));
+  CU(upload(c->k_rp, P.k_rp, s));
+  CU(upload(c->k_col, P.k_col, s));
+  CU(upload(c->g_rp, P.g_rp, s));
+  CU(upload(c->g_col, P.g_col, s));
+  CU(upload(c->gt_rp, P.gt_rp, s));
+  CU(upload(c->gt_col, P.gt_col, s));
+  CU(upload(c->gt_pos, P.gt_pos, s));
+  CU(upload(c->z_rp, P.z_rp, s));
+  CU(upload(c->z_col, P.z_col, s));
+  std::vector<unsigned char> mask(P.NN, 0);
+  std::vector<double> bcv(3 * P.bcnode.size());
+  for (size_t i = 0; i < P.bcnode.size(); i++) {
+    mask[P.bcnode[i]] = 1;
+    for (int d = 0; d < 3; d++) bcv[3 * i + d] = P.bcstr[3 * (size_t)P.bcid[i] + d];
+  }
+  CU(upload(c->bcmask, mask, s));
+  CU(upload(c->bcnodes, P.bcnode, s));
+  CU(upload(c->bcvals, bcv, s));
+  const size_t NN = P.NN, NNp = P.NNp;
+  const size_t nnzK = P.k_col.size(), nnzG = P.g_col.size(), nnzZ = P.z_col.size();
+  for (auto* b : {&c->kval}) CU(b->alloc(nnzK));
+  for (auto* b : {&c->g1, &c->g2, &c->g3, &c->gt1, &c->gt2, &c->gt3}) CU(b->alloc(nnzG));
+  CU(c->zval.alloc(nnzZ));
+  for (auto* b : {&c->zdiag, &c->zdinv}) CU(b->alloc(NNp));
+  for (auto* b : {&c->msum, &c->minv_orig, &c->minv_free}) CU(b->alloc(NN));
+  if (c->opt.precision == CFD_MIXED) {
+    CU(c->kval32.alloc(nnzK));
+    for (auto* b : {&c->g1_32, &c->g2_32, &c->g3_32, &c->gt1_32, &c->gt2_32, &c->gt3_32}) CU(b->alloc(nnzG));
+    CU(c->zval32.alloc(nnzZ));
+    CU(c->zdinv32.alloc(NNp));
+    for (auto* b : {&c->f_b, &c->f_x, &c->f_r, &c->f_z, &c->f_p, &c->f_q}) CU(b->alloc(NNp));
+  }
+  for (auto& b : c->vbuf) {
+    CU(b.alloc(NN));
+    CU(cudaMemsetAsync(b.p, 0, b.bytes(), s));
+  }
+  c->un = c->vbuf[0].p; c->unp1 = c->vbuf[1].p; c->unp1_prev = c->vbuf[2].p; c->unphalf = c->vbuf[3].p;
+  c->unphalf_prev = c->vbuf[4].p; c->acc = c->vbuf[5].p; c->acc_prev = c->vbuf[6].p; c->kacc = c->vbuf[7].p;
+  c->r1conv = c->vbuf[8].p; c->dvec = c->vbuf[9].p; c->r1dbg = c->vbuf[10].p; c->r3dbg = c->vbuf[11].p;
+  for (auto& b : c->pbuf) {
+    CU(b.alloc(NNp));
+    CU(cudaMemsetAsync(b.p, 0, b.bytes(), s));
+  }
+  c->pn = c->pbuf[0].p; c->pnp1 = c->pbuf[1].p; c->pnp1_prev = c->pbuf[2].p; c->pdot = c->pbuf[3].p;
+  c->r2 = c->pbuf[4].p; c->pzero = c->pbuf[5].p;
+  for (auto* b : {&c->cg_r, &c->cg_z, &c->cg_p, &c->cg_q, &c->ir_r}) CU(b->alloc(NNp));
+  c->pcg_grid64 = pcg_max_grid<double>((int)NNp, c->device);
+  c->pcg_grid32 = pcg_max_grid<float>((int)NNp, c->device);
+  CU(c->cg_part.alloc(6 * (size_t)std::max(c->pcg_grid64, c->pcg_grid32)));
+  CU(c->cg_res.alloc(8));
+  CU(c->cg_bar.alloc(2));
+  CU(c->cg_err.alloc(1));
+  c->res_blocks = residual_blocks((int)NNp, c->num_sms);
+  CU(c->ir_part.alloc(c->res_blocks));
+  CU(c->ir_sum.alloc(2));
+  c->nub = step3_blocks((int)NN, c->num_sms);
+  c->npb = pupdate_blocks((int)NNp, c->num_sms);
+  CU(c->upart.alloc(3 * (size_t)c->nub));
+  CU(c->ppart.alloc(2 * (size_t)c->npb));
+  CU(cudaMemsetAsync(c->upart.p, 0, c->upart.bytes(), s));
+  CU(cudaMemsetAsync(c->ppart.p, 0, c->ppart.bytes(), s));
+  CU(c->norms.alloc(8));
+  CU(c->blk.alloc(3 * NN));
+  // initial condition: Un = BC values at Dirichlet nodes, zero elsewhere
+  CU(launch_apply_bc((int)P.bcnode.size(), c->bcnodes.p, c->bcvals.p, c->un, s));
+  CU(cudaStreamSynchronize(s));
+  c->timeN = 0;
+  c->timeT = P.t_ini;
+  c->loaded = true;
+  c->assembled = false;
+  return CFD_OK;
+}
+
+// ---- pressure solves ----------------------------------------------------
+
+int run_pcg64(cfd_ctx* c, const double* b, double* x, int warm, double rtol, int maxit, double* res) {
+  cudaStream_t s = c->stream;
+  CU(cudaMemsetAsync(c->cg_bar.p, 0, 2 * sizeof(unsigned), s));
+  CU(cudaMemsetAsync(c->cg_err.p, 0, sizeof(int), s));
+  PcgArgs<double> a{};
+  a.n = c->P.NNp;
+  a.rp = c->z_rp.p; a.col = c->z_col.p; a.val = c->zval.p; a.dinv = c->zdinv.p;
+  a.b = b; a.x = x; a.r = c->cg_r.p; a.z = c->cg_z.p; a.p = c->cg_p.p; a.q = c->cg_q.p;
+  a.part = c->cg_part.p; a.bar = c->cg_bar.p; a.err = c->cg_err.p;
+  a.rtol = rtol; a.maxit = maxit; a.warm = warm; a.result = c->cg_res.p;
+  a.timeout_ns = 2000000000ULL;
+  KL(CFD_K_PCG64, launch_pcg<double>(a, c->pcg_grid64, s));
+  CU(cudaMemcpyAsync(c->h_small, c->cg_res.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  for (int i = 0; i < 4; i++) res[i] = c->h_small[i];
+  if (c->prof_on) c->prof[CFD_K_PCG64][2] += res[0];
+  return CFD_OK;
+}
+
+int run_pcg32(cfd_ctx* c, double rtol, int maxit, double* res) {
+  cudaStream_t s = c->stream;
+  CU(cudaMemsetAsync(c->cg_bar.p, 0, 2 * sizeof(unsigned), s));
+  CU(cudaMemsetAsync(c->cg_err.p, 0, sizeof(int), s));
+  PcgArgs<float> a{};
+  a.n = c->P.NNp;
+  a.rp = c->z_rp.p; a.col = c->z_col.p; a.val = c->zval32.p; a.dinv = c->zdinv32.p;
+  a.b = c->f_b.p; a.x = c->f_x.p; a.r = c->f_r.p; a.z = c->f_z.p; a.p = c->f_p.p; a.q = c->f_q.p;
+  a.part = c->cg_part.p; a.bar = c->cg_bar.p; a.err = c->cg_err.p;
+  a.rtol = rtol; a.maxit = maxit; a.warm = 0; a.result = c->cg_res.p;
+  a.timeout_ns = 2000000000ULL;
+  KL(CFD_K_PCG32, launch_pcg<float>(a, c->pcg_grid32, s));
+  CU(cudaMemcpyAsync(c->h_small, c->cg_res.p, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  for (int i = 0; i < 4; i++) res[i] = c->h_small[i];
+  if (c->prof_on) c->prof[CFD_K_PCG32][2] += res[0];
+  return CFD_OK;
+}
+
+// ||b - Z x||_2 in FP64 (also leaves r in ir_r and (float) r in f_b).
+int residual_norm(cfd_ctx* c, const double* b, const double* x, double* out) {
+  cudaStream_t s = c->stream;
+  KL(CFD_K_RESID64, launch_residual64(c->P.NNp, c->z_rp.p, c->z_col.p, c->zval.p, b, x, c->ir_r.p, c->f_b.p,
+                                      c->ir_part.p, c->res_blocks, s));
+  KL(CFD_K_OTHER, launch_sum_partials(c->ir_part.p, c->res_blocks, c->ir_sum.p, s));
+  CU(cudaMemcpyAsync(c->h_small, c->ir_sum.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  *out = std::sqrt(c->h_small[0]);
+  return CFD_OK;
+}
+
+// Solve Z x = b on the device.  FP64: one persistent Jacobi-PCG.  MIXED:
+// FP64 iterative refinement around FP32 Jacobi-PCG solves (residual and
+// update in FP64, inner tolerance opt.inner_rtol).
+int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_stats* st) {
+  cfd_solve_stats z{};
+  const double rtol = c->opt.cg_rtol;
+  if (c->opt.precision == CFD_FP64 || c->opt.precision != CFD_MIXED) {
+    double res[4] = {0, 0, 0, 0};
+    int rc = run_pcg64(c, b, x, warm, rtol, c->opt.cg_maxit, res);
+    if (rc) return rc;
+    z.iterations = (int)res[0];
+    z.relres = res[1];
+    z.status = (int)res[2];
+  } else {
+    cudaStream_t s = c->stream;
+    if (!warm) CU(cudaMemsetAsync(x, 0, c->P.NNp * sizeof(double), s));
+    double bnorm = 0, rnorm = 0;
+    int rc = residual_norm(c, b, c->pzero, &bnorm);
+    if (rc) return rc;
+    if (!std::isfinite(bnorm)) {
+      z.status = 2;
+    } else if (bnorm == 0.0) {
+      CU(cudaMemsetAsync(x, 0, c->P.NNp * sizeof(double), s));
+      z.status = 0;
+    } else {
+      rc = residual_norm(c, b, x, &rnorm);
+      if (rc) return rc;
+      z.status = 1;
+      int total = 0;
+      for (int outer = 0; outer <= c->opt.max_outer; outer++) {
+        if (!std::isfinite(rnorm)) { z.status = 2; break; }
+        if (rnorm <= rtol * bnorm) { z.status = 0; break; }
+        if (outer == c->opt.max_outer || total >= c->opt.cg_maxit) break;
+        double res[4] = {0, 0, 0, 0};
+        // inner target: inner_rtol relative, but no tighter than needed
+        double inner = std::max(c->opt.inner_rtol, 0.5 * rtol * bnorm / rnorm);
+        rc = run_pcg32(c, inner, c->opt.cg_maxit - total, res);
+        if (rc) return rc;
+        total += (int)res[0];
+        if ((int)res[2] == 3) { z.status = 3; break; }
+        KL(CFD_K_OTHER, launch_axpy_f2d(c->P.NNp, c->f_x.p, x, s));
+        z.outer = outer + 1;
+        rc = residual_norm(c, b, x, &rnorm);
+        if (rc) return rc;
+      }
+      z.iterations = total;
+      z.relres = rnorm / bnorm;
+    }
+  }
+  if (st) *st = z;
+  if (z.status == 3) return fail(c, CFD_E_TIMEOUT, "device-side barrier wait timed out in the pressure solve");
+  if (z.status == 2) return fail(c, CFD_E_NONFINITE, "non-finite residual in the pressure solve");
+  return CFD_OK;
+}
+
+int reduce_norms(cfd_ctx* c) {
+  cudaStream_t s = c->stream;
+  KL(CFD_K_OTHER, launch_reduce_norms(c->upart.p, c->nub, c->ppart.p, c->npb, c->norms.p, s));
+  CU(cudaMemcpyAsync(c->h_small, c->norms.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  for (int i = 0; i < 5; i++) c->last_norms[i] = c->h_small[i];
+  return CFD_OK;
+}
+
+bool mixed(const cfd_ctx* c) { return c->opt.precision == CFD_MIXED; }
+
+
+
+}  // namespace
+
+// =========================================================================
+extern "C" {
+
+int cfd_abi_version(void) { return CFDFS_ABI_VERSION; }
+
+void cfd_default_options(cfd_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->precision = CFD_FP64;
+  o->precond = CFD_PC_JACOBI;
+  o->cg_rtol = 1e-8;
+  o->cg_maxit = 1000;
+  o->cg_warm = 0;
+  o->ngp_override = 0;
+  o->inner_rtol = 1e-4;
+  o->max_outer = 12;
+}
+
+int cfd_create(cfd_ctx** out, int device) {
+  if (!out) return CFD_E_BADARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) return CFD_E_CUDA;
+  if (device < 0) device = n - 1;  // CUDAcodes.cu:141-148 picks the last device
+  if (device >= n) return CFD_E_BADARG;
+  std::unique_ptr<cfd_ctx> c(new cfd_ctx());
+  c->device = device;
+  cfd_default_options(&c->opt);
+  if (cudaSetDevice(device) != cudaSuccess) return CFD_E_CUDA;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return CFD_E_CUDA;
+  if (cudaMallocHost((void**)&c->h_small, 64 * sizeof(double)) != cudaSuccess) return CFD_E_CUDA;
+  *out = c.release();
+  return CFD_OK;
+}
+
+void cfd_destroy(cfd_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->h_small) cudaFreeHost(c->h_small);
+  cudaStream_t s = c->stream;
+  delete c;
+  if (s) cudaStreamDestroy(s);
+}
+
+const char* cfd_last_error(const cfd_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int cfd_set_options(cfd_ctx* c, const cfd_options* o) {
+  if (!c || !o) return CFD_E_BADARG;
+  NEED(o->precision == CFD_FP64 || o->precision == CFD_MIXED, "precision must be CFD_FP64 or CFD_MIXED");
+  NEED(o->precond == CFD_PC_JACOBI || o->precond == CFD_PC_LEARNED, "unknown preconditioner");
+  NEED(o->cg_rtol > 0 && o->cg_rtol < 1, "cg_rtol must be in (0, 1)");
+  NEED(o->cg_maxit > 0, "cg_maxit must be > 0");
+  NEED(o->ngp_override == 0 || o->ngp_override == 1 || o->ngp_override == 8 || o->ngp_override == 27,
+       "ngp_override must be 0, 1, 8 or 27");
+  NEED(!c->loaded || o->precision == c->opt.precision, "precision must be set before cfd_load_inp");
+  NEED(!c->loaded || o->ngp_override == c->opt.ngp_override, "ngp_override must be set before cfd_load_inp");
+  c->opt = *o;
+  if (c->opt.inner_rtol <= 0 || c->opt.inner_rtol >= 1) c->opt.inner_rtol = 1e-4;
+  if (c->opt.max_outer <= 0) c->opt.max_outer = 12;
+  return CFD_OK;
+}
+
+int cfd_load_inp(cfd_ctx* c, const char* path) {
+  if (!c || !path) return CFD_E_BADARG;
+  int rc = set_device(c);
+  if (rc) return rc;
+  c->P = HostProblem();
+  rc = read_inp(path, c->P, c->err);
+  if (rc) return rc;
+  rc = preprocess(c->P, c->err);
+  if (rc) return rc;
+  return upload_problem(c);
+}
+
+int cfd_load_mesh(cfd_ctx* c, const cfd_problem_info* info, const double* coords, const int* conn, int nBC,
+                  const double* bcvals, int nVelFaces, const int* velfaces, const double* monitor) {
+  if (!c || !info || !coords || !conn || (nBC > 0 && !bcvals) || (nVelFaces > 0 && !velfaces) || !monitor)
+    return CFD_E_BADARG;
+  int rc = set_device(c);
+  if (rc) return rc;
+  HostProblem& P = c->P;
+  P = HostProblem();
+  P.NE = info->NE; P.NCN = info->NCN; P.NGP = info->NGP; P.maxIter = info->maxIter;
+  P.dt = info->dt; P.t_ini = info->t_ini; P.t_final = info->t_final; P.tolerance = info->tolerance;
+  P.convergence = info->convergence; P.density = info->density; P.viscosity = info->viscosity;
+  P.zeroP = info->zeroPressureNode;
+  NEED(P.NE > 0 && P.NCN > 0 && P.dt > 0 && P.maxIter > 0, "bad problem sizes");
+  NEED(P.NGP == 1 || P.NGP == 8 || P.NGP == 27, "NGP must be 1, 8 or 27");
+  P.NNp = P.NCN;
+  P.coord.assign(coords, coords + 3 * (size_t)P.NCN);
+  P.ltog.assign((size_t)P.NE * 27, -1);
+  for (int e = 0; e < P.NE; e++)
+    for (int i = 0; i < 8; i++) {
+      int v = conn[(size_t)e * 8 + i];
+      NEED(v >= 0 && v < P.NCN, "connectivity out of range");
+      P.ltog[(size_t)e * 27 + i] = v;
+    }
+  P.nBC = nBC;
+  P.bcstr.assign(bcvals, bcvals + 3 * (size_t)nBC);
+  P.velfaces.assign(velfaces, velfaces + 3 * (size_t)nVelFaces);
+  for (int i = 0; i < nVelFaces; i++) {
+    NEED(velfaces[3 * i] >= 0 && velfaces[3 * i] < P.NE && velfaces[3 * i + 1] >= 0 && velfaces[3 * i + 1] < 6 &&
+             velfaces[3 * i + 2] >= 0 && velfaces[3 * i + 2] < nBC,
+         "velocity face out of range");
+  }
+  for (int d = 0; d < 3; d++) P.mon[d] = monitor[d];
+  rc = preprocess(P, c->err);
+  if (rc) return rc;
+  return upload_problem(c);
+}
+
+int cfd_info(const cfd_ctx* c, cfd_problem_info* i) {
+  if (!c || !i || !c->loaded) return CFD_E_BADARG;
+  const HostProblem& P = c->P;
+  std::memset(i, 0, sizeof(*i));
+  i->NE = P.NE; i->NCN = P.NCN; i->NN = P.NN; i->NNp = P.NNp; i->NGP = P.NGP; i->maxIter = P.maxIter;
+  i->nnzK = (long long)P.k_col.size(); i->nnzG = (long long)P.g_col.size(); i->nnzZ = (long long)P.z_col.size();
+  i->nBCnodes = (int)P.bcnode.size(); i->monPoint = P.monPoint; i->zeroPressureNode = P.zeroP;
+  i->dt = P.dt; i->t_ini = P.t_ini; i->t_final = P.t_final; i->tolerance = P.tolerance;
+  i->convergence = P.convergence; i->density = P.density; i->viscosity = P.viscosity;
+  i->timeN = c->timeN; i->timeT = c->timeT;
+  return CFD_OK;
+}
+
+int cfd_step0(cfd_ctx* c) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->loaded, "cfd_step0 before cfd_load_inp");
+  int rc = set_device(c);
+  if (rc) return rc;
+  HostProblem& P = c->P;
+  cudaStream_t s = c->stream;
+  for (auto* b : {&c->kval, &c->g1, &c->g2, &c->g3, &c->msum}) CU(cudaMemsetAsync(b->p, 0, b->bytes(), s));
+  AsmArgs a{};
+  a.NE = P.NE; a.ngp = P.NGP; a.ltog = c->ltog.p; a.coord = c->coord.p; a.basis = c->basis.p;
+  a.viscosity = P.viscosity; a.inv_density = 1.0 / P.density;
+  a.k_rp = c->k_rp.p; a.k_col = c->k_col.p; a.kval = c->kval.p;
+  a.g_rp = c->g_rp.p; a.g_col = c->g_col.p; a.g1 = c->g1.p; a.g2 = c->g2.p; a.g3 = c->g3.p;
+  a.msum = c->msum.p;
+  CU(launch_assemble(a, c->num_sms, s));
+  CU(launch_fill_gt((long long)P.gt_col.size(), c->gt_pos.p, c->g1.p, c->g2.p, c->g3.p, c->gt1.p, c->gt2.p,
+                    c->gt3.p, s));
+  CU(launch_md_finalize(P.NN, c->msum.p, c->bcmask.p, c->minv_orig.p, c->minv_free.p, s));
+  ZArgs z{};
+  z.NNp = P.NNp; z.maxrow = std::max(1, P.maxZrow); z.zeroP = P.zeroP;
+  z.z_rp = c->z_rp.p; z.z_col = c->z_col.p; z.zval = c->zval.p; z.zdiag = c->zdiag.p;
+  z.gt_rp = c->gt_rp.p; z.gt_col = c->gt_col.p; z.gt1 = c->gt1.p; z.gt2 = c->gt2.p; z.gt3 = c->gt3.p;
+  z.g_rp = c->g_rp.p; z.g_col = c->g_col.p; z.g1 = c->g1.p; z.g2 = c->g2.p; z.g3 = c->g3.p;
+  z.minv_orig = c->minv_orig.p;
+  CU(launch_build_z(z, s));
+  CU(launch_recip(P.NNp, c->zdiag.p, c->zdinv.p, mixed(c) ? c->zdinv32.p : nullptr, s));
+  if (mixed(c)) {
+    CU(launch_to_float((long long)P.k_col.size(), c->kval.p, c->kval32.p, s));
+    const size_t ng = P.g_col.size();
+    CU(launch_to_float(ng, c->g1.p, c->g1_32.p, s));
+    CU(launch_to_float(ng, c->g2.p, c->g2_32.p, s));
+    CU(launch_to_float(ng, c->g3.p, c->g3_32.p, s));
+    CU(launch_to_float(ng, c->gt1.p, c->gt1_32.p, s));
+    CU(launch_to_float(ng, c->gt2.p, c->gt2_32.p, s));
+    CU(launch_to_float(ng, c->gt3.p, c->gt3_32.p, s));
+    CU(launch_to_float((long long)P.z_col.size(), c->zval.p, c->zval32.p, s));
+  }
+  CU(cudaStreamSynchronize(s));
+  c->assembled = true;
+  return CFD_OK;
+}
+
+int cfd_begin_step(cfd_ctx* c) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->assembled, "cfd_begin_step before cfd_step0");
+  cudaStream_t s = c->stream;
+  const size_t NN = c->P.NN, NNp = c->P.NNp;
+  c->timeN = c->timeN + 1;
+  c->timeT = c->timeT + c->P.dt;
+  CU(cudaMemcpyAsync(c->unphalf_prev, c->un, NN * sizeof(double4), cudaMemcpyDeviceToDevice, s));
+  CU(cudaMemcpyAsync(c->pnp1_prev, c->pn, NNp * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  CU(cudaMemsetAsync(c->acc_prev, 0, NN * sizeof(double4), s));
+  return CFD_OK;
+}
+
+int cfd_convect(cfd_ctx* c) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->assembled, "cfd_convect before cfd_step0");
+  cudaStream_t s = c->stream;
+  CU(cudaMemsetAsync(c->r1conv, 0, c->P.NN * sizeof(double4), s));
+  if (mixed(c)) {
+    ConvArgs<float> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
+    KL(CFD_K_CONVECT, launch_convect<float>(a, c->num_sms, s));
+  } else {
+    ConvArgs<double> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
+    KL(CFD_K_CONVECT, launch_convect<double>(a, c->num_sms, s));
+  }
+  return CFD_OK;
+}
+
+int cfd_step1(cfd_ctx* c, int iter) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->assembled && iter >= 1, "cfd_step1: bad state or iter");
+  cudaStream_t s = c->stream;
+  auto fill = [&](auto& a) {
+    a.NN = c->P.NN; a.iter = iter; a.dt = c->P.dt;
+    a.k_rp = c->k_rp.p; a.k_col = c->k_col.p; a.g_rp = c->g_rp.p; a.g_col = c->g_col.p;
+    a.uprev = c->unphalf_prev; a.un = c->un; a.r1conv = c->r1conv; a.kacc = c->kacc;
+    a.pn = c->pn; a.minv_free = c->minv_free.p; a.minv_orig = c->minv_orig.p;
+    a.unphalf = c->unphalf; a.d = c->dvec; a.r1out = c->r_debug ? c->r1dbg : nullptr;
+  };
+  if (mixed(c)) {
+    Step1Args<float> a{};
+    fill(a);
+    a.kval = c->kval32.p; a.g1 = c->g1_32.p; a.g2 = c->g2_32.p; a.g3 = c->g3_32.p;
+    KL(CFD_K_STEP1, launch_step1<float>(a, c->num_sms, s));
+  } else {
+    Step1Args<double> a{};
+    fill(a);
+    a.kval = c->kval.p; a.g1 = c->g1.p; a.g2 = c->g2.p; a.g3 = c->g3.p;
+    KL(CFD_K_STEP1, launch_step1<double>(a, c->num_sms, s));
+  }
+  return CFD_OK;
+}
+
+int cfd_step2(cfd_ctx* c, int iter, cfd_solve_stats* st) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->assembled && iter >= 1, "cfd_step2: bad state or iter");
+  cudaStream_t s = c->stream;
+  const int pin = c->P.zeroP;
+  if (mixed(c)) {
+    GtArgs<float> a{c->P.NNp, pin, c->gt_rp.p, c->gt_col.p, c->gt1_32.p, c->gt2_32.p, c->gt3_32.p, c->dvec, c->r2};
+    KL(CFD_K_GT, launch_gt<float>(a, c->num_sms, s));
+  } else {
+    GtArgs<double> a{c->P.NNp, pin, c->gt_rp.p, c->gt_col.p, c->gt1.p, c->gt2.p, c->gt3.p, c->dvec, c->r2};
+    KL(CFD_K_GT, launch_gt<double>(a, c->num_sms, s));
+  }
+  int rc = pressure_solve(c, c->r2, c->pdot, c->opt.cg_warm, st);
+  if (rc) return rc;
+  KL(CFD_K_PUPDATE, launch_pressure_update(c->P.NNp, c->P.dt, c->pn, c->pdot, c->pnp1_prev, c->pnp1, c->ppart.p, c->npb, s));
+  return CFD_OK;
+}
+
+int cfd_step3(cfd_ctx* c, int iter) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->assembled && iter >= 1, "cfd_step3: bad state or iter");
+  cudaStream_t s = c->stream;
+  auto fill = [&](auto& a) {
+    a.NN = c->P.NN; a.iter = iter; a.dt = c->P.dt;
+    a.g_rp = c->g_rp.p; a.g_col = c->g_col.p; a.pdot = c->pdot; a.kacc = c->kacc; a.unphalf = c->unphalf;
+    a.un = c->un; a.unp1_prev = c->unp1_prev; a.minv_free = c->minv_free.p; a.acc = c->acc; a.unp1 = c->unp1;
+    a.r3out = c->r_debug ? c->r3dbg : nullptr; a.part = c->upart.p; a.nblocks = c->nub;
+  };
+  if (mixed(c)) {
+    Step3Args<float> a{};
+    fill(a);
+    a.g1 = c->g1_32.p; a.g2 = c->g2_32.p; a.g3 = c->g3_32.p;
+    KL(CFD_K_STEP3, launch_step3<float>(a, s));
+  } else {
+    Step3Args<double> a{};
+    fill(a);
+    a.g1 = c->g1.p; a.g2 = c->g2.p; a.g3 = c->g3.p;
+    KL(CFD_K_STEP3, launch_step3<double>(a, s));
+  }
+  return CFD_OK;
+}
+
+int cfd_check_iter(cfd_ctx* c, double tol, int* converged, double* norms) {
+  if (!c || !converged) return CFD_E_BADARG;
+  int rc = reduce_norms(c);
+  if (rc) return rc;
+  const double* v = c->last_norms;
+  double n1 = std::sqrt(v[1]) / std::sqrt(v[0]);
+  double n2 = std::sqrt(v[3]) / std::sqrt(v[2]);
+  *converged = (n1 < tol && n2 < tol) ? 1 : 0;
+  if (norms) {
+    norms[0] = n1;
+    norms[1] = n2;
+  }
+  return CFD_OK;
+}
+
+int cfd_rotate(cfd_ctx* c) {
+  if (!c) return CFD_E_BADARG;
+  std::swap(c->unphalf_prev, c->unphalf);
+  std::swap(c->unp1_prev, c->unp1);
+  std::swap(c->acc_prev, c->acc);
+  std::swap(c->pnp1_prev, c->pnp1);
+  return CFD_OK;
+}
+
+int cfd_k_times_acc(cfd_ctx* c) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->assembled, "cfd_k_times_acc before cfd_step0");
+  cudaStream_t s = c->stream;
+  if (mixed(c)) {
+    SpmvK3Args<float> a{c->P.NN, c->k_rp.p, c->k_col.p, c->kval32.p, c->acc_prev, c->kacc};
+    KL(CFD_K_SPMV_K3, launch_spmv_k3<float>(a, c->num_sms, s));
+  } else {
+    SpmvK3Args<double> a{c->P.NN, c->k_rp.p, c->k_col.p, c->kval.p, c->acc_prev, c->kacc};
+    KL(CFD_K_SPMV_K3, launch_spmv_k3<double>(a, c->num_sms, s));
+  }
+  return CFD_OK;
+}
+
+int cfd_check_steady(cfd_ctx* c, double crit, double* maxAcc, int* steady) {
+  if (!c) return CFD_E_BADARG;
+  int rc = reduce_norms(c);
+  if (rc) return rc;
+  c->maxAcc = c->last_norms[4];
+  if (maxAcc) *maxAcc = c->maxAcc;
+  if (steady) *steady = (c->maxAcc > crit) ? 0 : 1;
+  return CFD_OK;
+}
+
+int cfd_end_step(cfd_ctx* c) {
+  if (!c) return CFD_E_BADARG;
+  std::swap(c->un, c->unp1);
+  std::swap(c->pn, c->pnp1);
+  return CFD_OK;
+}
+
+int cfd_run(cfd_ctx* c, int nsteps, cfd_run_stats* st) {
+  if (!c) return CFD_E_BADARG;
+  NEED(c->assembled, "cfd_run before cfd_step0");
+  cfd_run_stats r{};
+  int rc = set_device(c);
+  if (rc) return rc;
+  const HostProblem& P = c->P;
+  while (nsteps < 0 ? (c->timeT < P.t_final) : (r.steps < nsteps)) {
+    if ((rc = cfd_begin_step(c))) return rc;
+    int iter;
+    for (iter = 1; iter <= P.maxIter; iter++) {
+      cfd_solve_stats ss{};
+      if ((rc = cfd_convect(c))) return rc;
+      if ((rc = cfd_step1(c, iter))) return rc;
+      if ((rc = cfd_step2(c, iter, &ss))) return rc;
+      if ((rc = cfd_step3(c, iter))) return rc;
+      r.cg_iters += ss.iterations;
+      r.subiters++;
+      int conv = 0;
+      if ((rc = cfd_check_iter(c, P.tolerance, &conv, nullptr))) return rc;
+      if (conv) break;
+      cfd_rotate(c);
+      if ((rc = cfd_k_times_acc(c))) return rc;
+    }
+    r.last_iter = iter;
+    int steady = 0;
+    c->maxAcc = c->last_norms[4];
+    steady = (c->maxAcc > P.convergence) ? 0 : 1;
+    cfd_end_step(c);
+    r.steps++;
+    r.maxAcc = c->maxAcc;
+    if (steady) {
+      r.steady = 1;
+      break;
+    }
+  }
+  if (st) *st = r;
+  return CFD_OK;
+}
+
+int cfd_get_monitor(cfd_ctx* c, int node, double* out) {
+  if (!c || !out || !c->loaded) return CFD_E_BADARG;
+  if (node < 0) node = c->P.monPoint;
+  NEED(node < c->P.NN, "monitor node out of range");
+  cudaStream_t s = c->stream;
+  CU(cudaMemcpyAsync(c->h_small, c->un + node, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (node < c->P.NNp)
+    CU(cudaMemcpyAsync(c->h_small + 3, c->pn + node, sizeof(double), cudaMemcpyDeviceToHost, s));
+  else
+    c->h_small[3] = 0.0;
+  CU(cudaStreamSynchronize(s));
+  for (int i = 0; i < 4; i++) out[i] = c->h_small[i];
+  return CFD_OK;
+}
+
+int cfd_download_state(cfd_ctx* c, double* U, double* Pv) {
+  if (!c || !c->loaded) return CFD_E_BADARG;
+  cudaStream_t s = c->stream;
+  if (U) {
+    CU(launch_vec4_to_blocks(c->P.NN, c->un, c->blk.p, s));
+    CU(cudaMemcpyAsync(U, c->blk.p, 3 * (size_t)c->P.NN * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  if (Pv) CU(cudaMemcpyAsync(Pv, c->pn, (size_t)c->P.NNp * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return CFD_OK;
+}
+
+int cfd_upload_state(cfd_ctx* c, const double* U, const double* Pv) {
+  if (!c || !c->loaded) return CFD_E_BADARG;
+  cudaStream_t s = c->stream;
+  if (U) {
+    CU(cudaMemcpyAsync(c->blk.p, U, 3 * (size_t)c->P.NN * sizeof(double), cudaMemcpyHostToDevice, s));
+    CU(launch_blocks_to_vec4(c->P.NN, c->blk.p, c->un, s));
+  }
+  if (Pv) CU(cudaMemcpyAsync(c->pn, Pv, (size_t)c->P.NNp * sizeof(double), cudaMemcpyHostToDevice, s));
+  CU(cudaStreamSynchronize(s));
+  return CFD_OK;
+}
+
+int cfd_download_vector(cfd_ctx* c, int which, double* out) {
+  if (!c || !out || !c->loaded) return CFD_E_BADARG;
+  cudaStream_t s = c->stream;
+  const size_t NN = c->P.NN, NNp = c->P.NNp;
+  const double4* v4 = nullptr;
+  const double* p1 = nullptr;
+  switch (which) {
+    case CFD_V_UN: v4 = c->un; break;
+    case CFD_V_UNP1: v4 = c->unp1; break;
+    case CFD_V_UNP1_PREV: v4 = c->unp1_prev; break;
+    case CFD_V_UNPHALF: v4 = c->unphalf; break;
+    case CFD_V_UNPHALF_PREV: v4 = c->unphalf_prev; break;
+    case CFD_V_ACC: v4 = c->acc; break;
+    case CFD_V_ACC_PREV: v4 = c->acc_prev; break;
+    case CFD_V_KACC_PREV: v4 = c->kacc; break;
+    case CFD_V_R1: v4 = c->r1dbg; break;
+    case CFD_V_R3: v4 = c->r3dbg; break;
+    case CFD_V_PN: p1 = c->pn; break;
+    case CFD_V_PNP1: p1 = c->pnp1; break;
+    case CFD_V_PNP1_PREV: p1 = c->pnp1_prev; break;
+    case CFD_V_PDOT: p1 = c->pdot; break;
+    case CFD_V_R2: p1 = c->r2; break;
+    case CFD_V_MDINV:
+    case CFD_V_MDORIGINV: {
+      NEED(c->assembled, "mass matrix not assembled");
+      std::vector<double> m(NN);
+      std::vector<unsigned char> bc(NN);
+      CU(cudaMemcpyAsync(m.data(), c->minv_orig.p, NN * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+      for (int i : c->P.bcnode) bc[i] = 1;
+      for (size_t i = 0; i < NN; i++) {
+        double v = (which == CFD_V_MDINV && bc[i]) ? 1.0 : m[i];
+        out[i] = out[NN + i] = out[2 * NN + i] = v;
+      }
+      return CFD_OK;
+    }
+    case CFD_V_DIV: {
+      NEED(c->assembled, "operators not assembled");
+      GtArgs<double> a{(int)NNp, 0, c->gt_rp.p, c->gt_col.p, c->gt1.p, c->gt2.p, c->gt3.p, c->unp1, c->ir_r.p};
+      CU(launch_gt<double>(a, c->num_sms, s));
+      p1 = c->ir_r.p;
+      break;
+    }
+    default:
+      return fail(c, CFD_E_BADARG, "unknown vector id %d", which);
+  }
+  if (v4) {
+    CU(launch_vec4_to_blocks((int)NN, v4, c->blk.p, s));
+    CU(cudaMemcpyAsync(out, c->blk.p, 3 * NN * sizeof(double), cudaMemcpyDeviceToHost, s));
+  } else {
+    CU(cudaMemcpyAsync(out, p1, NNp * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  CU(cudaStreamSynchronize(s));
+  return CFD_OK;
+}
+
+int cfd_download_matrix(cfd_ctx* c, int which, long long* nnz, int* rowptr, int* col, double* val) {
+  if (!c || !c->loaded) return CFD_E_BADARG;
+  const HostProblem& P = c->P;
+  const std::vector<int>* rp = nullptr;
+  const std::vector<int>* cl = nullptr;
+  const double* v[3] = {nullptr, nullptr, nullptr};
+  switch (which) {
+    case CFD_M_K: rp = &P.k_rp; cl = &P.k_col; v[0] = c->kval.p; break;
+    case CFD_M_G: rp = &P.g_rp; cl = &P.g_col; v[0] = c->g1.p; v[1] = c->g2.p; v[2] = c->g3.p; break;
+    case CFD_M_GT: rp = &P.gt_rp; cl = &P.gt_col; v[0] = c->gt1.p; v[1] = c->gt2.p; v[2] = c->gt3.p; break;
+    case CFD_M_Z: rp = &P.z_rp; cl = &P.z_col; v[0] = c->zval.p; break;
+    default: return fail(c, CFD_E_BADARG, "unknown matrix id %d", which);
+  }
+  const size_t n = cl->size();
+  if (nnz) *nnz = (long long)n;
+  if (rowptr) std::copy(rp->begin(), rp->end(), rowptr);
+  if (col) std::copy(cl->begin(), cl->end(), col);
+  if (val) {
+    NEED(c->assembled, "operators not assembled");
+    cudaStream_t s = c->stream;
+    if (!v[1]) {
+      CU(cudaMemcpyAsync(val, v[0], n * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+    } else {
+      std::vector<double> t(n);
+      for (int d = 0; d < 3; d++) {
+        CU(cudaMemcpyAsync(t.data(), v[d], n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        for (size_t i = 0; i < n; i++) val[3 * i + d] = t[i];
+      }
+    }
+  }
+  return CFD_OK;
+}
+
+int cfd_pressure_solve(cfd_ctx* c, const double* rhs, double* x, cfd_solve_stats* st) {
+  if (!c || !rhs || !x) return CFD_E_BADARG;
+  NEED(c->assembled, "cfd_pressure_solve before cfd_step0");
+  cudaStream_t s = c->stream;
+  const size_t NNp = c->P.NNp;
+  // use r2 as the right-hand side slot and pdot as the solution slot
+  CU(cudaMemcpyAsync(c->r2, rhs, NNp * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (c->opt.cg_warm) CU(cudaMemcpyAsync(c->pdot, x, NNp * sizeof(double), cudaMemcpyHostToDevice, s));
+  int rc = pressure_solve(c, c->r2, c->pdot, c->opt.cg_warm, st);
+  if (rc && rc != CFD_E_NOCONV) return rc;
+  CU(cudaMemcpyAsync(x, c->pdot, NNp * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return rc;
+}
+
+int cfd_write_tecplot(cfd_ctx* c, const char* path, const char* title) {
+  if (!c || !path || !c->loaded) return CFD_E_BADARG;
+  std::vector<double> U(3 * (size_t)c->P.NN), Pv(c->P.NNp);
+  int rc = cfd_download_state(c, U.data(), Pv.data());
+  if (rc) return rc;
+  rc = write_tecplot(c->P, U.data(), Pv.data(), path, title ? title : "");
+  if (rc) return fail(c, rc, "cannot write %s", path);
+  return CFD_OK;
+}
+
+int cfd_read_restart(cfd_ctx* c, const char* path) {
+  if (!c || !path || !c->loaded) return CFD_E_BADARG;
+  std::vector<double> U(3 * (size_t)c->P.NN, 0.0), Pv(c->P.NNp, 0.0);
+  int rc = read_restart(c->P, path, U.data(), Pv.data());
+  if (rc) return fail(c, rc, "cannot read restart file %s", path);
+  return cfd_upload_state(c, U.data(), Pv.data());
+}
+
+int cfd_set_bc_values(cfd_ctx* c, int n, const int* nodes, const double* uvw) {
+  if (!c || !c->loaded || n < 0 || (n > 0 && (!nodes || !uvw))) return CFD_E_BADARG;
+  for (int i = 0; i < n; i++) NEED(nodes[i] >= 0 && nodes[i] < c->P.NN, "BC node out of range");
+  DevBuf<int> dn;
+  DevBuf<double> dv;
+  cudaStream_t s = c->stream;
+  CU(dn.alloc(n));
+  CU(dv.alloc(3 * (size_t)n));
+  CU(cudaMemcpyAsync(dn.p, nodes, n * sizeof(int), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(dv.p, uvw, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CU(launch_apply_bc(n, dn.p, dv.p, c->un, s));
+  CU(cudaStreamSynchronize(s));
+  return CFD_OK;
+}
+
+void* cfd_stream(cfd_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+long long cfd_launch_count(const cfd_ctx* c) { return c ? c->launches : -1; }
+
+int cfd_profile(cfd_ctx* c, int on) {
+  if (!c) return CFD_E_BADARG;
+  cudaStream_t s = c->stream;
+  CU(cudaStreamSynchronize(s));
+  harvest(c);
+  if (on) std::memset(c->prof, 0, sizeof(c->prof));
+  c->prof_on = on != 0;
+  return CFD_OK;
+}
+
+int cfd_profile_read(cfd_ctx* c, double* out) {
+  if (!c || !out) return CFD_E_BADARG;
+  CU(cudaStreamSynchronize(c->stream));
+  harvest(c);
+  for (int k = 0; k < CFD_K_COUNT; k++)
+    for (int j = 0; j < 3; j++) out[3 * k + j] = c->prof[k][j];
+  return CFD_OK;
+}
+
+int cfd_selftest_wait_timeout(cfd_ctx* c, int timeout_ms) {
+  if (!c || timeout_ms <= 0 || timeout_ms > 10000) return CFD_E_BADARG;
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t s = c->stream;
+  DevBuf<int> flags;
+  CU(flags.alloc(2));
+  CU(cudaMemsetAsync(flags.p, 0, 2 * sizeof(int), s));
+  KL(CFD_K_OTHER, launch_wait_selftest(flags.p, flags.p + 1, (unsigned long long)timeout_ms * 1000000ULL, s));
+  int h[2] = {0, 0};
+  CU(cudaMemcpyAsync(h, flags.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (h[1]) return fail(c, CFD_E_TIMEOUT, "bounded wait gave up after %d ms (self-test)", timeout_ms);
+  return CFD_OK;
+}
+
+int cfd_unet_load(cfd_ctx* c, const char* path) {
+  if (!c || !path) return CFD_E_BADARG;
+  return fail(c, CFD_E_BADARG, "learned preconditioner weights are not supported by this build yet");
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// Device helpers shared by the solver kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cfd {
+
+constexpr int kMaxNGP = 27;
+
+// Quadrature and shape-function tables for hex27 velocity / hex8 pressure
+// elements at the Gauss points (blascoCodinaHuerta.cpp:2166-2488), laid out
+// for the device: Sv[k][j], dSv[d][k][j], Sp[k][m], dSp[d][k][m].
+struct Basis {
+  int ngp;
+  int pad;
+  double w[kMaxNGP];
+  double Sv[kMaxNGP][27];
+  double dSv[3][kMaxNGP][27];
+  double Sp[kMaxNGP][8];
+  double dSp[3][kMaxNGP][8];
+};
+
+#if defined(__CUDACC__)
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// Sum over aligned groups of G lanes (G a power of two <= 32); every lane of
+// the group receives the group sum.
+template <int G, class T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide sum of NV values (blockDim.x a multiple of 32, <= 1024).  The
+// result is valid in thread 0.  Fixed reduction tree: deterministic.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
+  __shared__ double sh[32][NV];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; k++) sh[warp][k] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double t = lane < nw ? sh[lane][k] : 0.0;
+      v[k] = warp_sum(t);
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_volatile_i32(const int* p) {
+  return *reinterpret_cast<const volatile int*>(p);
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier for a cooperative (co-resident) launch.  bar[0] counts
+// arrivals, bar[1] is the generation.  Every wait is bounded: after
+// timeout_ns a waiting block raises *err and returns false; blocks that see
+// *err set also return false.  The host clears bar and err before a launch.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned long long timeout_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    unsigned gen = ld_acquire_u32(bar + 1);
+    __threadfence();
+    unsigned arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned long long t0 = global_ns();
+      while (ld_acquire_u32(bar + 1) == gen) {
+        if (ld_volatile_i32(err)) { ok = 0; break; }
+        if (global_ns() - t0 > timeout_ns) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    if (ok && ld_volatile_i32(err)) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Read-only 32-byte load of a double4 node value (two 16-byte loads of the
+// same aligned sector).
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = __ldg(q), b = __ldg(q + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// Position of key in the sorted range col[b, e); -1 when absent.
+__device__ __forceinline__ int bsearch_slot(const int* __restrict__ col, int b, int e, int key) {
+  int lo = b, hi = e - 1;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1;
+    int c = __ldg(col + mid);
+    if (c == key) return mid;
+    if (c < key) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace cfd

@@ -1,0 +1,164 @@
+// Convection right-hand side R1 = -A(Un) UnpHalf_prev, matrix-free
+// (calculateMatrixA, blascoCodinaHuerta.cpp:3520-3685; calcAndAssembleMatrixA,
+// CUDAcodes.cu:695-899).
+//
+// The reference forms the 27x27 element matrix
+//   Ae[i][j] = sum_k (u0_k . grad Sv_j(k)) Sv_i(k) detJ_k w_k
+// and multiplies it with the element's UnpHalf_prev values.  The same sum is
+// evaluated here in factored form, which needs no Ae:
+//   c_k^d  = u0_k . grad(uprev^d)(k)       (u0_k interpolated from Un)
+//   R1e_i^d = sum_k Sv_i(k) detJ_k w_k c_k^d
+// with grad(uprev^d)(k) = J_k^{-1} (sum_j dSv_j(k) uprev_j^d), J_k rebuilt
+// from the 8 corner coordinates.  One thread per (element, Gauss point);
+// elements and their gathered nodal values sit in shared memory; results are
+// scattered with FP64 atomics (no element colouring).  Work per element is
+// about 30x fewer flops than the Ae form, so the kernel is bound by the
+// gathers of Un / UnpHalf_prev and the atomic scatter, not by arithmetic.
+#include "kernels.h"
+
+namespace cfd {
+
+namespace {
+
+constexpr int kConvThreads = 128;
+
+template <class T, int TPE>
+__global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
+  constexpr int EPB = kConvThreads / TPE;
+  constexpr int NG = TPE < kMaxNGP ? TPE : kMaxNGP;
+  __shared__ T sSv[NG][27];
+  __shared__ T sdSv[3][NG][27];
+  __shared__ T sdSp[3][NG][8];
+  __shared__ T sw[NG];
+  __shared__ T u0[EPB][27][3];
+  __shared__ T up[EPB][27][3];
+  __shared__ T X[EPB][8][3];
+  __shared__ T cc[EPB][NG][3];
+  __shared__ int lt[EPB][27];
+  const int t = threadIdx.x, ngp = a.ngp;
+  const Basis* B = a.basis;
+  for (int i = t; i < ngp * 27; i += blockDim.x) {
+    int k = i / 27, j = i % 27;
+    sSv[k][j] = (T)B->Sv[k][j];
+    sdSv[0][k][j] = (T)B->dSv[0][k][j];
+    sdSv[1][k][j] = (T)B->dSv[1][k][j];
+    sdSv[2][k][j] = (T)B->dSv[2][k][j];
+  }
+  for (int i = t; i < ngp * 8; i += blockDim.x) {
+    int k = i / 8, m = i % 8;
+    sdSp[0][k][m] = (T)B->dSp[0][k][m];
+    sdSp[1][k][m] = (T)B->dSp[1][k][m];
+    sdSp[2][k][m] = (T)B->dSp[2][k][m];
+  }
+  for (int i = t; i < ngp; i += blockDim.x) sw[i] = (T)B->w[i];
+  const int el = t / TPE, tk = t % TPE;
+  for (int e0 = blockIdx.x * EPB; e0 < a.NE; e0 += gridDim.x * EPB) {
+    __syncthreads();
+    for (int idx = t; idx < EPB * 27; idx += blockDim.x) {
+      int l = idx / 27, i = idx % 27, e = e0 + l;
+      if (e < a.NE) {
+        int node = __ldg(a.ltog + (size_t)e * 27 + i);
+        lt[l][i] = node;
+        double4 u = ldg4(a.un + node);
+        double4 p = ldg4(a.uprev + node);
+        u0[l][i][0] = (T)u.x; u0[l][i][1] = (T)u.y; u0[l][i][2] = (T)u.z;
+        up[l][i][0] = (T)p.x; up[l][i][1] = (T)p.y; up[l][i][2] = (T)p.z;
+      }
+    }
+    __syncthreads();
+    for (int idx = t; idx < EPB * 24; idx += blockDim.x) {
+      int l = idx / 24, r = idx % 24, e = e0 + l;
+      if (e < a.NE) X[l][r / 3][r % 3] = (T)__ldg(a.coord + 3 * (size_t)lt[l][r / 3] + r % 3);
+    }
+    __syncthreads();
+    const int e = e0 + el;
+    if (e < a.NE && tk < ngp) {
+      const int k = tk;
+      // Jacobian of the trilinear corner map at Gauss point k
+      T J[3][3];
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          T s = 0;
+#pragma unroll
+          for (int m = 0; m < 8; m++) s += sdSp[i][k][m] * X[el][m][j];
+          J[i][j] = s;
+        }
+      T det = J[0][0] * (J[1][1] * J[2][2] - J[2][1] * J[1][2]) + J[0][1] * (J[1][2] * J[2][0] - J[1][0] * J[2][2]) +
+              J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+      T inv = T(1) / det;
+      T iJ[3][3];
+      iJ[0][0] = (J[1][1] * J[2][2] - J[2][1] * J[1][2]) * inv;
+      iJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) * inv;
+      iJ[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * inv;
+      iJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) * inv;
+      iJ[1][1] = (J[2][2] * J[0][0] - J[2][0] * J[0][2]) * inv;
+      iJ[1][2] = -(J[1][2] * J[0][0] - J[1][0] * J[0][2]) * inv;
+      iJ[2][0] = (J[1][0] * J[2][1] - J[2][0] * J[1][1]) * inv;
+      iJ[2][1] = -(J[2][1] * J[0][0] - J[2][0] * J[0][1]) * inv;
+      iJ[2][2] = (J[1][1] * J[0][0] - J[1][0] * J[0][1]) * inv;
+      // u0 at the Gauss point and reference-space gradients of uprev
+      T uk[3] = {0, 0, 0};
+      T g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // g[a][d] = d uprev^d / d xi_a
+#pragma unroll 3
+      for (int j = 0; j < 27; j++) {
+        T sv = sSv[k][j], d0 = sdSv[0][k][j], d1 = sdSv[1][k][j], d2 = sdSv[2][k][j];
+        T a0 = u0[el][j][0], a1 = u0[el][j][1], a2 = u0[el][j][2];
+        T b0 = up[el][j][0], b1 = up[el][j][1], b2 = up[el][j][2];
+        uk[0] += sv * a0; uk[1] += sv * a1; uk[2] += sv * a2;
+        g[0][0] += d0 * b0; g[0][1] += d0 * b1; g[0][2] += d0 * b2;
+        g[1][0] += d1 * b0; g[1][1] += d1 * b1; g[1][2] += d1 * b2;
+        g[2][0] += d2 * b0; g[2][1] += d2 * b1; g[2][2] += d2 * b2;
+      }
+      const T f = det * sw[k];
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        // physical gradient of uprev^d: grad_i = sum_a iJ[i][a] g[a][d]
+        T gx = iJ[0][0] * g[0][d] + iJ[0][1] * g[1][d] + iJ[0][2] * g[2][d];
+        T gy = iJ[1][0] * g[0][d] + iJ[1][1] * g[1][d] + iJ[1][2] * g[2][d];
+        T gz = iJ[2][0] * g[0][d] + iJ[2][1] * g[1][d] + iJ[2][2] * g[2][d];
+        cc[el][k][d] = (uk[0] * gx + uk[1] * gy + uk[2] * gz) * f;
+      }
+    }
+    __syncthreads();
+    if (e < a.NE) {
+      for (int i = tk; i < 27; i += TPE) {
+        T s0 = 0, s1 = 0, s2 = 0;
+        for (int k = 0; k < ngp; k++) {
+          T sv = sSv[k][i];
+          s0 += sv * cc[el][k][0];
+          s1 += sv * cc[el][k][1];
+          s2 += sv * cc[el][k][2];
+        }
+        double4* dst = a.r1 + lt[el][i];
+        atomicAdd(&dst->x, -(double)s0);
+        atomicAdd(&dst->y, -(double)s1);
+        atomicAdd(&dst->z, -(double)s2);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+template <class T>
+cudaError_t launch_convect(const ConvArgs<T>& a, int num_sms, cudaStream_t s) {
+  if (a.ngp <= 8) {
+    constexpr int EPB = kConvThreads / 8;
+    int grid = (a.NE + EPB - 1) / EPB;
+    if (grid > num_sms * 12) grid = num_sms * 12;
+    k_convect<T, 8><<<grid, kConvThreads, 0, s>>>(a);
+  } else {
+    constexpr int EPB = kConvThreads / 32;
+    int grid = (a.NE + EPB - 1) / EPB;
+    if (grid > num_sms * 12) grid = num_sms * 12;
+    k_convect<T, 32><<<grid, kConvThreads, 0, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_convect<double>(const ConvArgs<double>&, int, cudaStream_t);
+template cudaError_t launch_convect<float>(const ConvArgs<float>&, int, cudaStream_t);
+
+}  // namespace cfd

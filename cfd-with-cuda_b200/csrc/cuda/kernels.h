@@ -1,0 +1,168 @@
+// Host-visible launch interface of the solver kernels (plain pointers only).
+//
+// Device data layout (HBM):
+//   velocity-sized vectors  double4 per node (x, y, z, pad = 0): one aligned
+//                           32-byte sector per gathered node
+//   pressure-sized vectors  double (or float for the FP32 inner solve)
+//   K (NN x NN)             CSR: int32 rowptr/col + FP64 (and FP32) values
+//   G (NN x NNp)            CSR: int32 rowptr/col + three value arrays G1..G3
+//   G^T (NNp x NN)          CSR of the transpose (gather form, no atomics)
+//   Z (NNp x NNp)           CSR: int32 rowptr/col + values
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace cfd {
+
+struct AsmArgs {
+  int NE, ngp;
+  const int* ltog;
+  const double* coord;
+  const Basis* basis;
+  double viscosity, inv_density;
+  const int *k_rp, *k_col;
+  double* kval;
+  const int *g_rp, *g_col;
+  double *g1, *g2, *g3;
+  double* msum;  // NN: row sums of M
+};
+cudaError_t launch_assemble(const AsmArgs& a, int num_sms, cudaStream_t s);
+
+// Gt values from G (Gt[k] = G[pos[k]]), MdOrigInv / MdInv-with-BC-mask.
+cudaError_t launch_fill_gt(long long nnz, const int* pos, const double* g1, const double* g2,
+                           const double* g3, double* gt1, double* gt2, double* gt3, cudaStream_t s);
+cudaError_t launch_md_finalize(int NN, const double* msum, const unsigned char* bcmask, double* minv_orig,
+                               double* minv_free, cudaStream_t s);
+
+struct ZArgs {
+  int NNp, maxrow, zeroP;
+  const int *z_rp, *z_col;
+  double* zval;
+  double* zdiag;
+  const int *gt_rp, *gt_col;
+  const double *gt1, *gt2, *gt3;
+  const int *g_rp, *g_col;
+  const double *g1, *g2, *g3;
+  const double* minv_orig;
+};
+cudaError_t launch_build_z(const ZArgs& a, cudaStream_t s);
+
+cudaError_t launch_to_float(long long n, const double* in, float* out, cudaStream_t s);
+cudaError_t launch_recip(long long n, const double* in, double* out64, float* out32, cudaStream_t s);
+
+template <class T>
+struct ConvArgs {
+  int NE, ngp;
+  const int* ltog;
+  const double* coord;
+  const Basis* basis;
+  const double4* un;     // convecting velocity (time level n)
+  const double4* uprev;  // UnpHalf_prev
+  double4* r1;           // accumulates -A(un) uprev (zeroed by the caller)
+};
+template <class T>
+cudaError_t launch_convect(const ConvArgs<T>& a, int num_sms, cudaStream_t s);
+
+template <class VT>
+struct Step1Args {
+  int NN, iter;
+  double dt;
+  const int *k_rp, *k_col;
+  const VT* kval;
+  const int *g_rp, *g_col;
+  const VT *g1, *g2, *g3;
+  const double4 *uprev, *un, *r1conv, *kacc;
+  const double *pn, *minv_free, *minv_orig;
+  double4 *unphalf, *d, *r1out;  // r1out may be null
+};
+template <class VT>
+cudaError_t launch_step1(const Step1Args<VT>& a, int num_sms, cudaStream_t s);
+
+template <class VT>
+struct GtArgs {
+  int NNp, pin;  // pin: row forced to 0 (< 1 disables, as the reference's node > 0 test)
+  const int *gt_rp, *gt_col;
+  const VT *gt1, *gt2, *gt3;
+  const double4* d;
+  double* out;
+};
+template <class VT>
+cudaError_t launch_gt(const GtArgs<VT>& a, int num_sms, cudaStream_t s);
+
+template <class VT>
+struct Step3Args {
+  int NN, iter;
+  double dt;
+  const int *g_rp, *g_col;
+  const VT *g1, *g2, *g3;
+  const double* pdot;
+  const double4 *kacc, *unphalf, *un, *unp1_prev;
+  const double* minv_free;
+  double4 *acc, *unp1, *r3out;  // r3out may be null
+  double* part;                 // 3 x nblocks partials: sum U^2, sum dU^2, max |dU|/dt
+  int nblocks;
+};
+template <class VT>
+cudaError_t launch_step3(const Step3Args<VT>& a, cudaStream_t s);
+int step3_blocks(int NN, int num_sms);
+
+template <class VT>
+struct SpmvK3Args {
+  int NN;
+  const int *rp, *col;
+  const VT* val;
+  const double4* x;
+  double4* y;
+};
+template <class VT>
+cudaError_t launch_spmv_k3(const SpmvK3Args<VT>& a, int num_sms, cudaStream_t s);
+
+// Pnp1 = Pn + dt*Pdot and the pressure-change partial sums.
+cudaError_t launch_pressure_update(int NNp, double dt, const double* pn, const double* pdot,
+                                   const double* pprev, double* pnp1, double* part, int nblocks,
+                                   cudaStream_t s);
+int pupdate_blocks(int NNp, int num_sms);
+
+// out[0..4] = {sum U^2, sum dU^2, sum P^2, sum dP^2, max|dU|/dt}
+cudaError_t launch_reduce_norms(const double* upart, int nub, const double* ppart, int npb, double* out,
+                                cudaStream_t s);
+
+// ---- Krylov ----
+template <class VT>
+struct PcgArgs {
+  int n;
+  const int *rp, *col;
+  const VT* val;
+  const VT* dinv;
+  const VT* b;
+  VT *x, *r, *z, *p, *q;
+  double* part;  // 2 x 3 x grid doubles
+  unsigned* bar; // 2 unsigned (host-zeroed)
+  int* err;      // host-zeroed
+  double rtol;
+  int maxit, warm;
+  double* result;  // its, relres, status, bnorm
+  unsigned long long timeout_ns;
+};
+template <class VT>
+cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s);
+template <class VT>
+int pcg_max_grid(int n, int device);
+
+// r = b - Z x (FP64) and the partial sum of r^2 per block; rf = (float) r.
+cudaError_t launch_residual64(int n, const int* rp, const int* col, const double* val, const double* b,
+                              const double* x, double* r, float* rf, double* part, int nblocks,
+                              cudaStream_t s);
+int residual_blocks(int n, int num_sms);
+cudaError_t launch_axpy_f2d(int n, const float* e, double* x, cudaStream_t s);
+cudaError_t launch_sum_partials(const double* part, int n, double* out, cudaStream_t s);
+
+cudaError_t launch_wait_selftest(const int* flag, int* err, unsigned long long timeout_ns, cudaStream_t s);
+
+// layout conversion between the reference's [u|v|w] blocks and double4 nodes
+cudaError_t launch_blocks_to_vec4(int NN, const double* blocks, double4* v, cudaStream_t s);
+cudaError_t launch_vec4_to_blocks(int NN, const double4* v, double* blocks, cudaStream_t s);
+cudaError_t launch_apply_bc(int n, const int* nodes, const double* uvw, double4* u, cudaStream_t s);
+
+}  // namespace cfd

@@ -1,0 +1,86 @@
+// Host-only part of the C ABI: deck reading and mesh preprocessing without
+// a device (cfdh_*), used to inspect numbering and patterns.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../../include/cfdfs.h"
+#include "problem.h"
+
+namespace cfd {
+int write_tecplot(const HostProblem& P, const double* U, const double* Pn, const std::string& path,
+                  const std::string& title);
+}
+
+struct cfd_host {
+  cfd::HostProblem P;
+};
+
+extern "C" {
+
+int cfdh_load(cfd_host** out, const char* path, char* errbuf, int errlen) {
+  if (!out || !path) return CFD_E_BADARG;
+  *out = nullptr;
+  cfd_host* h = new cfd_host();
+  std::string err;
+  int rc = cfd::read_inp(path, h->P, err);
+  if (!rc) rc = cfd::preprocess(h->P, err);
+  if (rc) {
+    if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", err.c_str());
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return CFD_OK;
+}
+
+void cfdh_free(cfd_host* h) { delete h; }
+
+int cfdh_sizes(const cfd_host* h, long long* o) {
+  if (!h || !o) return CFD_E_BADARG;
+  const cfd::HostProblem& P = h->P;
+  o[0] = P.NE; o[1] = P.NCN; o[2] = P.NN; o[3] = P.NNp;
+  o[4] = (long long)P.k_col.size(); o[5] = (long long)P.g_col.size(); o[6] = (long long)P.z_col.size();
+  o[7] = (long long)P.bcnode.size(); o[8] = P.monPoint; o[9] = P.zeroP; o[10] = P.NGP; o[11] = P.maxIter;
+  return CFD_OK;
+}
+
+int cfdh_get_ltog(const cfd_host* h, int* out) {
+  if (!h || !out) return CFD_E_BADARG;
+  std::copy(h->P.ltog.begin(), h->P.ltog.end(), out);
+  return CFD_OK;
+}
+
+int cfdh_get_coord(const cfd_host* h, double* out) {
+  if (!h || !out) return CFD_E_BADARG;
+  std::copy(h->P.coord.begin(), h->P.coord.end(), out);
+  return CFD_OK;
+}
+
+int cfdh_get_bcnodes(const cfd_host* h, int* out) {
+  if (!h || !out) return CFD_E_BADARG;
+  for (size_t i = 0; i < h->P.bcnode.size(); i++) {
+    out[2 * i] = h->P.bcnode[i];
+    out[2 * i + 1] = h->P.bcid[i];
+  }
+  return CFD_OK;
+}
+
+int cfdh_get_pattern(const cfd_host* h, int which, int* rowptr, int* col) {
+  if (!h) return CFD_E_BADARG;
+  const cfd::HostProblem& P = h->P;
+  const std::vector<int>* rp[4] = {&P.k_rp, &P.g_rp, &P.gt_rp, &P.z_rp};
+  const std::vector<int>* cl[4] = {&P.k_col, &P.g_col, &P.gt_col, &P.z_col};
+  if (which < 0 || which > 3) return CFD_E_BADARG;
+  if (rowptr) std::copy(rp[which]->begin(), rp[which]->end(), rowptr);
+  if (col) std::copy(cl[which]->begin(), cl[which]->end(), col);
+  return CFD_OK;
+}
+
+int cfdh_write_tecplot(const cfd_host* h, const double* U, const double* Pv, const char* path, const char* title) {
+  if (!h || !U || !Pv || !path) return CFD_E_BADARG;
+  return cfd::write_tecplot(h->P, U, Pv, path, title ? title : "");
+}
+
+}  // extern "C"

@@ -1,0 +1,249 @@
+/*
+ * cfdfs.h -- C ABI of the B200 fractional-step solver (libcfdfs.so).
+ *
+ * Drop-in replacement for the device seam of the reference solver: the eleven
+ * C++ functions that fractionalStep/Cpp/blascoCodinaHuerta.cpp declares at
+ * lines 365-377 and that fractionalStep/Cpp/CUDAcodes.cu defines, plus the
+ * host preprocessing of blascoCodinaHuerta.cpp:528-2711 that feeds them.
+ * Each entry point names the reference function it replaces.
+ *
+ * Conventions
+ *   - Every call returns CFD_OK (0) or a negative CFD_E_* code; none blocks
+ *     on user input or exits (the reference prints "ErrorNN" and waits on
+ *     std::cin, e.g. CUDAcodes.cu:184-250).  cfd_last_error() gives text.
+ *   - One context = one GPU, one CUDA stream, single-threaded use.
+ *   - Host buffers belong to the caller; device buffers to the context.
+ *   - Vectors crossing the ABI use the reference layout: velocity as three
+ *     component blocks [u(0..NN-1) | v | w] (blascoCodinaHuerta.cpp:1348-1368),
+ *     pressure on the NNp corner nodes.  Node numbers are the reference's
+ *     (corner nodes first, then mid-edge, mid-face and centre nodes).
+ */
+#ifndef CFDFS_H
+#define CFDFS_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CFDFS_ABI_VERSION 1
+
+enum cfd_status {
+  CFD_OK = 0,
+  CFD_E_CUDA = -1,      /* CUDA runtime error or no usable device */
+  CFD_E_NOCONV = -2,    /* Krylov solve hit its iteration limit */
+  CFD_E_NONFINITE = -3, /* NaN/Inf in a residual or norm */
+  CFD_E_TIMEOUT = -4,   /* a bounded device-side wait gave up */
+  CFD_E_BADARG = -5,    /* invalid argument or call order */
+  CFD_E_BADINPUT = -6,  /* malformed .inp deck */
+  CFD_E_IO = -7,        /* file could not be opened / written */
+  CFD_E_NOMEM = -8      /* device allocation failed */
+};
+
+enum cfd_precision {
+  CFD_FP64 = 0,  /* all operators, vectors and Krylov work in FP64 */
+  CFD_MIXED = 1  /* FP32 operators and inner CG; FP64 state, FP64 outer
+                    refinement residual, FP64 norms and divergence */
+};
+
+enum cfd_precond {
+  CFD_PC_JACOBI = 0,  /* Jacobi-preconditioned CG (reference behaviour) */
+  CFD_PC_LEARNED = 1  /* learned U-Net preconditioner in flexible CG, with
+                         Jacobi-PCG fallback when it stalls */
+};
+
+typedef struct cfd_ctx cfd_ctx;
+
+typedef struct {
+  int precision;     /* enum cfd_precision (default CFD_FP64) */
+  int precond;       /* enum cfd_precond (default CFD_PC_JACOBI) */
+  double cg_rtol;    /* stop when ||r||_2 <= cg_rtol*||b||_2 (default 1e-8) */
+  int cg_maxit;      /* default 1000, as blascoCodinaHuerta.cpp:4013 */
+  int cg_warm;       /* 0: x0 = 0 (MKL call site, blascoCodinaHuerta.cpp:4002);
+                        1: x0 = previous solution (CUSP call site, CUDAcodes.cu:268) */
+  int ngp_override;  /* 0: NGP from the deck; 8 or 27 overrides it */
+  double inner_rtol; /* CFD_MIXED: inner FP32 solve tolerance (default 1e-4) */
+  int max_outer;     /* CFD_MIXED: refinement sweeps (default 12) */
+} cfd_options;
+
+typedef struct {
+  int NE, NCN, NN, NNp, NGP, maxIter;
+  long long nnzK, nnzG, nnzZ;
+  int nBCnodes, monPoint, zeroPressureNode;
+  double dt, t_ini, t_final, tolerance, convergence, density, viscosity;
+  int timeN;
+  double timeT;
+} cfd_problem_info;
+
+typedef struct {
+  int iterations;   /* Krylov iterations (inner iterations in CFD_MIXED) */
+  int outer;        /* refinement sweeps (CFD_MIXED), 0 otherwise */
+  double relres;    /* final ||r||/||b|| (FP64 residual) */
+  int status;       /* 0 converged, 1 iteration limit, 2 non-finite, 3 timeout */
+  int fallback;     /* 1 when the learned preconditioner stalled and Jacobi took over */
+} cfd_solve_stats;
+
+typedef struct {
+  int steps;             /* time steps run */
+  long long subiters;    /* fractional-step sub-iterations run */
+  long long cg_iters;    /* Krylov iterations over all solves */
+  int steady;            /* 1 if the steady-state test fired */
+  double maxAcc;         /* last max |Unp1-Un|/dt */
+  int last_iter;         /* iteration index printed by the monitor (maxIter+1 if none converged) */
+} cfd_run_stats;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* selectCUDAdevice, CUDAcodes.cu:126-154 (device < 0 picks the last device,
+ * as the reference does). */
+int cfd_create(cfd_ctx** out, int device);
+void cfd_destroy(cfd_ctx* ctx);
+const char* cfd_last_error(const cfd_ctx* ctx);
+int cfd_abi_version(void);
+void cfd_default_options(cfd_options* opt);
+int cfd_set_options(cfd_ctx* ctx, const cfd_options* opt);
+
+/* ---- problem set-up ---------------------------------------------------- */
+
+/* readInputFile (blascoCodinaHuerta.cpp:528-725) followed by the mesh
+ * preprocessing of blascoCodinaHuerta.cpp:732-2159 (hex27 node generation,
+ * DOF maps, velocity-BC nodes, monitor node, CSR patterns), the basis set-up
+ * of blascoCodinaHuerta.cpp:2166-2488, the initial condition of
+ * applyBC_initial (blascoCodinaHuerta.cpp:4062-4110) and the device upload of
+ * initializeAndAllocateGPU (CUDAcodes.cu:161-274). */
+int cfd_load_inp(cfd_ctx* ctx, const char* path);
+
+/* Same as cfd_load_inp from in-memory deck data (0-based ids):
+ * coords NCN x 3, conn NE x 8, bcvals nBC x 3, velfaces nVelFaces x 3
+ * (element, face 0..5, bc).  Header values come from info (NE, NCN, NGP,
+ * maxIter, dt, t_ini, t_final, tolerance, convergence, density, viscosity,
+ * zeroPressureNode) and monitor[3]. */
+int cfd_load_mesh(cfd_ctx* ctx, const cfd_problem_info* info, const double* coords, const int* conn,
+                  int nBC, const double* bcvals, int nVelFaces, const int* velfaces,
+                  const double* monitor);
+
+int cfd_info(const cfd_ctx* ctx, cfd_problem_info* info);
+
+/* step0 (blascoCodinaHuerta.cpp:3127-3315) on the device: M row sums, K, G,
+ * G^T assembled into their CSR slots, MdInv/MdOrigInv, and calculateZ_CUSP
+ * (CUDAcodes.cu:281-411) including the Z[p][p] *= 1000 pin. */
+int cfd_step0(cfd_ctx* ctx);
+
+/* ---- one time step, stage by stage (timeLoop, blascoCodinaHuerta.cpp:2859-3094) */
+
+/* timeN++, timeT += dt, UnpHalf_prev <- Un, Pnp1_prev <- Pn, Acc_prev <- 0
+ * (blascoCodinaHuerta.cpp:2860-2881). */
+int cfd_begin_step(cfd_ctx* ctx);
+/* calculateMatrixAGPU, CUDAcodes.cu:906-939: R1 = -A(Un) UnpHalf_prev. */
+int cfd_convect(cfd_ctx* ctx);
+/* step1GPUpart, CUDAcodes.cu:946-973 (call cfd_convect first). */
+int cfd_step1(cfd_ctx* ctx, int iter);
+/* step2GPU, CUDAcodes.cu:980-1022 (pressure solve; stats may be NULL). */
+int cfd_step2(cfd_ctx* ctx, int iter, cfd_solve_stats* st);
+/* step3GPU, CUDAcodes.cu:1029-1060. */
+int cfd_step3(cfd_ctx* ctx, int iter);
+/* checkConvergenceGPU, CUDAcodes.cu:1084-1121; norms[0] = |dU|/|U|,
+ * norms[1] = |dP|/|P| (may be NULL). */
+int cfd_check_iter(cfd_ctx* ctx, double tol, int* converged, double* norms);
+/* "Get ready for the next iteration" copies, blascoCodinaHuerta.cpp:2929-2932. */
+int cfd_rotate(cfd_ctx* ctx);
+/* calculate_KtimesAcc_prevGPU, CUDAcodes.cu:1067-1077. */
+int cfd_k_times_acc(cfd_ctx* ctx);
+/* checkConvergenceInTimeGPU, CUDAcodes.cu:1151-1178, with the CPU
+ * semantics maxAcc = max |Unp1 - Un| / dt (blascoCodinaHuerta.cpp:3052-3060). */
+int cfd_check_steady(cfd_ctx* ctx, double crit, double* maxAcc, int* steady);
+/* Un <- Unp1, Pn <- Pnp1, blascoCodinaHuerta.cpp:3068-3081. */
+int cfd_end_step(cfd_ctx* ctx);
+
+/* Whole time loop on the device with one small readback per sub-iteration:
+ * nsteps > 0 runs that many steps, nsteps < 0 runs the reference's
+ * while (timeT < t_final) loop.  Stops early on steady state. */
+int cfd_run(cfd_ctx* ctx, int nsteps, cfd_run_stats* st);
+
+/* ---- state and diagnostics --------------------------------------------- */
+
+/* printMonitorDataGPU, CUDAcodes.cu:1128-1144, without the full-state copy:
+ * out = {u, v, w, p} at node (node < 0: the deck's monitor node). */
+int cfd_get_monitor(cfd_ctx* ctx, int node, double* out);
+int cfd_download_state(cfd_ctx* ctx, double* U3NN, double* P);
+int cfd_upload_state(cfd_ctx* ctx, const double* U3NN, const double* P);
+
+enum cfd_vector_id {
+  CFD_V_UN = 0, CFD_V_UNP1, CFD_V_UNP1_PREV, CFD_V_UNPHALF, CFD_V_UNPHALF_PREV, CFD_V_ACC,
+  CFD_V_ACC_PREV, CFD_V_PN, CFD_V_PNP1, CFD_V_PNP1_PREV, CFD_V_PDOT, CFD_V_MDINV,
+  CFD_V_MDORIGINV, CFD_V_KACC_PREV, CFD_V_R1, CFD_V_R2, CFD_V_R3, CFD_V_DIV
+};
+/* Any solver vector in the reference layout (3NN for velocity-sized, NNp
+ * for pressure-sized; MdInv/MdOrigInv are returned as 3NN). CFD_V_DIV is the
+ * discrete divergence G^T Unp1 (NNp), evaluated in FP64. */
+int cfd_download_vector(cfd_ctx* ctx, int which, double* out);
+
+enum cfd_matrix_id { CFD_M_K = 0, CFD_M_G = 1, CFD_M_GT = 2, CFD_M_Z = 3 };
+/* nnz of a matrix (into *nnz) and, when the arrays are non-NULL, its CSR:
+ * rowptr (nrows+1), col (nnz), val (nnz, or 3*nnz interleaved per entry
+ * for G and G^T as [G1 G2 G3]).  FP64 values. */
+int cfd_download_matrix(cfd_ctx* ctx, int which, long long* nnz, int* rowptr, int* col, double* val);
+
+/* Solve Z x = rhs on the device with the configured method (the minimal
+ * pressure-solve entry point); x holds the initial guess when cg_warm = 1. */
+int cfd_pressure_solve(cfd_ctx* ctx, const double* rhs, double* x, cfd_solve_stats* st);
+
+/* ---- files ---------------------------------------------------------------- */
+
+/* createTecplot, blascoCodinaHuerta.cpp:4249-4482 (same text layout). */
+int cfd_write_tecplot(cfd_ctx* ctx, const char* path, const char* title);
+/* readRestartFile, blascoCodinaHuerta.cpp:4214-4242. */
+int cfd_read_restart(cfd_ctx* ctx, const char* path);
+/* Per-node Dirichlet values overriding the deck's constant BC values
+ * (e.g. a parabolic duct inlet): n entries of node ids and 3n values. */
+int cfd_set_bc_values(cfd_ctx* ctx, int n, const int* nodes, const double* uvw);
+
+/* ---- learned preconditioner ----------------------------------------------- */
+
+/* Loads U-Net weights (raw file written by cfd_unet_save / the trainer). */
+int cfd_unet_load(cfd_ctx* ctx, const char* path);
+
+/* ---- timing, counters and self-tests ---------------------------------------- */
+
+/* The context's CUDA stream (cudaStream_t) so callers can record events on it. */
+void* cfd_stream(cfd_ctx* ctx);
+/* Number of kernel launches the context issued since creation. */
+long long cfd_launch_count(const cfd_ctx* ctx);
+
+enum cfd_kernel_class {
+  CFD_K_CONVECT = 0, CFD_K_STEP1, CFD_K_GT, CFD_K_PCG64, CFD_K_PCG32, CFD_K_RESID64, CFD_K_STEP3,
+  CFD_K_SPMV_K3, CFD_K_PUPDATE, CFD_K_OTHER, CFD_K_COUNT
+};
+/* Per-kernel-class CUDA-event timing on the context stream (on = 1 starts
+ * and clears, 0 stops).  out receives CFD_K_COUNT triples
+ * {launches, total milliseconds, Krylov iterations inside those launches}. */
+int cfd_profile(cfd_ctx* ctx, int on);
+int cfd_profile_read(cfd_ctx* ctx, double* out);
+
+/* Runs one small kernel whose bounded wait watches a flag nothing sets, with
+ * the given limit in milliseconds.  Returns CFD_E_TIMEOUT when the wait gave
+ * up as designed (the context stays usable), CFD_OK otherwise. */
+int cfd_selftest_wait_timeout(cfd_ctx* ctx, int timeout_ms);
+
+/* ---- host-only preprocessing (no GPU needed) --------------------------------
+ * The deck reader and mesh preprocessing of cfd_load_inp, exposed without a
+ * device so callers can inspect the generated numbering and patterns. */
+typedef struct cfd_host cfd_host;
+/* readInputFile + setupNonCornerNodes + determineVelBCnodes +
+ * findMonitorPoint + setupSparseM/G (blascoCodinaHuerta.cpp:528-2159). */
+int cfdh_load(cfd_host** out, const char* path, char* errbuf, int errlen);
+void cfdh_free(cfd_host* h);
+/* sizes: NE NCN NN NNp nnzK nnzG nnzZ nBCnodes monPoint zeroPressureNode NGP maxIter */
+int cfdh_sizes(const cfd_host* h, long long* out12);
+int cfdh_get_ltog(const cfd_host* h, int* out);     /* NE x 27 */
+int cfdh_get_coord(const cfd_host* h, double* out); /* NN x 3 */
+int cfdh_get_bcnodes(const cfd_host* h, int* out);  /* nBCnodes x 2 (node, bc) */
+/* which: 0 K (NN x NN), 1 G (NN x NNp), 2 G^T (NNp x NN), 3 Z (NNp x NNp) */
+int cfdh_get_pattern(const cfd_host* h, int which, int* rowptr, int* col);
+/* createTecplot layout (blascoCodinaHuerta.cpp:4249-4482) for given state. */
+int cfdh_write_tecplot(const cfd_host* h, const double* U3NN, const double* P, const char* path,
+                       const char* title);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CFDFS_H */

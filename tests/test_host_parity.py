@@ -1,0 +1,64 @@
+"""The product's host preprocessing (C++, cfdh_* entry points) against the
+oracle's restatement of the reference's own algorithms: identical node
+numbering, coordinates, BC nodes, monitor node and CSR patterns (bit-exact)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REFERENCE_DECK
+
+
+def _compare(path, oracle_mod):
+    from cfdfs import HostMesh
+    o = oracle_mod.Oracle(path)
+    o.step0()
+    h = HostMesh(path)
+    assert (h.NE, h.NCN, h.NN, h.NNp) == (o.NE, o.NCN, o.NN, o.NNp)
+    assert np.array_equal(h.ltog(), o.ltog())
+    assert np.array_equal(h.coord(), o.coord())          # bit-exact coordinates
+    assert np.array_equal(h.bcnodes(), o.bcnodes())
+    assert h.mon == o.mon and h.zero_p == o.zero_p
+    for which in ("K", "G", "Z"):
+        rp_h, col_h = h.pattern(which)
+        rp_o, col_o = o.pattern(which)
+        assert np.array_equal(rp_h, rp_o), which
+        assert np.array_equal(col_h, col_o), which
+    # G^T is the transpose of G
+    rp_g, col_g = h.pattern("G")
+    rp_t, col_t = h.pattern("GT")
+    import scipy.sparse as sp
+    Gs = sp.csr_matrix((np.ones(len(col_g)), col_g, rp_g), shape=(h.NN, h.NNp))
+    Ts = Gs.T.tocsr()
+    Ts.sort_indices()
+    assert np.array_equal(Ts.indptr, rp_t) and np.array_equal(Ts.indices, col_t)
+    h.close()
+    o.close()
+
+
+@pytest.mark.parametrize("key", ["c1", "graded", "perturbed", "duct_small"])
+def test_host_preprocessing_matches_oracle(decks, oracle_mod, key):
+    _compare(decks[key], oracle_mod)
+
+
+@pytest.mark.skipif(not os.path.exists(REFERENCE_DECK), reason="reference deck not present")
+def test_host_preprocessing_shipped_deck(oracle_mod):
+    _compare(REFERENCE_DECK, oracle_mod)
+
+
+def test_bad_decks_rejected(tmp_path, decks):
+    from cfdfs import HostMesh, CfdError
+    good = open(decks["c1"]).read()
+    cases = {
+        "truncated": good[: len(good) // 3],
+        "bad_corner": good.replace("\n     1        1        2", "\n     1        0        2", 1),
+        "not_hex": good.replace("NENv     : 27", "NENv     : 8"),
+        "empty": "",
+    }
+    for name, text in cases.items():
+        p = tmp_path / f"{name}.inp"
+        p.write_text(text)
+        with pytest.raises(CfdError):
+            HostMesh(str(p))
+    with pytest.raises(CfdError):
+        HostMesh(str(tmp_path / "missing.inp"))
