@@ -33,7 +33,7 @@ def test_operators_match_oracle(decks, oracle_mod, key):
     orp, ocol = o.pattern("K")
     assert np.array_equal(rp, orp) and np.array_equal(col, ocol)
     assert rel_l2(kv, o.values("K")) < OP_TOL
-    rp, col, gv = s.matrix("G")
+    g_rp, g_col, gv = s.matrix("G")
     for d, name in enumerate(("G1", "G2", "G3")):
         assert rel_l2(gv[:, d], o.values(name)) < OP_TOL, name
     rp, col, zv = s.matrix("Z")
@@ -45,7 +45,7 @@ def test_operators_match_oracle(decks, oracle_mod, key):
     # G^T values are the transpose of G
     import scipy.sparse as sp
     rpt, colt, gtv = s.matrix("GT")
-    G1 = sp.csr_matrix((gv[:, 0], col, rp), shape=(len(rp) - 1, o.NNp)).T.tocsr()
+    G1 = sp.csr_matrix((gv[:, 0], g_col, g_rp), shape=(len(g_rp) - 1, o.NNp)).T.tocsr()
     G1.sort_indices()
     assert np.array_equal(G1.data, gtv[:, 0])
     s.close()
