@@ -108,6 +108,8 @@ _PROTOS = {
     "cfd_profile": (C.c_int, [_vp, C.c_int]),
     "cfd_profile_read": (C.c_int, [_vp, _dp]),
     "cfd_selftest_wait_timeout": (C.c_int, [_vp, C.c_int]),
+    "cfd_pcg_solve_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_double, C.c_int, _vp, _dp,
+                                        C.c_char_p, C.c_int]),
     "cfdh_load": (C.c_int, [C.POINTER(C.c_void_p), _cp, C.c_char_p, C.c_int]),
     "cfdh_free": (None, [_vp]),
     "cfdh_sizes": (C.c_int, [_vp, _llp]),
@@ -422,6 +424,19 @@ class Solver:
         nodes = np.ascontiguousarray(nodes, dtype=np.int32)
         uvw = np.ascontiguousarray(uvw, dtype=np.float64)
         self._check(self.L.cfd_set_bc_values(self.h, len(nodes), _p(nodes, C.c_int), _p(uvw, C.c_double)))
+
+
+NOALLOC_MAX_N = 524288
+
+
+def pcg_solve_noalloc(rowptr, col, val, dinv, b, x, n, rtol=1e-8, maxit=1000, stream=0):
+    """cfd_pcg_solve_noalloc on caller-owned device buffers (integer device
+    addresses).  Returns (status, info[3], message)."""
+    info = np.zeros(3)
+    err = C.create_string_buffer(256)
+    rc = lib().cfd_pcg_solve_noalloc(rowptr, col, val, dinv, b, x, n, rtol, maxit, stream or None,
+                                     _p(info, C.c_double), err, 256)
+    return rc, info, err.value.decode()
 
 
 def selectCUDAdevice(device: int = -1) -> Solver:

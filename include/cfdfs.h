@@ -224,6 +224,27 @@ int cfd_profile_read(cfd_ctx* ctx, double* out);
  * up as designed (the context stays usable), CFD_OK otherwise. */
 int cfd_selftest_wait_timeout(cfd_ctx* ctx, int timeout_ms);
 
+/* ---- pressure solve that allocates nothing ----------------------------------
+ * No counterpart in the reference.  For callers that must not allocate or
+ * free device memory while they solve (cudaFree synchronizes the whole
+ * device; some hosts reserve all device memory up front in their own pool).
+ * Jacobi-PCG (x0 = 0, stop at ||r||_2 <= rtol ||b||_2) on a CSR system whose
+ * arrays -- rowptr (n+1), col and val (nnz), dinv = 1/diag (n), b (n) and the
+ * output x (n) -- are DEVICE pointers owned by the caller, on the caller's
+ * stream (NULL = legacy default stream) and the current device.  Work
+ * vectors live in one static device array of fixed size (16.1 MiB, held by
+ * every GPU that loads the library until exit), so n is limited to
+ * CFD_NOALLOC_MAX_N; larger n returns CFD_E_BADARG with a message in errbuf.
+ * The first call on a device looks the array up (once per device); make it
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race and must not be issued.  info (may be NULL) receives
+ * {iterations, ||r||/||b||, status}; returns CFD_OK, CFD_E_NOCONV,
+ * CFD_E_NONFINITE, CFD_E_TIMEOUT, CFD_E_BADARG or CFD_E_CUDA. */
+#define CFD_NOALLOC_MAX_N 524288
+int cfd_pcg_solve_noalloc(const int* rowptr, const int* col, const double* val, const double* dinv,
+                          const double* b, double* x, int n, double rtol, int maxit, void* stream,
+                          double* info, char* errbuf, int errlen);
+
 /* ---- host-only preprocessing (no GPU needed) --------------------------------
  * The deck reader and mesh preprocessing of cfd_load_inp, exposed without a
  * device so callers can inspect the generated numbering and patterns. */
