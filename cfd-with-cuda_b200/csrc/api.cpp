@@ -79,8 +79,11 @@ struct cfd_ctx {
   DevBuf<int> k_rp, k_col, g_rp, g_col, gt_rp, gt_col, gt_pos, z_rp, z_col;
   // FP64 operators
   DevBuf<double> kval, g1, g2, g3, gt1, gt2, gt3, zval, zdiag, zdinv, msum, minv_orig, minv_free;
-  // FP32 operators (CFD_MIXED)
-  DevBuf<float> kval32, g1_32, g2_32, g3_32, gt1_32, gt2_32, gt3_32, zval32, zdinv32;
+  // SELL-32 copies used by the per-step kernels: layout, FP64 values and
+  // (CFD_MIXED) FP32 values
+  DevBuf<int> ks_off, ks_col, gs_off, gs_col, gts_off, gts_col, zs_off, zs_col;
+  DevBuf<double> ks_val, gs1, gs2, gs3, gts1, gts2, gts3, zs_val;
+  DevBuf<float> ks_val32, gs1_32, gs2_32, gs3_32, gts1_32, gts2_32, gts3_32, zs_val32, zdinv32;
   // velocity-sized state, double4 per node
   DevBuf<double4> vbuf[12];
   double4 *un = nullptr, *unp1 = nullptr, *unp1_prev = nullptr, *unphalf = nullptr, *unphalf_prev = nullptr,
@@ -237,6 +240,14 @@ int upload_problem(cfd_ctx* c) {
   CU(upload(c->gt_pos, P.gt_pos, s));
   CU(upload(c->z_rp, P.z_rp, s));
   CU(upload(c->z_col, P.z_col, s));
+  CU(upload(c->ks_off, P.k_soff, s));
+  CU(upload(c->ks_col, P.k_scol, s));
+  CU(upload(c->gs_off, P.g_soff, s));
+  CU(upload(c->gs_col, P.g_scol, s));
+  CU(upload(c->gts_off, P.gt_soff, s));
+  CU(upload(c->gts_col, P.gt_scol, s));
+  CU(upload(c->zs_off, P.z_soff, s));
+  CU(upload(c->zs_col, P.z_scol, s));
   std::vector<unsigned char> mask(P.NN, 0);
   std::vector<double> bcv(3 * P.bcnode.size());
   for (size_t i = 0; i < P.bcnode.size(); i++) {
@@ -253,12 +264,19 @@ int upload_problem(cfd_ctx* c) {
   CU(c->zval.alloc(nnzZ));
   for (auto* b : {&c->zdiag, &c->zdinv}) CU(b->alloc(NNp));
   for (auto* b : {&c->msum, &c->minv_orig, &c->minv_free}) CU(b->alloc(NN));
+  const size_t sK = P.k_scol.size(), sG = P.g_scol.size(), sGt = P.gt_scol.size(), sZ = P.z_scol.size();
+  CU(c->ks_val.alloc(sK));
+  for (auto* b : {&c->gs1, &c->gs2, &c->gs3}) CU(b->alloc(sG));
+  for (auto* b : {&c->gts1, &c->gts2, &c->gts3}) CU(b->alloc(sGt));
+  CU(c->zs_val.alloc(sZ));
   if (c->opt.precision == CFD_MIXED) {
-    CU(c->kval32.alloc(nnzK));
-    for (auto* b : {&c->g1_32, &c->g2_32, &c->g3_32, &c->gt1_32, &c->gt2_32, &c->gt3_32}) CU(b->alloc(nnzG));
-    CU(c->zval32.alloc(nnzZ));
+    CU(c->ks_val32.alloc(sK));
+    for (auto* b : {&c->gs1_32, &c->gs2_32, &c->gs3_32}) CU(b->alloc(sG));
+    for (auto* b : {&c->gts1_32, &c->gts2_32, &c->gts3_32}) CU(b->alloc(sGt));
+    CU(c->zs_val32.alloc(sZ));
     CU(c->zdinv32.alloc(NNp));
-    for (auto* b : {&c->f_b, &c->f_x, &c->f_r, &c->f_z, &c->f_p, &c->f_q}) CU(b->alloc(NNp));
+    for (auto* b : {&c->f_b, &c->f_x, &c->f_r, &c->f_z, &c->f_q}) CU(b->alloc(NNp));
+    CU(c->f_p.alloc(2 * NNp));
   }
   for (auto& b : c->vbuf) {
     CU(b.alloc(NN));
@@ -273,7 +291,8 @@ int upload_problem(cfd_ctx* c) {
   }
   c->pn = c->pbuf[0].p; c->pnp1 = c->pbuf[1].p; c->pnp1_prev = c->pbuf[2].p; c->pdot = c->pbuf[3].p;
   c->r2 = c->pbuf[4].p; c->pzero = c->pbuf[5].p;
-  for (auto* b : {&c->cg_r, &c->cg_z, &c->cg_p, &c->cg_q, &c->ir_r}) CU(b->alloc(NNp));
+  for (auto* b : {&c->cg_r, &c->cg_z, &c->cg_q, &c->ir_r}) CU(b->alloc(NNp));
+  CU(c->cg_p.alloc(2 * NNp));
   c->pcg_grid64 = pcg_max_grid<double>((int)NNp, c->device);
   c->pcg_grid32 = pcg_max_grid<float>((int)NNp, c->device);
   CU(c->cg_part.alloc(6 * (size_t)std::max(c->pcg_grid64, c->pcg_grid32)));
@@ -309,7 +328,7 @@ int run_pcg64(cfd_ctx* c, const double* b, double* x, int warm, double rtol, int
   CU(cudaMemsetAsync(c->cg_err.p, 0, sizeof(int), s));
   PcgArgs<double> a{};
   a.n = c->P.NNp;
-  a.rp = c->z_rp.p; a.col = c->z_col.p; a.val = c->zval.p; a.dinv = c->zdinv.p;
+  a.off = c->zs_off.p; a.col = c->zs_col.p; a.val = c->zs_val.p; a.dinv = c->zdinv.p;
   a.b = b; a.x = x; a.r = c->cg_r.p; a.z = c->cg_z.p; a.p = c->cg_p.p; a.q = c->cg_q.p;
   a.part = c->cg_part.p; a.bar = c->cg_bar.p; a.err = c->cg_err.p;
   a.rtol = rtol; a.maxit = maxit; a.warm = warm; a.result = c->cg_res.p;
@@ -328,7 +347,7 @@ int run_pcg32(cfd_ctx* c, double rtol, int maxit, double* res) {
   CU(cudaMemsetAsync(c->cg_err.p, 0, sizeof(int), s));
   PcgArgs<float> a{};
   a.n = c->P.NNp;
-  a.rp = c->z_rp.p; a.col = c->z_col.p; a.val = c->zval32.p; a.dinv = c->zdinv32.p;
+  a.off = c->zs_off.p; a.col = c->zs_col.p; a.val = c->zs_val32.p; a.dinv = c->zdinv32.p;
   a.b = c->f_b.p; a.x = c->f_x.p; a.r = c->f_r.p; a.z = c->f_z.p; a.p = c->f_p.p; a.q = c->f_q.p;
   a.part = c->cg_part.p; a.bar = c->cg_bar.p; a.err = c->cg_err.p;
   a.rtol = rtol; a.maxit = maxit; a.warm = 0; a.result = c->cg_res.p;
@@ -344,7 +363,7 @@ int run_pcg32(cfd_ctx* c, double rtol, int maxit, double* res) {
 // ||b - Z x||_2 in FP64 (also leaves r in ir_r and (float) r in f_b).
 int residual_norm(cfd_ctx* c, const double* b, const double* x, double* out) {
   cudaStream_t s = c->stream;
-  KL(CFD_K_RESID64, launch_residual64(c->P.NNp, c->z_rp.p, c->z_col.p, c->zval.p, b, x, c->ir_r.p, c->f_b.p,
+  KL(CFD_K_RESID64, launch_residual64(c->P.NNp, c->zs_off.p, c->zs_col.p, c->zs_val.p, b, x, c->ir_r.p, c->f_b.p,
                                       c->ir_part.p, c->res_blocks, s));
   KL(CFD_K_OTHER, launch_sum_partials(c->ir_part.p, c->res_blocks, c->ir_sum.p, s));
   CU(cudaMemcpyAsync(c->h_small, c->ir_sum.p, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -575,16 +594,24 @@ int cfd_step0(cfd_ctx* c) {
   z.minv_orig = c->minv_orig.p;
   CU(launch_build_z(z, s));
   CU(launch_recip(P.NNp, c->zdiag.p, c->zdinv.p, mixed(c) ? c->zdinv32.p : nullptr, s));
+  // SELL-32 copies of the assembled operators (FP64, and FP32 in CFD_MIXED)
+  CU(launch_csr_to_sell<double>(P.NN, c->k_rp.p, c->kval.p, c->ks_off.p, c->ks_val.p, s));
+  CU(launch_csr_to_sell<double>(P.NN, c->g_rp.p, c->g1.p, c->gs_off.p, c->gs1.p, s));
+  CU(launch_csr_to_sell<double>(P.NN, c->g_rp.p, c->g2.p, c->gs_off.p, c->gs2.p, s));
+  CU(launch_csr_to_sell<double>(P.NN, c->g_rp.p, c->g3.p, c->gs_off.p, c->gs3.p, s));
+  CU(launch_csr_to_sell<double>(P.NNp, c->gt_rp.p, c->gt1.p, c->gts_off.p, c->gts1.p, s));
+  CU(launch_csr_to_sell<double>(P.NNp, c->gt_rp.p, c->gt2.p, c->gts_off.p, c->gts2.p, s));
+  CU(launch_csr_to_sell<double>(P.NNp, c->gt_rp.p, c->gt3.p, c->gts_off.p, c->gts3.p, s));
+  CU(launch_csr_to_sell<double>(P.NNp, c->z_rp.p, c->zval.p, c->zs_off.p, c->zs_val.p, s));
   if (mixed(c)) {
-    CU(launch_to_float((long long)P.k_col.size(), c->kval.p, c->kval32.p, s));
-    const size_t ng = P.g_col.size();
-    CU(launch_to_float(ng, c->g1.p, c->g1_32.p, s));
-    CU(launch_to_float(ng, c->g2.p, c->g2_32.p, s));
-    CU(launch_to_float(ng, c->g3.p, c->g3_32.p, s));
-    CU(launch_to_float(ng, c->gt1.p, c->gt1_32.p, s));
-    CU(launch_to_float(ng, c->gt2.p, c->gt2_32.p, s));
-    CU(launch_to_float(ng, c->gt3.p, c->gt3_32.p, s));
-    CU(launch_to_float((long long)P.z_col.size(), c->zval.p, c->zval32.p, s));
+    CU(launch_csr_to_sell<float>(P.NN, c->k_rp.p, c->kval.p, c->ks_off.p, c->ks_val32.p, s));
+    CU(launch_csr_to_sell<float>(P.NN, c->g_rp.p, c->g1.p, c->gs_off.p, c->gs1_32.p, s));
+    CU(launch_csr_to_sell<float>(P.NN, c->g_rp.p, c->g2.p, c->gs_off.p, c->gs2_32.p, s));
+    CU(launch_csr_to_sell<float>(P.NN, c->g_rp.p, c->g3.p, c->gs_off.p, c->gs3_32.p, s));
+    CU(launch_csr_to_sell<float>(P.NNp, c->gt_rp.p, c->gt1.p, c->gts_off.p, c->gts1_32.p, s));
+    CU(launch_csr_to_sell<float>(P.NNp, c->gt_rp.p, c->gt2.p, c->gts_off.p, c->gts2_32.p, s));
+    CU(launch_csr_to_sell<float>(P.NNp, c->gt_rp.p, c->gt3.p, c->gts_off.p, c->gts3_32.p, s));
+    CU(launch_csr_to_sell<float>(P.NNp, c->z_rp.p, c->zval.p, c->zs_off.p, c->zs_val32.p, s));
   }
   CU(cudaStreamSynchronize(s));
   c->assembled = true;
@@ -625,7 +652,7 @@ int cfd_step1(cfd_ctx* c, int iter) {
   cudaStream_t s = c->stream;
   auto fill = [&](auto& a) {
     a.NN = c->P.NN; a.iter = iter; a.dt = c->P.dt;
-    a.k_rp = c->k_rp.p; a.k_col = c->k_col.p; a.g_rp = c->g_rp.p; a.g_col = c->g_col.p;
+    a.k_off = c->ks_off.p; a.k_col = c->ks_col.p; a.g_off = c->gs_off.p; a.g_col = c->gs_col.p;
     a.uprev = c->unphalf_prev; a.un = c->un; a.r1conv = c->r1conv; a.kacc = c->kacc;
     a.pn = c->pn; a.minv_free = c->minv_free.p; a.minv_orig = c->minv_orig.p;
     a.unphalf = c->unphalf; a.d = c->dvec; a.r1out = c->r_debug ? c->r1dbg : nullptr;
@@ -633,12 +660,12 @@ int cfd_step1(cfd_ctx* c, int iter) {
   if (mixed(c)) {
     Step1Args<float> a{};
     fill(a);
-    a.kval = c->kval32.p; a.g1 = c->g1_32.p; a.g2 = c->g2_32.p; a.g3 = c->g3_32.p;
+    a.kval = c->ks_val32.p; a.g1 = c->gs1_32.p; a.g2 = c->gs2_32.p; a.g3 = c->gs3_32.p;
     KL(CFD_K_STEP1, launch_step1<float>(a, c->num_sms, s));
   } else {
     Step1Args<double> a{};
     fill(a);
-    a.kval = c->kval.p; a.g1 = c->g1.p; a.g2 = c->g2.p; a.g3 = c->g3.p;
+    a.kval = c->ks_val.p; a.g1 = c->gs1.p; a.g2 = c->gs2.p; a.g3 = c->gs3.p;
     KL(CFD_K_STEP1, launch_step1<double>(a, c->num_sms, s));
   }
   return CFD_OK;
@@ -650,10 +677,10 @@ int cfd_step2(cfd_ctx* c, int iter, cfd_solve_stats* st) {
   cudaStream_t s = c->stream;
   const int pin = c->P.zeroP;
   if (mixed(c)) {
-    GtArgs<float> a{c->P.NNp, pin, c->gt_rp.p, c->gt_col.p, c->gt1_32.p, c->gt2_32.p, c->gt3_32.p, c->dvec, c->r2};
+    GtArgs<float> a{c->P.NNp, pin, c->gts_off.p, c->gts_col.p, c->gts1_32.p, c->gts2_32.p, c->gts3_32.p, c->dvec, c->r2};
     KL(CFD_K_GT, launch_gt<float>(a, c->num_sms, s));
   } else {
-    GtArgs<double> a{c->P.NNp, pin, c->gt_rp.p, c->gt_col.p, c->gt1.p, c->gt2.p, c->gt3.p, c->dvec, c->r2};
+    GtArgs<double> a{c->P.NNp, pin, c->gts_off.p, c->gts_col.p, c->gts1.p, c->gts2.p, c->gts3.p, c->dvec, c->r2};
     KL(CFD_K_GT, launch_gt<double>(a, c->num_sms, s));
   }
   int rc = pressure_solve(c, c->r2, c->pdot, c->opt.cg_warm, st);
@@ -668,19 +695,19 @@ int cfd_step3(cfd_ctx* c, int iter) {
   cudaStream_t s = c->stream;
   auto fill = [&](auto& a) {
     a.NN = c->P.NN; a.iter = iter; a.dt = c->P.dt;
-    a.g_rp = c->g_rp.p; a.g_col = c->g_col.p; a.pdot = c->pdot; a.kacc = c->kacc; a.unphalf = c->unphalf;
+    a.g_off = c->gs_off.p; a.g_col = c->gs_col.p; a.pdot = c->pdot; a.kacc = c->kacc; a.unphalf = c->unphalf;
     a.un = c->un; a.unp1_prev = c->unp1_prev; a.minv_free = c->minv_free.p; a.acc = c->acc; a.unp1 = c->unp1;
     a.r3out = c->r_debug ? c->r3dbg : nullptr; a.part = c->upart.p; a.nblocks = c->nub;
   };
   if (mixed(c)) {
     Step3Args<float> a{};
     fill(a);
-    a.g1 = c->g1_32.p; a.g2 = c->g2_32.p; a.g3 = c->g3_32.p;
+    a.g1 = c->gs1_32.p; a.g2 = c->gs2_32.p; a.g3 = c->gs3_32.p;
     KL(CFD_K_STEP3, launch_step3<float>(a, s));
   } else {
     Step3Args<double> a{};
     fill(a);
-    a.g1 = c->g1.p; a.g2 = c->g2.p; a.g3 = c->g3.p;
+    a.g1 = c->gs1.p; a.g2 = c->gs2.p; a.g3 = c->gs3.p;
     KL(CFD_K_STEP3, launch_step3<double>(a, s));
   }
   return CFD_OK;
@@ -715,10 +742,10 @@ int cfd_k_times_acc(cfd_ctx* c) {
   NEED(c->assembled, "cfd_k_times_acc before cfd_step0");
   cudaStream_t s = c->stream;
   if (mixed(c)) {
-    SpmvK3Args<float> a{c->P.NN, c->k_rp.p, c->k_col.p, c->kval32.p, c->acc_prev, c->kacc};
+    SpmvK3Args<float> a{c->P.NN, c->ks_off.p, c->ks_col.p, c->ks_val32.p, c->acc_prev, c->kacc};
     KL(CFD_K_SPMV_K3, launch_spmv_k3<float>(a, c->num_sms, s));
   } else {
-    SpmvK3Args<double> a{c->P.NN, c->k_rp.p, c->k_col.p, c->kval.p, c->acc_prev, c->kacc};
+    SpmvK3Args<double> a{c->P.NN, c->ks_off.p, c->ks_col.p, c->ks_val.p, c->acc_prev, c->kacc};
     KL(CFD_K_SPMV_K3, launch_spmv_k3<double>(a, c->num_sms, s));
   }
   return CFD_OK;
@@ -858,7 +885,7 @@ int cfd_download_vector(cfd_ctx* c, int which, double* out) {
     }
     case CFD_V_DIV: {
       NEED(c->assembled, "operators not assembled");
-      GtArgs<double> a{(int)NNp, 0, c->gt_rp.p, c->gt_col.p, c->gt1.p, c->gt2.p, c->gt3.p, c->unp1, c->ir_r.p};
+      GtArgs<double> a{(int)NNp, 0, c->gts_off.p, c->gts_col.p, c->gts1.p, c->gts2.p, c->gts3.p, c->unp1, c->ir_r.p};
       CU(launch_gt<double>(a, c->num_sms, s));
       p1 = c->ir_r.p;
       break;

@@ -4,10 +4,14 @@
 //   velocity-sized vectors  double4 per node (x, y, z, pad = 0): one aligned
 //                           32-byte sector per gathered node
 //   pressure-sized vectors  double (or float for the FP32 inner solve)
-//   K (NN x NN)             CSR: int32 rowptr/col + FP64 (and FP32) values
-//   G (NN x NNp)            CSR: int32 rowptr/col + three value arrays G1..G3
-//   G^T (NNp x NN)          CSR of the transpose (gather form, no atomics)
-//   Z (NNp x NNp)           CSR: int32 rowptr/col + values
+//   K, G, G^T, Z            CSR (int32 rowptr/col, FP64 values) for assembly
+//                           and download, plus a SELL-32 copy used by every
+//                           per-step kernel: rows in slices of 32, each slice
+//                           padded to its longest row and stored column-major
+//                           (entry j of row r at off[r/32] + 32 j + r%32), so
+//                           one thread owns one row and a warp-wide load of
+//                           entry j is one contiguous 128/256-byte segment.
+//                           Padding entries hold value 0 and a valid column.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -68,9 +72,9 @@ template <class VT>
 struct Step1Args {
   int NN, iter;
   double dt;
-  const int *k_rp, *k_col;
+  const int *k_off, *k_col;  // SELL-32
   const VT* kval;
-  const int *g_rp, *g_col;
+  const int *g_off, *g_col;  // SELL-32
   const VT *g1, *g2, *g3;
   const double4 *uprev, *un, *r1conv, *kacc;
   const double *pn, *minv_free, *minv_orig;
@@ -82,7 +86,7 @@ cudaError_t launch_step1(const Step1Args<VT>& a, int num_sms, cudaStream_t s);
 template <class VT>
 struct GtArgs {
   int NNp, pin;  // pin: row forced to 0 (< 1 disables, as the reference's node > 0 test)
-  const int *gt_rp, *gt_col;
+  const int *gt_off, *gt_col;  // SELL-32
   const VT *gt1, *gt2, *gt3;
   const double4* d;
   double* out;
@@ -94,7 +98,7 @@ template <class VT>
 struct Step3Args {
   int NN, iter;
   double dt;
-  const int *g_rp, *g_col;
+  const int *g_off, *g_col;  // SELL-32
   const VT *g1, *g2, *g3;
   const double* pdot;
   const double4 *kacc, *unphalf, *un, *unp1_prev;
@@ -110,7 +114,7 @@ int step3_blocks(int NN, int num_sms);
 template <class VT>
 struct SpmvK3Args {
   int NN;
-  const int *rp, *col;
+  const int *off, *col;  // SELL-32
   const VT* val;
   const double4* x;
   double4* y;
@@ -132,11 +136,11 @@ cudaError_t launch_reduce_norms(const double* upart, int nub, const double* ppar
 template <class VT>
 struct PcgArgs {
   int n;
-  const int *rp, *col;
+  const int *off, *col;  // SELL-32
   const VT* val;
   const VT* dinv;
   const VT* b;
-  VT *x, *r, *z, *p, *q;
+  VT *x, *r, *z, *p, *q;  // p holds two n-vectors (double-buffered search direction)
   double* part;  // 2 x 3 x grid doubles
   unsigned* bar; // 2 unsigned (host-zeroed)
   int* err;      // host-zeroed
@@ -150,13 +154,17 @@ cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s);
 template <class VT>
 int pcg_max_grid(int n, int device);
 
-// r = b - Z x (FP64) and the partial sum of r^2 per block; rf = (float) r.
-cudaError_t launch_residual64(int n, const int* rp, const int* col, const double* val, const double* b,
+// r = b - Z x (FP64, SELL-32 Z) and the partial sum of r^2 per block; rf = (float) r.
+cudaError_t launch_residual64(int n, const int* off, const int* col, const double* val, const double* b,
                               const double* x, double* r, float* rf, double* part, int nblocks,
                               cudaStream_t s);
 int residual_blocks(int n, int num_sms);
 cudaError_t launch_axpy_f2d(int n, const float* e, double* x, cudaStream_t s);
 cudaError_t launch_sum_partials(const double* part, int n, double* out, cudaStream_t s);
+
+// CSR values -> SELL-32 values (padding entries set to 0).
+template <class T>
+cudaError_t launch_csr_to_sell(int nrows, const int* rp, const double* csr, const int* off, T* sell, cudaStream_t s);
 
 cudaError_t launch_wait_selftest(const int* flag, int* err, unsigned long long timeout_ns, cudaStream_t s);
 

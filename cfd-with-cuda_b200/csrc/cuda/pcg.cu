@@ -3,15 +3,20 @@
 // precond::diagonal, CUDAcodes.cu:418-451, and MKL dcg, blascoCodinaHuerta.cpp:
 // 3981-4055).
 //
-// Each warp owns a contiguous block of rows.  Per iteration:
-//   A: q = Z p on own rows (one warp per row), partial p.q      -> grid reduce
-//   B: x += a p, r -= a q, z = Dinv r, partial r.r and r.z      -> grid reduce
-//   C: p = z + b p on own rows                                  -> grid barrier
-// Grid reductions write per-block partials, pass a bounded grid barrier, and
-// every block sums all partials in the same fixed order (FP64), so all blocks
-// take identical decisions and results do not depend on timing.  Stopping
-// rule: ||r||_2 <= rtol ||b||_2 on the recursively updated residual, checked
-// after each update, exactly as the CPU oracle.
+// Z is stored SELL-32; thread g owns rows g, g+T, g+2T, ... (T = all
+// threads, a multiple of 32, so a warp always owns whole slices).  The
+// search-direction update p = z + beta p is folded into the next SpMV, which
+// evaluates q = Z (z + beta p_old) from gathers of z and p_old and writes
+// p_new for its own rows into the other half of a double buffer.  That leaves
+// two grid-wide reductions per iteration:
+//   A: p_new = z + beta p_old, q = Z p_new (own rows), partial p_new.q  -> reduce
+//   B: x += alpha p_new, r -= alpha q, z = Dinv r, partial r.r, r.z     -> reduce
+// Each reduction writes per-block partials, passes a bounded grid barrier,
+// and every block sums all partials in the same fixed order (FP64), so every
+// block takes the same decisions.  Vectors written inside the kernel are
+// gathered with L2 loads (ld.cg); the matrix is streamed (ld.cs) so the
+// vectors stay resident in L2.  Stopping rule: ||r||_2 <= rtol ||b||_2 on the
+// recursively updated residual, checked after each update (as the oracle).
 #include <algorithm>
 
 #include "kernels.h"
@@ -51,38 +56,38 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* part, int p
 }
 
 template <class VT>
-__global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs<VT> a) {
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  const long long gw = (long long)blockIdx.x * wpb + wib, nw = (long long)gridDim.x * wpb;
+__global__ void __launch_bounds__(kPcgThreads, 5) k_pcg(PcgArgs<VT> a) {
+  const int T = gridDim.x * blockDim.x;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n;
-  const int r0 = (int)(n * gw / nw), r1 = (int)(n * (gw + 1) / nw);
+  VT* P0 = a.p;
+  VT* P1 = a.p + n;
   int phase = 0;
-  bool alive = true;
 
   // ---- initial residual ----
-  if (a.warm) {
-    for (int i = r0; i < r1; i++) {
-      double s = 0;
-      for (int j = a.rp[i] + lane; j < a.rp[i + 1]; j += 32) s += (double)a.val[j] * (double)a.x[a.col[j]];
-      s = warp_sum(s);
-      if (lane == 0) a.q[i] = (VT)s;
-    }
-    __syncwarp();
-  }
   double v3[3] = {0, 0, 0};
-  for (int i = r0 + lane; i < r1; i += 32) {
-    double bi = (double)a.b[i];
-    double ri = a.warm ? bi - (double)a.q[i] : bi;
-    if (!a.warm) a.x[i] = (VT)0;
-    double zi = ri * (double)a.dinv[i];
-    a.r[i] = (VT)ri;
-    a.z[i] = (VT)zi;
-    a.p[i] = (VT)zi;
+  for (int i = g; i < n; i += T) {
+    const double bi = (double)a.b[i];
+    double ri = bi;
+    if (a.warm) {
+      const int s = i >> 5, l = i & 31;
+      const int b = __ldg(a.off + s) + l, w = (__ldg(a.off + s + 1) - __ldg(a.off + s)) >> 5;
+      VT q = 0;
+      for (int j = 0; j < w; j++) q += __ldcs(a.val + b + 32 * j) * a.x[__ldcs(a.col + b + 32 * j)];
+      ri = bi - (double)q;
+    } else {
+      a.x[i] = (VT)0;
+    }
+    const VT rv = (VT)ri;
+    const VT zv = (VT)((double)rv * (double)a.dinv[i]);
+    a.r[i] = rv;
+    a.z[i] = zv;
+    P0[i] = (VT)0;
     v3[0] += bi * bi;
-    v3[1] += ri * (double)(VT)zi;
-    v3[2] += ri * ri;
+    v3[1] += (double)rv * (double)zv;
+    v3[2] += (double)rv * (double)rv;
   }
-  alive = grid_reduce<3>(v3, a.part, phase++, a.bar, a.err, a.timeout_ns);
+  const bool alive = grid_reduce<3>(v3, a.part, phase++, a.bar, a.err, a.timeout_ns);
   const double bnorm = sqrt(v3[0]);
   double rz = v3[1];
   double rn = sqrt(v3[2]);
@@ -93,36 +98,43 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs<VT> a) {
   } else if (!isfinite(bnorm) || !isfinite(rn)) {
     status = 2;
   } else if (bnorm == 0.0) {
-    for (int i = r0 + lane; i < r1; i += 32) a.x[i] = (VT)0;
+    for (int i = g; i < n; i += T) a.x[i] = (VT)0;
     status = 0;
     rn = 0;
   } else if (rn <= tol) {
     status = 0;
   } else {
+    VT beta = 0;
+    VT* pold = P0;
+    VT* pnew = P1;
     while (its < a.maxit) {
-      // A: q = Z p
+      // A: p_new = z + beta p_old;  q = Z p_new
       double pq = 0;
-      for (int i = r0; i < r1; i++) {
-        VT s = 0;
-        const int b = __ldg(a.rp + i), e = __ldg(a.rp + i + 1);
-        for (int j = b + lane; j < e; j += 32) s += __ldg(a.val + j) * __ldcg(a.p + __ldg(a.col + j));
-        s = warp_sum(s);
-        if (lane == 0) {
-          a.q[i] = s;
-          pq += (double)a.p[i] * (double)s;
+      for (int i = g; i < n; i += T) {
+        const int s = i >> 5, l = i & 31;
+        const int b = __ldg(a.off + s) + l, w = (__ldg(a.off + s + 1) - __ldg(a.off + s)) >> 5;
+        VT q = 0;
+#pragma unroll 4
+        for (int j = 0; j < w; j++) {
+          const int c = __ldcs(a.col + b + 32 * j);
+          const VT pc = __ldcg(a.z + c) + beta * __ldcg(pold + c);
+          q += __ldcs(a.val + b + 32 * j) * pc;
         }
+        const VT pi = a.z[i] + beta * pold[i];
+        pnew[i] = pi;
+        a.q[i] = q;
+        pq += (double)pi * (double)q;
       }
       double v1[1] = {pq};
       if (!grid_reduce<1>(v1, a.part, phase++, a.bar, a.err, a.timeout_ns)) { status = 3; break; }
       const double alpha = rz / v1[0];
-      // B: updates
+      // B: updates on own rows
       double v2[2] = {0, 0};
-      for (int i = r0 + lane; i < r1; i += 32) {
-        double pi = (double)a.p[i], qi = (double)__ldcg(a.q + i);
+      for (int i = g; i < n; i += T) {
+        const double pi = (double)pnew[i], qi = (double)a.q[i];
         a.x[i] = (VT)((double)a.x[i] + alpha * pi);
-        double ri = (double)a.r[i] - alpha * qi;
-        VT rv = (VT)ri;
-        VT zv = (VT)((double)rv * (double)a.dinv[i]);
+        const VT rv = (VT)((double)a.r[i] - alpha * qi);
+        const VT zv = (VT)((double)rv * (double)a.dinv[i]);
         a.r[i] = rv;
         a.z[i] = zv;
         v2[0] += (double)rv * (double)rv;
@@ -133,11 +145,11 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs<VT> a) {
       rn = sqrt(v2[0]);
       if (!isfinite(rn)) { status = 2; break; }
       if (rn <= tol) { status = 0; break; }
-      const double beta = v2[1] / rz;
+      beta = (VT)(v2[1] / rz);
       rz = v2[1];
-      // C: p = z + beta p
-      for (int i = r0 + lane; i < r1; i += 32) a.p[i] = (VT)((double)a.z[i] + beta * (double)a.p[i]);
-      if (!grid_barrier(a.bar, a.err, a.timeout_ns)) { status = 3; break; }
+      VT* t = pold;
+      pold = pnew;
+      pnew = t;
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -150,27 +162,25 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg(PcgArgs<VT> a) {
 
 constexpr int kResThreads = 256;
 
-// r = b - Z x in FP64, rf = (float) r, per-block partial of r^2.
-__global__ void __launch_bounds__(kResThreads) k_residual64(int n, const int* __restrict__ rp,
+// r = b - Z x in FP64 (SELL-32 Z), rf = (float) r, per-block partial of r^2.
+__global__ void __launch_bounds__(kResThreads) k_residual64(int n, const int* __restrict__ off,
                                                              const int* __restrict__ col,
                                                              const double* __restrict__ val,
                                                              const double* __restrict__ b,
                                                              const double* __restrict__ x, double* r, float* rf,
                                                              double* part) {
-  const int lane = threadIdx.x & 31;
-  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0};
-  for (long long i = gw; i < n; i += nw) {
-    double s = 0;
-    for (int j = rp[i] + lane; j < rp[i + 1]; j += 32) s += __ldg(val + j) * __ldg(x + __ldg(col + j));
-    s = warp_sum(s);
-    if (lane == 0) {
-      double ri = b[i] - s;
-      r[i] = ri;
-      if (rf) rf[i] = (float)ri;
-      acc[0] += ri * ri;
-    }
+  if (i < n) {
+    const int s = i >> 5, l = i & 31;
+    const int bb = __ldg(off + s) + l, w = (__ldg(off + s + 1) - __ldg(off + s)) >> 5;
+    double q = 0;
+#pragma unroll 4
+    for (int j = 0; j < w; j++) q += __ldcs(val + bb + 32 * j) * __ldg(x + __ldcs(col + bb + 32 * j));
+    const double ri = b[i] - q;
+    r[i] = ri;
+    if (rf) rf[i] = (float)ri;
+    acc[0] = ri * ri;
   }
   block_sum<1>(acc);
   if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
@@ -214,8 +224,7 @@ int pcg_max_grid(int n, int device) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<VT>, kPcgThreads, 0);
   long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
-  // about 8 rows per warp at least, so that small systems use few blocks
-  long long want = ((long long)n + (kPcgThreads / 32) * 8 - 1) / ((kPcgThreads / 32) * 8);
+  long long want = ((long long)n + kPcgThreads - 1) / kPcgThreads;  // one row per thread at most
   if (want < 1) want = 1;
   return (int)std::min(cap, want);
 }
@@ -227,14 +236,11 @@ cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s) {
   return cudaLaunchCooperativeKernel((const void*)k_pcg<VT>, dim3(grid), dim3(kPcgThreads), params, 0, s);
 }
 
-int residual_blocks(int n, int num_sms) {
-  long long g = ((long long)n + (kResThreads / 32) - 1) / (kResThreads / 32);
-  return (int)std::max(1LL, std::min(g, (long long)num_sms * 8));
-}
+int residual_blocks(int n, int) { return std::max(1, (n + kResThreads - 1) / kResThreads); }
 
-cudaError_t launch_residual64(int n, const int* rp, const int* col, const double* val, const double* b,
+cudaError_t launch_residual64(int n, const int* off, const int* col, const double* val, const double* b,
                               const double* x, double* r, float* rf, double* part, int nblocks, cudaStream_t s) {
-  k_residual64<<<nblocks, kResThreads, 0, s>>>(n, rp, col, val, b, x, r, rf, part);
+  k_residual64<<<nblocks, kResThreads, 0, s>>>(n, off, col, val, b, x, r, rf, part);
   return cudaGetLastError();
 }
 

@@ -1,12 +1,16 @@
 // Fractional-step stage kernels (step1GPUpart, step2GPU, step3GPU,
 // calculate_KtimesAcc_prevGPU and the convergence norms of CUDAcodes.cu:
-// 946-1121).  Each stage is one CSR pass with its elementwise work fused
-// into the epilogue, replacing the reference's 3-6 library SpMVs plus 2-4
-// elementwise kernels and temporary cudaMalloc/cudaFree per call.
+// 946-1121).  Each stage is one pass over its SELL-32 operator(s) with the
+// elementwise work fused into the epilogue, replacing the reference's 3-6
+// library SpMVs plus 2-4 elementwise kernels and the temporary
+// cudaMalloc/cudaFree of every call.
 //
-// Row kernels use LPR lanes per row (LPR | 32); loops run over warp-uniform
-// row bases so every lane reaches every shuffle.  Matrix values are VT
-// (double or float, accumulated in VT); vectors stay FP64.
+// One thread owns one row; a warp owns one 32-row slice, so the entry loop
+// has a warp-uniform trip count, needs no shuffles, and every load of the
+// matrix is a contiguous warp-wide segment.  Matrix values and columns are
+// read with streaming (evict-first) loads so the gathered vectors stay in
+// L2.  Matrix values are VT (double or float, accumulated in VT); vectors
+// stay FP64.
 #include "kernels.h"
 
 namespace cfd {
@@ -15,13 +19,9 @@ namespace {
 
 constexpr int kRowThreads = 256;
 
-inline int row_grid(long long rows, int lpr, int num_sms) {
-  long long rows_per_block = kRowThreads / lpr;
-  long long g = (rows + rows_per_block - 1) / rows_per_block;
-  long long cap = (long long)num_sms * 16;
-  if (g > cap) g = cap;
-  if (g < 1) g = 1;
-  return (int)g;
+inline int rows_grid(long long rows) {
+  long long g = (rows + kRowThreads - 1) / kRowThreads;
+  return (int)(g < 1 ? 1 : g);
 }
 
 // step1: R1 = R1conv - K UnpHalf_prev - G Pn (blascoCodinaHuerta.cpp:
@@ -29,143 +29,126 @@ inline int row_grid(long long rows, int lpr, int num_sms) {
 // UnpHalf = Un + dt R1 MdInv (:3781-3783) -- the Dirichlet zeroing is the
 // zero in minv_free.  Also writes d = UnpHalf/dt^2 - [iter>1] MdOrigInv KAcc,
 // the input of step2 (blascoCodinaHuerta.cpp:3821-3832).
-template <class VT, int LPR>
+template <class VT>
 __global__ void __launch_bounds__(kRowThreads) k_step1(Step1Args<VT> a) {
-  constexpr int RPW = 32 / LPR;
-  const int lane = threadIdx.x & 31, sub = lane % LPR;
-  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= a.NN) return;
+  const int s = row >> 5, l = row & 31;
   const double inv_dt2 = 1.0000000000000000 / (a.dt * a.dt);
-  for (long long base = gw * RPW; base < a.NN; base += nw * RPW) {
-    const long long row = base + lane / LPR;
-    const bool ok = row < a.NN;
-    VT kx = 0, ky = 0, kz = 0, gx = 0, gy = 0, gz = 0;
-    if (ok) {
-      const int kb = __ldg(a.k_rp + row), ke = __ldg(a.k_rp + row + 1);
-      for (int j = kb + sub; j < ke; j += LPR) {
-        VT v = __ldg(a.kval + j);
-        double4 x = ldg4(a.uprev + __ldg(a.k_col + j));
-        kx += v * (VT)x.x;
-        ky += v * (VT)x.y;
-        kz += v * (VT)x.z;
-      }
-      const int gb = __ldg(a.g_rp + row), ge = __ldg(a.g_rp + row + 1);
-      for (int j = gb + sub; j < ge; j += LPR) {
-        VT p = (VT)__ldg(a.pn + __ldg(a.g_col + j));
-        gx += __ldg(a.g1 + j) * p;
-        gy += __ldg(a.g2 + j) * p;
-        gz += __ldg(a.g3 + j) * p;
-      }
-    }
-    kx = group_sum<LPR>(kx); ky = group_sum<LPR>(ky); kz = group_sum<LPR>(kz);
-    gx = group_sum<LPR>(gx); gy = group_sum<LPR>(gy); gz = group_sum<LPR>(gz);
-    if (ok && sub == 0) {
-      const double4 rc = a.r1conv[row];
-      const double mf = a.minv_free[row];
-      double rx = (rc.x - (double)kx) - (double)gx;
-      double ry = (rc.y - (double)ky) - (double)gy;
-      double rz = (rc.z - (double)kz) - (double)gz;
-      if (mf == 0.0) rx = ry = rz = 0.0;  // Dirichlet node
-      const double4 u = a.un[row];
-      double4 h;
-      h.x = u.x + a.dt * rx * mf;
-      h.y = u.y + a.dt * ry * mf;
-      h.z = u.z + a.dt * rz * mf;
-      h.w = 0.0;
-      a.unphalf[row] = h;
-      double4 d;
-      d.x = inv_dt2 * h.x;
-      d.y = inv_dt2 * h.y;
-      d.z = inv_dt2 * h.z;
-      d.w = 0.0;
-      if (a.iter != 1) {
-        const double mo = a.minv_orig[row];
-        const double4 ka = a.kacc[row];
-        d.x = d.x - mo * ka.x;
-        d.y = d.y - mo * ka.y;
-        d.z = d.z - mo * ka.z;
-      }
-      a.d[row] = d;
-      if (a.r1out) a.r1out[row] = make_double4(rx, ry, rz, 0.0);
+  VT kx = 0, ky = 0, kz = 0, gx = 0, gy = 0, gz = 0;
+  {
+    const int b = __ldg(a.k_off + s), w = (__ldg(a.k_off + s + 1) - b) >> 5;
+    const int* col = a.k_col + b + l;
+    const VT* val = a.kval + b + l;
+#pragma unroll 4
+    for (int j = 0; j < w; j++) {
+      const VT v = __ldcs(val + 32 * j);
+      const double4 x = ldg4(a.uprev + __ldcs(col + 32 * j));
+      kx += v * (VT)x.x;
+      ky += v * (VT)x.y;
+      kz += v * (VT)x.z;
     }
   }
+  {
+    const int b = __ldg(a.g_off + s), w = (__ldg(a.g_off + s + 1) - b) >> 5;
+    const int* col = a.g_col + b + l;
+#pragma unroll 4
+    for (int j = 0; j < w; j++) {
+      const VT p = (VT)__ldg(a.pn + __ldcs(col + 32 * j));
+      gx += __ldcs(a.g1 + b + l + 32 * j) * p;
+      gy += __ldcs(a.g2 + b + l + 32 * j) * p;
+      gz += __ldcs(a.g3 + b + l + 32 * j) * p;
+    }
+  }
+  const double4 rc = a.r1conv[row];
+  const double mf = a.minv_free[row];
+  double rx = (rc.x - (double)kx) - (double)gx;
+  double ry = (rc.y - (double)ky) - (double)gy;
+  double rz = (rc.z - (double)kz) - (double)gz;
+  if (mf == 0.0) rx = ry = rz = 0.0;  // Dirichlet node
+  const double4 u = a.un[row];
+  double4 h;
+  h.x = u.x + a.dt * rx * mf;
+  h.y = u.y + a.dt * ry * mf;
+  h.z = u.z + a.dt * rz * mf;
+  h.w = 0.0;
+  a.unphalf[row] = h;
+  double4 d;
+  d.x = inv_dt2 * h.x;
+  d.y = inv_dt2 * h.y;
+  d.z = inv_dt2 * h.z;
+  d.w = 0.0;
+  if (a.iter != 1) {
+    const double mo = a.minv_orig[row];
+    const double4 ka = a.kacc[row];
+    d.x = d.x - mo * ka.x;
+    d.y = d.y - mo * ka.y;
+    d.z = d.z - mo * ka.z;
+  }
+  a.d[row] = d;
+  if (a.r1out) a.r1out[row] = make_double4(rx, ry, rz, 0.0);
 }
 
 // out[p] = sum_d (G_d^T d_d)[p]; out[pin] = 0 when pin > 0
 // (step2GPU's three transposed csrmv calls + applyPresBC, CUDAcodes.cu:1006-1011).
-template <class VT, int LPR>
+template <class VT>
 __global__ void __launch_bounds__(kRowThreads) k_gt(GtArgs<VT> a) {
-  constexpr int RPW = 32 / LPR;
-  const int lane = threadIdx.x & 31, sub = lane % LPR;
-  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long base = gw * RPW; base < a.NNp; base += nw * RPW) {
-    const long long row = base + lane / LPR;
-    const bool ok = row < a.NNp;
-    VT s = 0;
-    if (ok) {
-      const int b = __ldg(a.gt_rp + row), e = __ldg(a.gt_rp + row + 1);
-      for (int j = b + sub; j < e; j += LPR) {
-        double4 d = ldg4(a.d + __ldg(a.gt_col + j));
-        s += __ldg(a.gt1 + j) * (VT)d.x + __ldg(a.gt2 + j) * (VT)d.y + __ldg(a.gt3 + j) * (VT)d.z;
-      }
-    }
-    s = group_sum<LPR>(s);
-    if (ok && sub == 0) a.out[row] = (a.pin > 0 && row == a.pin) ? 0.0 : (double)s;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= a.NNp) return;
+  const int s = row >> 5, l = row & 31;
+  const int b = __ldg(a.gt_off + s) + l, w = (__ldg(a.gt_off + s + 1) - __ldg(a.gt_off + s)) >> 5;
+  VT acc = 0;
+#pragma unroll 4
+  for (int j = 0; j < w; j++) {
+    const int e = b + 32 * j;
+    const double4 d = ldg4(a.d + __ldcs(a.gt_col + e));
+    acc += __ldcs(a.gt1 + e) * (VT)d.x + __ldcs(a.gt2 + e) * (VT)d.y + __ldcs(a.gt3 + e) * (VT)d.z;
   }
+  a.out[row] = (a.pin > 0 && row == a.pin) ? 0.0 : (double)acc;
 }
 
 // step3: R3 = -dt G Pdot - [iter>1] dt KAcc, R3 = 0 at Dirichlet nodes,
 // Acc = R3 MdInv, Unp1 = UnpHalf + dt Acc (blascoCodinaHuerta.cpp:3920-3967)
 // plus the partial sums of the convergence test (:2936-2961) and of the
 // steady-state test (:3052-3057).
-template <class VT, int LPR>
+template <class VT>
 __global__ void __launch_bounds__(kRowThreads) k_step3(Step3Args<VT> a) {
-  constexpr int RPW = 32 / LPR;
-  const int lane = threadIdx.x & 31, sub = lane % LPR;
-  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   const double inv_dt = 1.0000000000000000 / a.dt;
   double s_u2 = 0, s_du2 = 0, m_acc = 0;
-  for (long long base = gw * RPW; base < a.NN; base += nw * RPW) {
-    const long long row = base + lane / LPR;
-    const bool ok = row < a.NN;
+  if (row < a.NN) {
+    const int s = row >> 5, l = row & 31;
+    const int b = __ldg(a.g_off + s) + l, w = (__ldg(a.g_off + s + 1) - __ldg(a.g_off + s)) >> 5;
     VT gx = 0, gy = 0, gz = 0;
-    if (ok) {
-      const int gb = __ldg(a.g_rp + row), ge = __ldg(a.g_rp + row + 1);
-      for (int j = gb + sub; j < ge; j += LPR) {
-        VT p = (VT)__ldg(a.pdot + __ldg(a.g_col + j));
-        gx += __ldg(a.g1 + j) * p;
-        gy += __ldg(a.g2 + j) * p;
-        gz += __ldg(a.g3 + j) * p;
-      }
+#pragma unroll 4
+    for (int j = 0; j < w; j++) {
+      const int e = b + 32 * j;
+      const VT p = (VT)__ldg(a.pdot + __ldcs(a.g_col + e));
+      gx += __ldcs(a.g1 + e) * p;
+      gy += __ldcs(a.g2 + e) * p;
+      gz += __ldcs(a.g3 + e) * p;
     }
-    gx = group_sum<LPR>(gx); gy = group_sum<LPR>(gy); gz = group_sum<LPR>(gz);
-    if (ok && sub == 0) {
-      double rx = -a.dt * (double)gx, ry = -a.dt * (double)gy, rz = -a.dt * (double)gz;
-      if (a.iter != 1) {
-        const double4 ka = a.kacc[row];
-        rx = rx - a.dt * ka.x;
-        ry = ry - a.dt * ka.y;
-        rz = rz - a.dt * ka.z;
-      }
-      const double mf = a.minv_free[row];
-      if (mf == 0.0) rx = ry = rz = 0.0;  // Dirichlet node
-      double4 acc = make_double4(rx * mf, ry * mf, rz * mf, 0.0);
-      const double4 h = a.unphalf[row];
-      double4 u1 = make_double4(h.x + a.dt * acc.x, h.y + a.dt * acc.y, h.z + a.dt * acc.z, 0.0);
-      a.acc[row] = acc;
-      a.unp1[row] = u1;
-      if (a.r3out) a.r3out[row] = make_double4(rx, ry, rz, 0.0);
-      const double4 pv = a.unp1_prev[row];
-      const double4 un = a.un[row];
-      s_u2 += u1.x * u1.x + u1.y * u1.y + u1.z * u1.z;
-      double dx = u1.x - pv.x, dy = u1.y - pv.y, dz = u1.z - pv.z;
-      s_du2 += dx * dx + dy * dy + dz * dz;
-      m_acc = fmax(m_acc, fabs((u1.x - un.x) * inv_dt));
-      m_acc = fmax(m_acc, fabs((u1.y - un.y) * inv_dt));
-      m_acc = fmax(m_acc, fabs((u1.z - un.z) * inv_dt));
+    double rx = -a.dt * (double)gx, ry = -a.dt * (double)gy, rz = -a.dt * (double)gz;
+    if (a.iter != 1) {
+      const double4 ka = a.kacc[row];
+      rx = rx - a.dt * ka.x;
+      ry = ry - a.dt * ka.y;
+      rz = rz - a.dt * ka.z;
     }
+    const double mf = a.minv_free[row];
+    if (mf == 0.0) rx = ry = rz = 0.0;  // Dirichlet node
+    const double4 acc = make_double4(rx * mf, ry * mf, rz * mf, 0.0);
+    const double4 h = a.unphalf[row];
+    const double4 u1 = make_double4(h.x + a.dt * acc.x, h.y + a.dt * acc.y, h.z + a.dt * acc.z, 0.0);
+    a.acc[row] = acc;
+    a.unp1[row] = u1;
+    if (a.r3out) a.r3out[row] = make_double4(rx, ry, rz, 0.0);
+    const double4 pv = a.unp1_prev[row];
+    const double4 un = a.un[row];
+    s_u2 = u1.x * u1.x + u1.y * u1.y + u1.z * u1.z;
+    const double dx = u1.x - pv.x, dy = u1.y - pv.y, dz = u1.z - pv.z;
+    s_du2 = dx * dx + dy * dy + dz * dz;
+    m_acc = fmax(fabs((u1.x - un.x) * inv_dt), fmax(fabs((u1.y - un.y) * inv_dt), fabs((u1.z - un.z) * inv_dt)));
   }
   double v[2] = {s_u2, s_du2};
   m_acc = warp_max(m_acc);
@@ -181,29 +164,23 @@ __global__ void __launch_bounds__(kRowThreads) k_step3(Step3Args<VT> a) {
   }
 }
 
-template <class VT, int LPR>
+template <class VT>
 __global__ void __launch_bounds__(kRowThreads) k_spmv_k3(SpmvK3Args<VT> a) {
-  constexpr int RPW = 32 / LPR;
-  const int lane = threadIdx.x & 31, sub = lane % LPR;
-  const long long gw = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long base = gw * RPW; base < a.NN; base += nw * RPW) {
-    const long long row = base + lane / LPR;
-    const bool ok = row < a.NN;
-    VT sx = 0, sy = 0, sz = 0;
-    if (ok) {
-      const int b = __ldg(a.rp + row), e = __ldg(a.rp + row + 1);
-      for (int j = b + sub; j < e; j += LPR) {
-        VT v = __ldg(a.val + j);
-        double4 x = ldg4(a.x + __ldg(a.col + j));
-        sx += v * (VT)x.x;
-        sy += v * (VT)x.y;
-        sz += v * (VT)x.z;
-      }
-    }
-    sx = group_sum<LPR>(sx); sy = group_sum<LPR>(sy); sz = group_sum<LPR>(sz);
-    if (ok && sub == 0) a.y[row] = make_double4((double)sx, (double)sy, (double)sz, 0.0);
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= a.NN) return;
+  const int s = row >> 5, l = row & 31;
+  const int b = __ldg(a.off + s) + l, w = (__ldg(a.off + s + 1) - __ldg(a.off + s)) >> 5;
+  VT sx = 0, sy = 0, sz = 0;
+#pragma unroll 4
+  for (int j = 0; j < w; j++) {
+    const int e = b + 32 * j;
+    const VT v = __ldcs(a.val + e);
+    const double4 x = ldg4(a.x + __ldcs(a.col + e));
+    sx += v * (VT)x.x;
+    sy += v * (VT)x.y;
+    sz += v * (VT)x.z;
   }
+  a.y[row] = make_double4((double)sx, (double)sy, (double)sz, 0.0);
 }
 
 __global__ void __launch_bounds__(kRowThreads) k_pressure_update(int n, double dt, const double* __restrict__ pn,
@@ -250,6 +227,18 @@ __global__ void k_reduce_norms(const double* __restrict__ up, int nub, const dou
   }
 }
 
+template <class T>
+__global__ void k_csr_to_sell(int nrows, const int* __restrict__ rp, const double* __restrict__ csr,
+                              const int* __restrict__ off, T* sell) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nslices = (nrows + 31) >> 5;
+  if (row >= nslices * 32) return;
+  const int s = row >> 5, l = row & 31;
+  const int b = off[s] + l, w = (off[s + 1] - off[s]) >> 5;
+  const int cb = row < nrows ? rp[row] : 0, len = row < nrows ? rp[row + 1] - cb : 0;
+  for (int j = 0; j < w; j++) sell[b + 32 * j] = j < len ? (T)csr[cb + j] : (T)0;
+}
+
 __global__ void k_blocks_to_vec4(int NN, const double* __restrict__ b, double4* v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x)
     v[i] = make_double4(b[i], b[(size_t)NN + i], b[2 * (size_t)NN + i], 0.0);
@@ -277,24 +266,24 @@ inline int ew_grid(long long n) {
 }  // namespace
 
 template <class VT>
-cudaError_t launch_step1(const Step1Args<VT>& a, int num_sms, cudaStream_t s) {
-  k_step1<VT, 16><<<row_grid(a.NN, 16, num_sms), kRowThreads, 0, s>>>(a);
+cudaError_t launch_step1(const Step1Args<VT>& a, int, cudaStream_t s) {
+  k_step1<VT><<<rows_grid(a.NN), kRowThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 template <class VT>
-cudaError_t launch_gt(const GtArgs<VT>& a, int num_sms, cudaStream_t s) {
-  k_gt<VT, 32><<<row_grid(a.NNp, 32, num_sms), kRowThreads, 0, s>>>(a);
+cudaError_t launch_gt(const GtArgs<VT>& a, int, cudaStream_t s) {
+  k_gt<VT><<<rows_grid(a.NNp), kRowThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
-int step3_blocks(int NN, int num_sms) { return row_grid(NN, 8, num_sms); }
+int step3_blocks(int NN, int) { return rows_grid(NN); }
 template <class VT>
 cudaError_t launch_step3(const Step3Args<VT>& a, cudaStream_t s) {
-  k_step3<VT, 8><<<a.nblocks, kRowThreads, 0, s>>>(a);
+  k_step3<VT><<<a.nblocks, kRowThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 template <class VT>
-cudaError_t launch_spmv_k3(const SpmvK3Args<VT>& a, int num_sms, cudaStream_t s) {
-  k_spmv_k3<VT, 16><<<row_grid(a.NN, 16, num_sms), kRowThreads, 0, s>>>(a);
+cudaError_t launch_spmv_k3(const SpmvK3Args<VT>& a, int, cudaStream_t s) {
+  k_spmv_k3<VT><<<rows_grid(a.NN), kRowThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 int pupdate_blocks(int NNp, int num_sms) { return ew_grid(NNp) < num_sms * 4 ? ew_grid(NNp) : num_sms * 4; }
@@ -306,6 +295,12 @@ cudaError_t launch_pressure_update(int NNp, double dt, const double* pn, const d
 cudaError_t launch_reduce_norms(const double* upart, int nub, const double* ppart, int npb, double* out,
                                 cudaStream_t s) {
   k_reduce_norms<<<1, 1024, 0, s>>>(upart, nub, ppart, npb, out);
+  return cudaGetLastError();
+}
+template <class T>
+cudaError_t launch_csr_to_sell(int nrows, const int* rp, const double* csr, const int* off, T* sell, cudaStream_t s) {
+  const int nslices = (nrows + 31) / 32;
+  k_csr_to_sell<T><<<rows_grid((long long)nslices * 32), kRowThreads, 0, s>>>(nrows, rp, csr, off, sell);
   return cudaGetLastError();
 }
 cudaError_t launch_blocks_to_vec4(int NN, const double* blocks, double4* v, cudaStream_t s) {
@@ -330,5 +325,7 @@ template cudaError_t launch_step3<double>(const Step3Args<double>&, cudaStream_t
 template cudaError_t launch_step3<float>(const Step3Args<float>&, cudaStream_t);
 template cudaError_t launch_spmv_k3<double>(const SpmvK3Args<double>&, int, cudaStream_t);
 template cudaError_t launch_spmv_k3<float>(const SpmvK3Args<float>&, int, cudaStream_t);
+template cudaError_t launch_csr_to_sell<double>(int, const int*, const double*, const int*, double*, cudaStream_t);
+template cudaError_t launch_csr_to_sell<float>(int, const int*, const double*, const int*, float*, cudaStream_t);
 
 }  // namespace cfd
