@@ -93,9 +93,10 @@ struct cfd_ctx {
   DevBuf<double> pbuf[6];
   double *pn = nullptr, *pnp1 = nullptr, *pnp1_prev = nullptr, *pdot = nullptr, *r2 = nullptr, *pzero = nullptr;
   // Krylov work
-  DevBuf<double> cg_r, cg_z, cg_p, cg_q, cg_part, cg_res, ir_r, ir_part, ir_sum;
-  DevBuf<float> f_b, f_x, f_r, f_z, f_p, f_q;
-  DevBuf<unsigned> cg_bar;
+  DevBuf<double> cg_work, cg_part, cg_res, ir_r, ir_part, ir_sum;
+  DevBuf<float> f_b, f_x, f_work;
+  DevBuf<unsigned> cg_sync;
+  DevBuf<int> nb64, nb32;  // per PCG block: [lo..., hi...] neighbour block ranges
   DevBuf<int> cg_err;
   int pcg_grid64 = 1, pcg_grid32 = 1, res_blocks = 1;
   // reductions
@@ -275,8 +276,8 @@ int upload_problem(cfd_ctx* c) {
     for (auto* b : {&c->gts1_32, &c->gts2_32, &c->gts3_32}) CU(b->alloc(sGt));
     CU(c->zs_val32.alloc(sZ));
     CU(c->zdinv32.alloc(NNp));
-    for (auto* b : {&c->f_b, &c->f_x, &c->f_r, &c->f_z, &c->f_q}) CU(b->alloc(NNp));
-    CU(c->f_p.alloc(2 * NNp));
+    for (auto* b : {&c->f_b, &c->f_x}) CU(b->alloc(NNp));
+    CU(c->f_work.alloc(10 * NNp));
   }
   for (auto& b : c->vbuf) {
     CU(b.alloc(NN));
@@ -291,13 +292,21 @@ int upload_problem(cfd_ctx* c) {
   }
   c->pn = c->pbuf[0].p; c->pnp1 = c->pbuf[1].p; c->pnp1_prev = c->pbuf[2].p; c->pdot = c->pbuf[3].p;
   c->r2 = c->pbuf[4].p; c->pzero = c->pbuf[5].p;
-  for (auto* b : {&c->cg_r, &c->cg_z, &c->cg_q, &c->ir_r}) CU(b->alloc(NNp));
-  CU(c->cg_p.alloc(2 * NNp));
+  CU(c->ir_r.alloc(NNp));
+  CU(c->cg_work.alloc(10 * NNp));
   c->pcg_grid64 = pcg_max_grid<double>((int)NNp, c->device);
   c->pcg_grid32 = pcg_max_grid<float>((int)NNp, c->device);
-  CU(c->cg_part.alloc(6 * (size_t)std::max(c->pcg_grid64, c->pcg_grid32)));
+  const int gmax = std::max(c->pcg_grid64, c->pcg_grid32);
+  CU(c->cg_part.alloc(8 * (size_t)gmax));
+  CU(c->cg_sync.alloc(1 + (size_t)gmax));
+  for (int pass = 0; pass < 2; pass++) {
+    const int grid = pass == 0 ? c->pcg_grid64 : c->pcg_grid32;
+    std::vector<int> nb(2 * (size_t)grid);
+    pcg_neighbor_ranges((int)NNp, grid, P.z_soff.data(), P.z_scol.data(), nb.data(), nb.data() + grid);
+    CU(upload(pass == 0 ? c->nb64 : c->nb32, nb, s));
+  }
   CU(c->cg_res.alloc(8));
-  CU(c->cg_bar.alloc(2));
+
   CU(c->cg_err.alloc(1));
   c->res_blocks = residual_blocks((int)NNp, c->num_sms);
   CU(c->ir_part.alloc(c->res_blocks));
@@ -324,13 +333,14 @@ int upload_problem(cfd_ctx* c) {
 
 int run_pcg64(cfd_ctx* c, const double* b, double* x, int warm, double rtol, int maxit, double* res) {
   cudaStream_t s = c->stream;
-  CU(cudaMemsetAsync(c->cg_bar.p, 0, 2 * sizeof(unsigned), s));
+  CU(cudaMemsetAsync(c->cg_sync.p, 0, c->cg_sync.bytes(), s));
   CU(cudaMemsetAsync(c->cg_err.p, 0, sizeof(int), s));
   PcgArgs<double> a{};
   a.n = c->P.NNp;
   a.off = c->zs_off.p; a.col = c->zs_col.p; a.val = c->zs_val.p; a.dinv = c->zdinv.p;
-  a.b = b; a.x = x; a.r = c->cg_r.p; a.z = c->cg_z.p; a.p = c->cg_p.p; a.q = c->cg_q.p;
-  a.part = c->cg_part.p; a.bar = c->cg_bar.p; a.err = c->cg_err.p;
+  a.b = b; a.x = x; a.work = c->cg_work.p;
+  a.part = c->cg_part.p; a.sync = c->cg_sync.p; a.err = c->cg_err.p;
+  a.nb_lo = c->nb64.p; a.nb_hi = c->nb64.p + c->pcg_grid64;
   a.rtol = rtol; a.maxit = maxit; a.warm = warm; a.result = c->cg_res.p;
   a.timeout_ns = 2000000000ULL;
   KL(CFD_K_PCG64, launch_pcg<double>(a, c->pcg_grid64, s));
@@ -343,13 +353,14 @@ int run_pcg64(cfd_ctx* c, const double* b, double* x, int warm, double rtol, int
 
 int run_pcg32(cfd_ctx* c, double rtol, int maxit, double* res) {
   cudaStream_t s = c->stream;
-  CU(cudaMemsetAsync(c->cg_bar.p, 0, 2 * sizeof(unsigned), s));
+  CU(cudaMemsetAsync(c->cg_sync.p, 0, c->cg_sync.bytes(), s));
   CU(cudaMemsetAsync(c->cg_err.p, 0, sizeof(int), s));
   PcgArgs<float> a{};
   a.n = c->P.NNp;
   a.off = c->zs_off.p; a.col = c->zs_col.p; a.val = c->zs_val32.p; a.dinv = c->zdinv32.p;
-  a.b = c->f_b.p; a.x = c->f_x.p; a.r = c->f_r.p; a.z = c->f_z.p; a.p = c->f_p.p; a.q = c->f_q.p;
-  a.part = c->cg_part.p; a.bar = c->cg_bar.p; a.err = c->cg_err.p;
+  a.b = c->f_b.p; a.x = c->f_x.p; a.work = c->f_work.p;
+  a.part = c->cg_part.p; a.sync = c->cg_sync.p; a.err = c->cg_err.p;
+  a.nb_lo = c->nb32.p; a.nb_hi = c->nb32.p + c->pcg_grid32;
   a.rtol = rtol; a.maxit = maxit; a.warm = 0; a.result = c->cg_res.p;
   a.timeout_ns = 2000000000ULL;
   KL(CFD_K_PCG32, launch_pcg<float>(a, c->pcg_grid32, s));

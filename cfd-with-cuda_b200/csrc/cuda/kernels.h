@@ -136,19 +136,23 @@ cudaError_t launch_reduce_norms(const double* upart, int nub, const double* ppar
 template <class VT>
 struct PcgArgs {
   int n;
-  const int *off, *col;  // SELL-32
+  const int *off, *col;  // SELL-32 Z
   const VT* val;
   const VT* dinv;
   const VT* b;
-  VT *x, *r, *z, *p, *q;  // p holds two n-vectors (double-buffered search direction)
-  double* part;  // 2 x 3 x grid doubles
-  unsigned* bar; // 2 unsigned (host-zeroed)
-  int* err;      // host-zeroed
+  VT* x;
+  VT* work;                    // 10 n: r, u, w, z, q, s, p, n, m (two buffers)
+  double* part;                // 2 x 4 x grid partial sums
+  unsigned* sync;              // 1 + grid words, host-zeroed: arrival counter, block progress
+  const int *nb_lo, *nb_hi;    // per block: range of blocks whose rows it gathers
+  int* err;                    // host-zeroed
   double rtol;
   int maxit, warm;
   double* result;  // its, relres, status, bnorm
   unsigned long long timeout_ns;
 };
+// Block ranges each PCG block gathers from, for a given grid (host).
+void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi);
 template <class VT>
 cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s);
 template <class VT>

@@ -3,21 +3,18 @@
 // precond::diagonal, CUDAcodes.cu:418-451, and MKL dcg, blascoCodinaHuerta.cpp:
 // 3981-4055).
 //
-// Z is stored SELL-32; thread g owns rows g, g+T, g+2T, ... (T = all
-// threads, a multiple of 32, so a warp always owns whole slices).  The
-// search-direction update p = z + beta p is folded into the next SpMV, which
-// evaluates q = Z (z + beta p_old) from gathers of z and p_old and writes
-// p_new for its own rows into the other half of a double buffer.  That leaves
-// two grid-wide reductions per iteration:
-//   A: p_new = z + beta p_old, q = Z p_new (own rows), partial p_new.q  -> reduce
-//   B: x += alpha p_new, r -= alpha q, z = Dinv r, partial r.r, r.z     -> reduce
-// Each reduction writes per-block partials, passes a bounded grid barrier,
-// and every block sums all partials in the same fixed order (FP64), so every
-// block takes the same decisions.  Vectors written inside the kernel are
-// gathered with L2 loads (ld.cg); the matrix is streamed (ld.cs) so the
-// vectors stay resident in L2.  Stopping rule: ||r||_2 <= rtol ||b||_2 on the
-// recursively updated residual, checked after each update (as the oracle).
+// Z is stored SELL-32; a warp owns a contiguous range of 32-row slices and
+// streams their columns and values through shared memory with bulk
+// asynchronous copies (ChunkStream).  The iteration is the pipelined form of
+// PCG (k_pcg below): the three dot products of an iteration are posted before
+// its SpMV and collected after it, and blocks wait only for the neighbouring
+// blocks whose rows they gather, so no grid-wide barrier sits on the critical
+// path.  Every block sums the posted partials in the same fixed order
+// (FP64), so all blocks take the same decisions.  Every wait (progress
+// flag, arrival counter, mbarrier) is bounded and reports a timeout status.
+// Stopping rule: ||r||_2 <= rtol ||b||_2 on the recursively updated residual.
 #include <algorithm>
+#include <vector>
 
 #include "kernels.h"
 
@@ -25,133 +22,412 @@ namespace cfd {
 
 namespace {
 
-constexpr int kPcgThreads = 256;
+constexpr int kPcgWarps = 16;
+constexpr int kPcgThreads = kPcgWarps * 32;
 
-template <int NV>
-__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* part, int phase, unsigned* bar, int* err,
-                                            unsigned long long timeout_ns) {
-  __shared__ double res[NV];
-  const int G = gridDim.x;
-  double* buf = part + (size_t)(phase & 1) * 3 * G;
-  block_sum<NV>(v);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < NV; k++) buf[(size_t)k * G + blockIdx.x] = v[k];
-  if (!grid_barrier(bar, err, timeout_ns)) return false;
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-#pragma unroll
-    for (int k = 0; k < NV; k++) {
-      double s = 0;
-      for (int i = lane; i < G; i += 32) s += __ldcg(buf + (size_t)k * G + i);
-      s = warp_sum(s);
-      if (lane == 0) res[k] = s;
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int k = 0; k < NV; k++) v[k] = res[k];
-  __syncthreads();
-  return true;
+// Shared-memory staging of the streamed SELL matrix: each warp walks its own
+// contiguous range of slices as a cyclic stream of chunks (kCh columns x 32
+// rows of columns and values).  Lane 0 keeps kNbuf<VT> chunks in flight with
+// bulk asynchronous copies completed on one mbarrier per buffer; the stream
+// repeats every iteration, so copies for the next iteration's first chunks
+// are already in flight while the warp waits at the grid barrier.
+constexpr int kCh = 8;
+// chunk buffers per warp: three FP32 or two FP64 chunks keep two blocks of
+// 16 warps per SM within the shared-memory budget
+template <class VT>
+constexpr int kNbuf = sizeof(VT) == 4 ? 3 : 2;
+
+template <class VT>
+struct __align__(16) Chunk {
+  int col[kCh * 32];
+  VT val[kCh * 32];
+};
+
+template <class VT>
+constexpr size_t pcg_smem_bytes() {
+  return (size_t)kPcgWarps * kNbuf<VT> * (sizeof(Chunk<VT>) + sizeof(unsigned long long));
 }
 
 template <class VT>
-__global__ void __launch_bounds__(kPcgThreads, 5) k_pcg(PcgArgs<VT> a) {
-  const int T = gridDim.x * blockDim.x;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = a.n;
-  VT* P0 = a.p;
-  VT* P1 = a.p + n;
-  int phase = 0;
+struct ChunkStream {
+  const int* off;
+  const int* col;
+  const VT* val;
+  Chunk<VT>* buf;               // kNbuf<VT> buffers of this warp
+  unsigned long long* mbar;     // kNbuf<VT> mbarriers of this warp
+  int s_begin, s_end;           // owned slices [s_begin, s_end)
+  int is, ik, nbi;              // next chunk to issue (slice, chunk, buffer)
+  int cs, ck, nbc;              // next chunk to consume
+  unsigned parity;              // phase parity per buffer (bit b)
+  bool failed;
 
-  // ---- initial residual ----
-  double v3[3] = {0, 0, 0};
-  for (int i = g; i < n; i += T) {
+  __device__ int nchunks(int s) const { return ((__ldg(off + s + 1) - __ldg(off + s)) / 32 + kCh - 1) / kCh; }
+
+  __device__ void issue(int lane) {
+    if (lane == 0) {
+      const int base = __ldg(off + is), w = (__ldg(off + is + 1) - base) >> 5;
+      const int c0 = ik * kCh, nc = min(kCh, w - c0);
+      Chunk<VT>* B = buf + nbi;
+      fence_proxy_async_smem();
+      mbar_expect_tx(mbar + nbi, (unsigned)(nc * 32 * (4 + (int)sizeof(VT))));
+      bulk_g2s(B->col, col + base + c0 * 32, (unsigned)(nc * 32 * 4), mbar + nbi);
+      bulk_g2s(B->val, val + base + c0 * 32, (unsigned)(nc * 32 * (int)sizeof(VT)), mbar + nbi);
+    }
+    if (++ik == nchunks(is)) {
+      ik = 0;
+      if (++is == s_end) is = s_begin;
+    }
+    nbi = (nbi + 1 == kNbuf<VT>) ? 0 : nbi + 1;
+  }
+
+  __device__ void start(int lane) {
+    if (s_begin < s_end)
+      for (int k = 0; k < kNbuf<VT>; k++) issue(lane);
+  }
+
+  // Waits for the next chunk; false (and *err set) when the bounded wait gave up.
+  __device__ bool wait(int* err, unsigned long long timeout_ns) {
+    if (failed) return false;
+    if (!mbar_wait_bounded(mbar + nbc, (parity >> nbc) & 1u, timeout_ns)) {
+      failed = true;
+      atomicExch(err, 1);
+      return false;
+    }
+    return true;
+  }
+
+  // Releases the consumed buffer, refills it, advances; true at slice end.
+  __device__ bool release(int lane) {
+    __syncwarp();
+    parity ^= 1u << nbc;
+    nbc = (nbc + 1 == kNbuf<VT>) ? 0 : nbc + 1;
+    if (!failed) issue(lane);
+    if (++ck == nchunks(cs)) {
+      ck = 0;
+      if (++cs == s_end) cs = s_begin;
+      return true;
+    }
+    return false;
+  }
+
+  // Waits (bounded) for every copy still in flight before the block exits.
+  __device__ void drain(unsigned long long timeout_ns) {
+    if (s_begin >= s_end) return;
+    for (int k = 0; k < kNbuf<VT>; k++) {
+      const int b = (nbc + k) % kNbuf<VT>;
+      if (!mbar_wait_bounded(mbar + b, (parity >> b) & 1u, timeout_ns)) break;
+      parity ^= 1u << b;
+    }
+  }
+};
+
+// Product of one staged chunk with a gathered vector g.  Gathers are plain
+// (L1-cached) loads: g is written by other blocks during the solve, and the
+// release/acquire progress flags make those writes visible before use.
+template <class VT>
+__device__ __forceinline__ VT chunk_dot(const Chunk<VT>* B, int nc, int lane, const VT* g) {
+  VT acc = 0;
+#pragma unroll
+  for (int jj = 0; jj < kCh; jj++)
+    if (jj < nc) acc += B->val[jj * 32 + lane] * g[B->col[jj * 32 + lane]];
+  return acc;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) { return ld_acquire_u32(p); }
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Block-level synchronisation of the pipelined solve (all waits bounded):
+//   publish(k)        this block's own rows of phase k are written
+//   wait_nb(k)        every block owning a row this block gathers reached k
+//   arrive/wait_red   monotonic arrival counter of the per-iteration reduction
+struct BlockSync {
+  unsigned* cnt;
+  unsigned* prog;
+  int lo, hi;
+  int* err;
+  unsigned long long timeout_ns;
+
+  __device__ void publish(unsigned k) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release_gpu(prog + blockIdx.x, k);
+    }
+  }
+  __device__ bool wait_nb(unsigned k) {
+    __shared__ int ok;
+    if (threadIdx.x < 32) {
+      // one lane per neighbour block, all polled at once
+      int good = 1;
+      const unsigned long long t0 = global_ns();
+      for (int j0 = lo; j0 <= hi; j0 += 32) {
+        const int j = j0 + (int)threadIdx.x;
+        bool done = j > hi;
+        while (true) {
+          if (!done) done = ld_acquire_gpu(prog + j) >= k;
+          if (__all_sync(0xffffffffu, done)) break;
+          if (ld_volatile_i32(err) || global_ns() - t0 > timeout_ns) {
+            good = 0;
+            break;
+          }
+        }
+        good = __all_sync(0xffffffffu, good);
+        if (!good) break;
+      }
+      __threadfence();
+      if (threadIdx.x == 0) {
+        if (!good) atomicExch(err, 1);
+        ok = good;
+      }
+    }
+    __syncthreads();
+    return ok != 0;
+  }
+  // partials already written by thread 0 of this block
+  __device__ void arrive() {
+    if (threadIdx.x == 0) {
+      __threadfence();
+      red_release_add(cnt, 1u);
+    }
+  }
+  // Waits until `target` arrivals, then every block sums the partials in the
+  // same fixed order (FP64): all blocks see identical values.
+  template <int NV>
+  __device__ bool wait_red(unsigned target, const double* buf, double (&v)[NV]) {
+    __shared__ double res[NV];
+    __shared__ int ok;
+    const int G = gridDim.x;
+    if (threadIdx.x < 32) {
+      int good = 1;
+      const unsigned long long t0 = global_ns();
+      while (ld_acquire_gpu(cnt) < target) {
+        if (ld_volatile_i32(err) || global_ns() - t0 > timeout_ns) {
+          good = 0;
+          break;
+        }
+      }
+      good = __all_sync(0xffffffffu, good);
+      if (good) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+          double sum = 0;
+          for (int i = threadIdx.x; i < G; i += 32) sum += __ldcg(buf + (size_t)k * G + i);
+          sum = warp_sum(sum);
+          if (threadIdx.x == 0) res[k] = sum;
+        }
+      } else if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+      }
+      if (threadIdx.x == 0) ok = good;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = res[k];
+    const bool r = ok != 0;
+    __syncthreads();
+    return r;
+  }
+};
+
+// Writes this block's partial sums of NV values into buf (thread 0).
+template <int NV>
+__device__ __forceinline__ void block_partials(double (&v)[NV], double* buf) {
+  block_sum<NV>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; k++) buf[(size_t)k * gridDim.x + blockIdx.x] = v[k];
+}
+
+// Pipelined Jacobi-PCG (Ghysels & Vanroose 2014) with M = diag(Z)^-1:
+//   g_i = (r_i,u_i), d_i = (w_i,u_i), m_i = M w_i, n_i = Z m_i
+//   b_i = g_i/g_{i-1}, a_i = g_i/(d_i - b_i g_i/a_{i-1})   (b_0 = 0, a_0 = g_0/d_0)
+//   z = n + b z,  q = m + b q,  s = w + b s,  p = u + b p
+//   x += a p,  r -= a s,  u -= a q,  w -= a z
+// Same iterates as standard PCG in exact arithmetic.  The dot products of
+// iteration i are posted (partials + release-add on a counter) before the SpMV
+// n_i = Z m_i and collected after it, so the reduction is off the critical
+// path; blocks synchronise only with the blocks whose rows they gather
+// (progress flags), never grid-wide.  A warp owns whole 32-row slices
+// (lane = row) and streams them through shared memory (ChunkStream).
+template <class VT>
+__global__ void __launch_bounds__(kPcgThreads, 2) k_pcg(PcgArgs<VT> a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int n = a.n, nslices = (n + 31) >> 5;
+  const int W = gridDim.x * kPcgWarps, gw = blockIdx.x * kPcgWarps + wib;
+  Chunk<VT>* chunks = reinterpret_cast<Chunk<VT>*>(smem);
+  unsigned long long* mbars =
+      reinterpret_cast<unsigned long long*>(smem + (size_t)kPcgWarps * kNbuf<VT> * sizeof(Chunk<VT>));
+  ChunkStream<VT> st;
+  st.off = a.off;
+  st.col = a.col;
+  st.val = a.val;
+  st.buf = chunks + wib * kNbuf<VT>;
+  st.mbar = mbars + wib * kNbuf<VT>;
+  st.s_begin = (int)((long long)nslices * gw / W);
+  st.s_end = (int)((long long)nslices * (gw + 1) / W);
+  st.is = st.cs = st.s_begin;
+  st.ik = st.ck = 0;
+  st.nbi = st.nbc = 0;
+  st.parity = 0;
+  st.failed = false;
+  if (lane == 0)
+    for (int k = 0; k < kNbuf<VT>; k++) mbar_init(st.mbar + k, 1);
+  mbar_init_fence();
+  __syncthreads();
+
+  BlockSync bs;
+  bs.cnt = a.sync;
+  bs.prog = a.sync + 1;
+  bs.lo = a.nb_lo[blockIdx.x];
+  bs.hi = a.nb_hi[blockIdx.x];
+  bs.err = a.err;
+  bs.timeout_ns = a.timeout_ns;
+
+  VT* r = a.work;
+  VT* u = r + n;
+  VT* w = u + n;
+  VT* z = w + n;
+  VT* q = z + n;
+  VT* s = q + n;
+  VT* p = s + n;
+  VT* nv = p + n;
+  VT* mb[2] = {nv + n, nv + 2 * (size_t)n};
+  const int G = gridDim.x;
+
+  // P1: r = b - Z x0, u = M r (own rows)
+  double bb = 0;
+  for (int sl = st.s_begin; sl < st.s_end; sl++) {
+    const int i = sl * 32 + lane;
+    if (i >= n) continue;
     const double bi = (double)a.b[i];
     double ri = bi;
     if (a.warm) {
-      const int s = i >> 5, l = i & 31;
-      const int b = __ldg(a.off + s) + l, w = (__ldg(a.off + s + 1) - __ldg(a.off + s)) >> 5;
-      VT q = 0;
-      for (int j = 0; j < w; j++) q += __ldcs(a.val + b + 32 * j) * a.x[__ldcs(a.col + b + 32 * j)];
-      ri = bi - (double)q;
-    } else {
-      a.x[i] = (VT)0;
+      const int b0 = __ldg(a.off + sl) + lane, wd = (__ldg(a.off + sl + 1) - __ldg(a.off + sl)) >> 5;
+      VT acc = 0;
+      for (int j = 0; j < wd; j++) acc += __ldg(a.val + b0 + 32 * j) * a.x[__ldg(a.col + b0 + 32 * j)];
+      ri = bi - (double)acc;
     }
     const VT rv = (VT)ri;
-    const VT zv = (VT)((double)rv * (double)a.dinv[i]);
-    a.r[i] = rv;
-    a.z[i] = zv;
-    P0[i] = (VT)0;
-    v3[0] += bi * bi;
-    v3[1] += (double)rv * (double)zv;
-    v3[2] += (double)rv * (double)rv;
+    r[i] = rv;
+    u[i] = rv * a.dinv[i];
+    bb += bi * bi;
   }
-  const bool alive = grid_reduce<3>(v3, a.part, phase++, a.bar, a.err, a.timeout_ns);
-  const double bnorm = sqrt(v3[0]);
-  double rz = v3[1];
-  double rn = sqrt(v3[2]);
-  const double tol = a.rtol * bnorm;
-  int its = 0, status = 1;
-  if (!alive) {
-    status = 3;
-  } else if (!isfinite(bnorm) || !isfinite(rn)) {
-    status = 2;
-  } else if (bnorm == 0.0) {
-    for (int i = g; i < n; i += T) a.x[i] = (VT)0;
-    status = 0;
-    rn = 0;
-  } else if (rn <= tol) {
-    status = 0;
-  } else {
-    VT beta = 0;
-    VT* pold = P0;
-    VT* pnew = P1;
-    while (its < a.maxit) {
-      // A: p_new = z + beta p_old;  q = Z p_new
-      double pq = 0;
-      for (int i = g; i < n; i += T) {
-        const int s = i >> 5, l = i & 31;
-        const int b = __ldg(a.off + s) + l, w = (__ldg(a.off + s + 1) - __ldg(a.off + s)) >> 5;
-        VT q = 0;
-#pragma unroll 4
-        for (int j = 0; j < w; j++) {
-          const int c = __ldcs(a.col + b + 32 * j);
-          const VT pc = __ldcg(a.z + c) + beta * __ldcg(pold + c);
-          q += __ldcs(a.val + b + 32 * j) * pc;
-        }
-        const VT pi = a.z[i] + beta * pold[i];
-        pnew[i] = pi;
-        a.q[i] = q;
-        pq += (double)pi * (double)q;
-      }
-      double v1[1] = {pq};
-      if (!grid_reduce<1>(v1, a.part, phase++, a.bar, a.err, a.timeout_ns)) { status = 3; break; }
-      const double alpha = rz / v1[0];
-      // B: updates on own rows
-      double v2[2] = {0, 0};
-      for (int i = g; i < n; i += T) {
-        const double pi = (double)pnew[i], qi = (double)a.q[i];
-        a.x[i] = (VT)((double)a.x[i] + alpha * pi);
-        const VT rv = (VT)((double)a.r[i] - alpha * qi);
-        const VT zv = (VT)((double)rv * (double)a.dinv[i]);
-        a.r[i] = rv;
-        a.z[i] = zv;
-        v2[0] += (double)rv * (double)rv;
-        v2[1] += (double)rv * (double)zv;
-      }
-      if (!grid_reduce<2>(v2, a.part, phase++, a.bar, a.err, a.timeout_ns)) { status = 3; break; }
-      its++;
-      rn = sqrt(v2[0]);
-      if (!isfinite(rn)) { status = 2; break; }
-      if (rn <= tol) { status = 0; break; }
-      beta = (VT)(v2[1] / rz);
-      rz = v2[1];
-      VT* t = pold;
-      pold = pnew;
-      pnew = t;
+  st.start(lane);
+  bs.publish(1);
+  if (!a.warm)
+    for (int sl = st.s_begin; sl < st.s_end; sl++)
+      if (sl * 32 + lane < n) a.x[sl * 32 + lane] = (VT)0;
+  // P2: w = Z u, m0 = M w, dots of iteration 0
+  bool alive = bs.wait_nb(1);
+  if (!alive) st.failed = true;  // stop refilling: chunks may still be in flight
+  double v[4] = {0, 0, 0, bb};
+  for (int sl = st.s_begin; sl < st.s_end; sl++) {
+    VT acc = 0;
+    const int wd = (__ldg(a.off + sl + 1) - __ldg(a.off + sl)) >> 5;
+    for (int c0 = 0; c0 < wd; c0 += kCh) {
+      if (alive && st.wait(a.err, a.timeout_ns)) acc += chunk_dot<VT>(st.buf + st.nbc, min(kCh, wd - c0), lane, u);
+      st.release(lane);
+    }
+    const int i = sl * 32 + lane;
+    if (i < n) {
+      w[i] = acc;
+      mb[0][i] = acc * a.dinv[i];
+      z[i] = (VT)0;
+      q[i] = (VT)0;
+      s[i] = (VT)0;
+      p[i] = (VT)0;
+      const double ri = (double)r[i], ui = (double)u[i];
+      v[0] += ri * ui;
+      v[1] += (double)acc * ui;
+      v[2] += ri * ri;
     }
   }
+  block_partials<4>(v, a.part);
+  bs.publish(2);
+  bs.arrive();
+
+  double bnorm = 0, tol = 0, rn = 0, gam_old = 1, alpha_old = 1;
+  int its = 0, status = 1;
+  for (int i = 0;; i++) {
+    // n_i = Z m_i  (neighbours' m_i published at phase i + 2)
+    if (alive) alive = bs.wait_nb((unsigned)i + 2);
+    if (!alive) st.failed = true;
+    const VT* mi = mb[i & 1];
+    for (int sl = st.s_begin; sl < st.s_end; sl++) {
+      VT acc = 0;
+      const int wd = (__ldg(a.off + sl + 1) - __ldg(a.off + sl)) >> 5;
+      for (int c0 = 0; c0 < wd; c0 += kCh) {
+        if (alive && st.wait(a.err, a.timeout_ns)) acc += chunk_dot<VT>(st.buf + st.nbc, min(kCh, wd - c0), lane, mi);
+        st.release(lane);
+      }
+      const int ii = sl * 32 + lane;
+      if (ii < n) nv[ii] = acc;
+    }
+    // reduction of iteration i (posted before the SpMV)
+    double red[4];
+    if (!alive || !bs.wait_red<4>((unsigned)(i + 1) * (unsigned)G, a.part + (size_t)(i & 1) * 4 * G, red)) {
+      status = 3;
+      break;
+    }
+    if (i == 0) {
+      bnorm = sqrt(red[3]);
+      tol = a.rtol * bnorm;
+    }
+    rn = sqrt(red[2]);
+    if (!isfinite(bnorm) || !isfinite(rn)) { status = 2; break; }
+    if (bnorm == 0.0) {
+      for (int sl = st.s_begin; sl < st.s_end; sl++)
+        if (sl * 32 + lane < n) a.x[sl * 32 + lane] = (VT)0;
+      rn = 0;
+      status = 0;
+      break;
+    }
+    if (rn <= tol) { status = 0; break; }
+    if (its >= a.maxit) { status = 1; break; }
+    const double gam = red[0], del = red[1];
+    const double beta = i > 0 ? gam / gam_old : 0.0;
+    const double alpha = i > 0 ? gam / (del - beta * gam / alpha_old) : gam / del;
+    gam_old = gam;
+    alpha_old = alpha;
+    const VT al = (VT)alpha, be = (VT)beta;
+    VT* mnext = mb[(i + 1) & 1];
+    double d[4] = {0, 0, 0, 0};
+    for (int sl = st.s_begin; sl < st.s_end; sl++) {
+      const int ii = sl * 32 + lane;
+      if (ii >= n) continue;
+      const VT zi = nv[ii] + be * z[ii];
+      const VT qi = mi[ii] + be * q[ii];
+      const VT si = w[ii] + be * s[ii];
+      const VT pi = u[ii] + be * p[ii];
+      const VT xi = a.x[ii] + al * pi;
+      const VT ri = r[ii] - al * si;
+      const VT ui = u[ii] - al * qi;
+      const VT wi = w[ii] - al * zi;
+      z[ii] = zi;
+      q[ii] = qi;
+      s[ii] = si;
+      p[ii] = pi;
+      a.x[ii] = xi;
+      r[ii] = ri;
+      u[ii] = ui;
+      w[ii] = wi;
+      mnext[ii] = wi * a.dinv[ii];
+      d[0] += (double)ri * (double)ui;
+      d[1] += (double)wi * (double)ui;
+      d[2] += (double)ri * (double)ri;
+    }
+    its++;
+    block_partials<4>(d, a.part + (size_t)((i + 1) & 1) * 4 * G);
+    bs.publish((unsigned)i + 3);
+    bs.arrive();
+  }
+  st.drain(a.timeout_ns);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     a.result[0] = its;
     a.result[1] = bnorm > 0 ? rn / bnorm : 0.0;
@@ -222,18 +498,47 @@ template <class VT>
 int pcg_max_grid(int n, int device) {
   int sms = 0, per_sm = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<VT>, kPcgThreads, 0);
+  const size_t smem = pcg_smem_bytes<VT>();
+  cudaFuncSetAttribute(k_pcg<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<VT>, kPcgThreads, smem);
   long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
   long long want = ((long long)n + kPcgThreads - 1) / kPcgThreads;  // one row per thread at most
   if (want < 1) want = 1;
   return (int)std::min(cap, want);
 }
 
+void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi) {
+  const int ns = (n + 31) / 32;
+  const long long W = (long long)grid * kPcgWarps;
+  std::vector<int> owner(ns);
+  for (int b = 0; b < grid; b++) {
+    const int s0 = (int)(ns * (kPcgWarps * (long long)b) / W), s1 = (int)(ns * (kPcgWarps * (long long)(b + 1)) / W);
+    for (int s = s0; s < s1; s++) owner[s] = b;
+  }
+  for (int b = 0; b < grid; b++) {
+    const int s0 = (int)(ns * (kPcgWarps * (long long)b) / W), s1 = (int)(ns * (kPcgWarps * (long long)(b + 1)) / W);
+    int cmin = n, cmax = -1;
+    for (int s = s0; s < s1; s++)
+      for (int e = soff[s]; e < soff[s + 1]; e++) {
+        cmin = std::min(cmin, scol[e]);
+        cmax = std::max(cmax, scol[e]);
+      }
+    if (cmax < 0) {
+      lo[b] = b;
+      hi[b] = b - 1;  // no neighbours
+    } else {
+      lo[b] = owner[cmin / 32];
+      hi[b] = owner[cmax / 32];
+    }
+  }
+}
+
 template <class VT>
 cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s) {
   PcgArgs<VT> args = a;
   void* params[] = {&args};
-  return cudaLaunchCooperativeKernel((const void*)k_pcg<VT>, dim3(grid), dim3(kPcgThreads), params, 0, s);
+  return cudaLaunchCooperativeKernel((const void*)k_pcg<VT>, dim3(grid), dim3(kPcgThreads), params,
+                                     pcg_smem_bytes<VT>(), s);
 }
 
 int residual_blocks(int n, int) { return std::max(1, (n + kResThreads - 1) / kResThreads); }
