@@ -70,6 +70,7 @@ class RunStats(C.Structure):
 
 _lib = None
 _vp, _ip, _dp, _cp, _llp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_char_p, C.POINTER(C.c_longlong)
+_fp = C.POINTER(C.c_float)
 
 _PROTOS = {
     "cfd_abi_version": (C.c_int, []),
@@ -102,7 +103,22 @@ _PROTOS = {
     "cfd_write_tecplot": (C.c_int, [_vp, _cp, _cp]),
     "cfd_read_restart": (C.c_int, [_vp, _cp]),
     "cfd_set_bc_values": (C.c_int, [_vp, C.c_int, _ip, _dp]),
-    "cfd_unet_load": (C.c_int, [_vp, _cp]),
+    "cfd_unet_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_ulonglong]),
+    "cfd_unet_destroy": (None, [_vp]),
+    "cfd_unet_last_error": (C.c_char_p, [_vp]),
+    "cfd_unet_param_count": (C.c_longlong, []),
+    "cfd_unet_get_params": (C.c_int, [_vp, _fp, C.c_longlong]),
+    "cfd_unet_set_params": (C.c_int, [_vp, _fp, C.c_longlong]),
+    "cfd_unet_save": (C.c_int, [_vp, _cp]),
+    "cfd_unet_read": (C.c_int, [_vp, _cp]),
+    "cfd_unet_forward": (C.c_int, [_vp, _ip, _vp, _vp, C.c_int]),
+    "cfd_unet_gradient": (C.c_int, [_vp, _ip, _vp, _vp, C.c_int, _fp, _fp]),
+    "cfd_unet_train_batch": (C.c_int, [_vp, _ip, C.c_int, _vp, _vp, C.c_int, C.c_float, _fp]),
+    "cfd_unet_set_loss": (C.c_int, [_vp, C.c_float, C.c_float]),
+    "cfd_unet_tensor": (C.c_int, [_vp, C.c_int, _fp, C.c_longlong]),
+    "cfd_unet_attach": (C.c_int, [_vp, _vp, _ip, _ip]),
+    "cfd_unet_load": (C.c_int, [_vp, _cp, _ip]),
+    "cfd_pressure_residual": (C.c_int, [_vp, _dp, _dp, _dp, _dp]),
     "cfd_stream": (C.c_void_p, [_vp]),
     "cfd_launch_count": (C.c_longlong, [_vp]),
     "cfd_profile": (C.c_int, [_vp, C.c_int]),
@@ -224,7 +240,21 @@ class Solver:
         o.precision, o.precond, o.cg_rtol, o.cg_maxit, o.cg_warm = precision, precond, cg_rtol, cg_maxit, cg_warm
         o.ngp_override, o.inner_rtol, o.max_outer = ngp, inner_rtol, max_outer
         self._check(L.cfd_set_options(h, C.byref(o)))
+        self.opts = o
         self.info = None
+        self._unet = None
+
+    def set_options(self, **kw):
+        """Changes options of a live context (precision and ngp only before
+        load): precond, cg_rtol, cg_maxit, cg_warm, inner_rtol, max_outer."""
+        o = Options()
+        C.memmove(C.byref(o), C.byref(self.opts), C.sizeof(Options))
+        for k, v in kw.items():
+            if k == "ngp":
+                k = "ngp_override"
+            setattr(o, k, v)
+        self._check(self.L.cfd_set_options(self.h, C.byref(o)))
+        self.opts = o
 
     # ---- plumbing ----
     def _check(self, rc: int):
@@ -322,8 +352,9 @@ class Solver:
         self._check(self.L.cfd_run(self.h, nsteps, C.byref(st)))
         return st
 
-    def time_step(self):
-        """One time step through the stage calls (timeLoop body)."""
+    def time_step(self, after_step2=None):
+        """One time step through the stage calls (timeLoop body);
+        ``after_step2(it)`` is called after each pressure solve."""
         i = self.refresh()
         self.begin_step()
         cg = []
@@ -332,6 +363,8 @@ class Solver:
             self.calculateMatrixAGPU()
             self.step1GPUpart(it)
             cg.append(self.step2GPU(it).iterations)
+            if after_step2 is not None:
+                after_step2(it)
             self.step3GPU(it)
             conv, _ = self.checkConvergenceGPU(i.tolerance)
             if conv:
@@ -392,8 +425,41 @@ class Solver:
             self._check(rc)
         return x, st
 
+    def pressure_residual(self, rhs, x):
+        """r = rhs - Z x in FP64 on the device; returns (r, ||r||)."""
+        i = self.info or self.refresh()
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        r = np.zeros(i.NNp)
+        nrm = C.c_double()
+        self._check(self.L.cfd_pressure_residual(self.h, _p(rhs, C.c_double), _p(x, C.c_double),
+                                                 _p(r, C.c_double), C.byref(nrm)))
+        return r, nrm.value
+
+    # ---- learned preconditioner ----
+    def attach_unet(self, net, dims=None, p_of_vox=None):
+        """Use ``net`` (a ``UNet``) as the learned preconditioner on the
+        pressure grid ``dims`` (default: a cube); None detaches."""
+        if net is None:
+            self._check(self.L.cfd_unet_attach(self.h, None, None, None))
+            self._unet = None
+            return
+        i = self.info or self.refresh()
+        if dims is None:
+            m = round(i.NNp ** (1 / 3))
+            dims = (m, m, m)
+        d = np.ascontiguousarray(dims, dtype=np.int32)
+        pm = None if p_of_vox is None else np.ascontiguousarray(p_of_vox, dtype=np.int32)
+        self._check(self.L.cfd_unet_attach(self.h, net.h, _p(d, C.c_int), None if pm is None else _p(pm, C.c_int)))
+        self._unet = net  # keep it alive while attached
+
+    def load_unet(self, path: str, dims=None):
+        d = None if dims is None else np.ascontiguousarray(dims, dtype=np.int32)
+        self._check(self.L.cfd_unet_load(self.h, path.encode(), None if d is None else _p(d, C.c_int)))
+
     # ---- timing / counters ----
-    KCLASS = ["convect", "step1", "gt", "pcg64", "pcg32", "resid64", "step3", "spmv_k3", "pupdate", "other"]
+    KCLASS = ["convect", "step1", "gt", "pcg64", "pcg32", "resid64", "step3", "spmv_k3", "pupdate", "other",
+              "unet", "fcg"]
 
     @property
     def stream_ptr(self) -> int:
@@ -424,6 +490,117 @@ class Solver:
         nodes = np.ascontiguousarray(nodes, dtype=np.int32)
         uvw = np.ascontiguousarray(uvw, dtype=np.float64)
         self._check(self.L.cfd_set_bc_values(self.h, len(nodes), _p(nodes, C.c_int), _p(uvw, C.c_double)))
+
+
+class UNet:
+    """The learned pressure preconditioner's network (cfd_unet): a 3-level 3D
+    conv U-Net with BF16 weights / activations and FP32 accumulation, trained
+    by the library's own forward and backward kernels."""
+
+    def __init__(self, device: int = -1, seed: int = 0, path: str | None = None):
+        L = lib()
+        h = C.c_void_p()
+        rc = L.cfd_unet_create(C.byref(h), device, seed)
+        if rc != CFD_OK:
+            raise CfdError(rc, "cfd_unet_create failed (no usable CUDA device?)")
+        self.h, self.L = h, L
+        self.nparam = int(L.cfd_unet_param_count())
+        if path:
+            self.read(path)
+
+    def _check(self, rc: int):
+        if rc != CFD_OK:
+            raise CfdError(rc, self.L.cfd_unet_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.cfd_unet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def param_count() -> int:
+        return int(lib().cfd_unet_param_count())
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.nparam, dtype=np.float32)
+        self._check(self.L.cfd_unet_get_params(self.h, _p(out, C.c_float), self.nparam))
+        return out
+
+    def set_params(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(self.L.cfd_unet_set_params(self.h, _p(w, C.c_float), len(w)))
+
+    def save(self, path: str):
+        self._check(self.L.cfd_unet_save(self.h, path.encode()))
+
+    def read(self, path: str):
+        self._check(self.L.cfd_unet_read(self.h, path.encode()))
+
+    def set_loss(self, w_l2: float = 1.0, w_h1: float = 0.0):
+        """Training loss weights (mean squared error, neighbour-difference term)."""
+        self._check(self.L.cfd_unet_set_loss(self.h, w_l2, w_h1))
+
+    @staticmethod
+    def _dims(dims):
+        return np.ascontiguousarray(dims, dtype=np.int32)
+
+    def forward(self, x, dims=None):
+        """f(x) for one grid; x is a (nz, ny, nx) float array (host)."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        d = self._dims(dims if dims is not None else x.shape[::-1])
+        y = np.zeros_like(x)
+        self._check(self.L.cfd_unet_forward(self.h, _p(d, C.c_int), x.ctypes.data, y.ctypes.data, 0))
+        return y
+
+    TENSOR_CH = (1, 16, 32, 32, 64, 64, 64, 32, 32, 32, 16, 16, 16, 1)
+    TENSOR_LEVEL = (0, 0, 1, 1, 2, 2, 2, 2, 1, 1, 1, 0, 0, 0)
+
+    def tensor(self, t: int, dims):
+        """Stored tensor t of the last forward pass on grid dims, shaped
+        (nz, ny, nx, ch) at its level."""
+        d = [int(v) for v in dims]
+        for _ in range(self.TENSOR_LEVEL[t]):
+            d = [(v - 1) // 2 + 1 for v in d]
+        n = d[0] * d[1] * d[2] * self.TENSOR_CH[t]
+        out = np.zeros(n, dtype=np.float32)
+        self._check(self.L.cfd_unet_tensor(self.h, t, _p(out, C.c_float), n))
+        return out.reshape(d[2], d[1], d[0], self.TENSOR_CH[t])
+
+    def forward_device(self, x_ptr: int, y_ptr: int, dims):
+        d = self._dims(dims)
+        self._check(self.L.cfd_unet_forward(self.h, _p(d, C.c_int), x_ptr, y_ptr, 1))
+
+    def gradient(self, x, t, dims=None):
+        """(loss, dloss/dparams) of one host sample."""
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        d = self._dims(dims if dims is not None else x.shape[::-1])
+        g = np.zeros(self.nparam, dtype=np.float32)
+        loss = C.c_float()
+        self._check(self.L.cfd_unet_gradient(self.h, _p(d, C.c_int), x.ctypes.data, t.ctypes.data, 0,
+                                             C.byref(loss), _p(g, C.c_float)))
+        return float(loss.value), g
+
+    def train_batch(self, x, t, dims, lr: float, on_device: bool = False, nb: int | None = None) -> float:
+        """One Adam step on nb samples.  Host arrays (nb, nz, ny, nx), or with
+        on_device=True integer device addresses of nb consecutive grids."""
+        d = self._dims(dims)
+        loss = C.c_float()
+        if on_device:
+            self._check(self.L.cfd_unet_train_batch(self.h, _p(d, C.c_int), int(nb), x, t, 1, lr, C.byref(loss)))
+        else:
+            x = np.ascontiguousarray(x, dtype=np.float32)
+            t = np.ascontiguousarray(t, dtype=np.float32)
+            self._check(self.L.cfd_unet_train_batch(self.h, _p(d, C.c_int), x.shape[0], x.ctypes.data,
+                                                    t.ctypes.data, 0, lr, C.byref(loss)))
+        return float(loss.value)
 
 
 NOALLOC_MAX_N = 524288

@@ -1,0 +1,269 @@
+"""Learned pressure preconditioner: training data from the solver's own
+pressure solves, and training of the U-Net on the GPU with the library's
+forward and backward kernels.
+
+Data.  For a right-hand side R2 met during a run, a FP64 Jacobi-PCG solve to
+||r|| <= 1e-12 ||R2|| gives x*; Jacobi-PCG stopped after k iterations gives
+x_k (x_0 = 0); each pair is (r_k = R2 - Z x_k, e_k = x* - x_k).  Network
+input x = r_k / s and target t = e_k * d / s, with s = RMS(r_k) and d the
+median diagonal entry of Z, so that neither the residual's size nor the
+mesh spacing reaches the network (flexible CG is invariant to the scale of
+the preconditioned vector, so inference needs no rescaling).  Cavity runs
+draw Re ~ U[100, 1000] and lid speed ~ U[0.5, 1.5] from
+numpy.random.Generator(PCG64(seed)); duct runs use the bent duct with a
+parabolic inlet.
+
+Run ``python -m cfdfs.learned --out weights.bin`` on a GPU machine; it
+writes the weights and a JSON log of the data, the loss curve and the
+flexible-CG evaluation.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+
+from . import FP64, MIXED, PC_JACOBI, PC_LEARNED, HostMesh, Solver, UNet, meshgen
+
+KS = (0, 3, 10, 30, 100)  # Jacobi-PCG iterations of the x_k in each pair
+
+
+def cavity_params(seed: int):
+    """(Re, lid speed) of a seeded cavity run."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return float(rng.uniform(100.0, 1000.0)), float(rng.uniform(0.5, 1.5))
+
+
+class PairSampler:
+    """Two FP64 contexts on one deck: ``run`` advances the flow, ``pair``
+    solves for the pairs (so the running state is never disturbed)."""
+
+    def __init__(self, deck: str, dims, device: int = 0, inlet=None):
+        self.dims = tuple(dims)
+        self.run = Solver(device=device, precision=FP64)
+        self.run.load(deck)
+        self.run.step0()
+        if inlet is not None:
+            self.run.set_bc_values(*inlet)
+        self.pair = Solver(device=device, precision=FP64, cg_rtol=1e-12, cg_maxit=20000)
+        self.pair.load(deck)
+        self.pair.step0()
+        rp, col, val = self.pair.matrix("Z")
+        rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+        diag = val[col == rows]
+        self.dscale = float(np.median(diag))
+        self.n = len(rp) - 1
+        assert int(np.prod(self.dims)) == self.n
+
+    def close(self):
+        self.run.close()
+        self.pair.close()
+
+    def advance(self, nsteps: int, iters=(1, 2)):
+        """Runs nsteps time steps; returns the R2 of the given sub-iterations
+        of the last one."""
+        if nsteps > 1:
+            self.run.run(nsteps - 1)
+        got = []
+        self.run.time_step(after_step2=lambda it: got.append(self.run.vector("R2")) if it in iters else None)
+        return got
+
+    def pairs(self, rhs, ks=KS):
+        """Normalised (input, target) pairs, float32 arrays shaped (nz, ny, nx)."""
+        out = []
+        if not np.any(rhs):
+            return out
+        self.pair.set_options(cg_rtol=1e-12, cg_maxit=20000)
+        xs, st = self.pair.pressure_solve(rhs)
+        shape = self.dims[::-1]
+        for k in ks:
+            if k == 0:
+                xk = np.zeros(self.n)
+            else:
+                self.pair.set_options(cg_maxit=k)
+                xk, _ = self.pair.pressure_solve(rhs)
+            r, nr = self.pair.pressure_residual(rhs, xk)
+            if nr == 0.0:
+                continue
+            s = nr / np.sqrt(self.n)
+            x = (r / s).astype(np.float32).reshape(shape)
+            t = ((xs - xk) * (self.dscale / s)).astype(np.float32).reshape(shape)
+            out.append((x, t))
+        return out
+
+
+def cavity_pairs(seeds, n=64, dt=0.002, snap_steps=(1, 5, 15, 35, 70, 100), device=0, tmpdir=None, log=None):
+    """Pairs from seeded cavity runs; returns (x, t) stacked arrays."""
+    xs, ts = [], []
+    tmpdir = tmpdir or tempfile.mkdtemp()
+    for seed in seeds:
+        re, lid = cavity_params(seed)
+        deck = meshgen.write_cavity(os.path.join(tmpdir, f"cav_{seed}.inp"),
+                                    meshgen.CavitySpec(n, re=re, dt=dt, steps=max(snap_steps), ngp=8, lid=lid))
+        ps = PairSampler(deck, (n + 1,) * 3, device=device)
+        done = 0
+        for stp in snap_steps:
+            for rhs in ps.advance(stp - done):
+                for x, t in ps.pairs(rhs):
+                    xs.append(x)
+                    ts.append(t)
+            done = stp
+        ps.close()
+        if log is not None:
+            log.append(dict(source="cavity", seed=seed, re=re, lid=lid, pairs=len(xs)))
+    return np.stack(xs), np.stack(ts)
+
+
+def duct_pairs(n_cross=24, n_axial=160, dt=0.005, snap_steps=(1, 10, 30, 60, 100, 150, 200, 250, 300, 301),
+               device=0, tmpdir=None, log=None):
+    tmpdir = tmpdir or tempfile.mkdtemp()
+    deck = meshgen.write_duct(os.path.join(tmpdir, "duct.inp"), n_cross=n_cross, n_axial=n_axial, dt=dt,
+                              steps=max(snap_steps))
+    hm = HostMesh(deck)
+    inlet = meshgen.duct_inlet_profile(hm)
+    hm.close()
+    ps = PairSampler(deck, meshgen.duct_grid_dims(n_cross, n_axial), device=device, inlet=inlet)
+    xs, ts = [], []
+    done = 0
+    for stp in snap_steps:
+        for rhs in ps.advance(stp - done):
+            for x, t in ps.pairs(rhs):
+                xs.append(x)
+                ts.append(t)
+        done = stp
+    ps.close()
+    if log is not None:
+        log.append(dict(source="duct", n_cross=n_cross, n_axial=n_axial, pairs=len(xs)))
+    return np.stack(xs), np.stack(ts)
+
+
+def train(net: UNet, sets, budget_s: float, lr0=1e-3, batch=4, seed=0, log=None):
+    """Adam with cosine-decayed learning rate for budget_s seconds over the
+    given data sets [(x_dev, t_dev, dims, count)] (torch CUDA tensors hold
+    the data; the library reads them through their device addresses).
+    Batches alternate between sets in proportion to their sizes."""
+    rng = np.random.default_rng(seed)
+    sizes = np.array([s[3] for s in sets], dtype=np.float64)
+    t0 = time.time()
+    step = 0
+    curve = []
+    while True:
+        el = time.time() - t0
+        if el >= budget_s:
+            break
+        lr = lr0 * 0.5 * (1 + np.cos(np.pi * el / budget_s)) + 1e-5
+        k = rng.choice(len(sets), p=sizes / sizes.sum())
+        x, t, dims, cnt = sets[k]
+        i0 = int(rng.integers(0, cnt - batch + 1))
+        nv = int(np.prod(dims))
+        loss = net.train_batch(x.data_ptr() + 4 * i0 * nv, t.data_ptr() + 4 * i0 * nv, dims, lr, on_device=True,
+                               nb=batch)
+        step += 1
+        if step % 25 == 0:
+            curve.append((round(el, 2), step, k, float(loss)))
+    if log is not None:
+        log["train_curve"] = curve
+        log["train_steps"] = step
+    return step
+
+
+def eval_loss(net: UNet, x, t, dims):
+    """Mean loss over host pairs (no update)."""
+    tot = 0.0
+    for i in range(len(x)):
+        tot += net.gradient(x[i], t[i], dims)[0]
+    return tot / max(1, len(x))
+
+
+def fcg_eval(net_path: str | None, deck: str, steps: int, precision: int, dims=None, inlet=None, device=0):
+    """Pressure-CG iterations and wall time per step of a run, with the
+    learned preconditioner (net_path) or Jacobi-PCG (None)."""
+    s = Solver(device=device, precision=precision, precond=PC_LEARNED if net_path else PC_JACOBI)
+    s.load(deck)
+    s.step0()
+    if inlet is not None:
+        s.set_bc_values(*inlet)
+    if net_path:
+        s.load_unet(net_path, dims)
+    s.run(1)  # warm-up step
+    t0 = time.time()
+    st = s.run(steps)
+    el = time.time() - t0
+    res = dict(steps=st.steps, cg_iters=int(st.cg_iters), subiters=int(st.subiters),
+               its_per_solve=st.cg_iters / max(1, st.subiters), ms_per_step=1e3 * el / max(1, st.steps))
+    s.close()
+    return res
+
+
+def main(argv=None):
+    import torch
+
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--out", required=True, help="weight file to write")
+    ap.add_argument("--log", default=None, help="JSON log (default: <out>.json)")
+    ap.add_argument("--train-seeds", type=int, default=30)
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--budget", type=float, default=300.0, help="training seconds")
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--w-h1", type=float, default=0.0)
+    ap.add_argument("--no-duct", action="store_true")
+    ap.add_argument("--eval-steps", type=int, default=10)
+    ap.add_argument("--init", default=None, help="start from these weights")
+    a = ap.parse_args(argv)
+    log = dict(args=vars(a), data=[])
+    t0 = time.time()
+    cx, ct = cavity_pairs(range(a.train_seeds), n=a.n, log=log["data"])
+    log["cavity_pairs"] = len(cx)
+    perm = np.random.default_rng(0).permutation(len(cx))  # batches are contiguous runs of pairs
+    cx, ct = cx[perm], ct[perm]
+    sets = []
+    dims_c = (a.n + 1,) * 3
+    # hold out the last 5% of cavity pairs for a validation loss
+    nval = max(1, len(cx) // 20)
+    vx, vt = cx[-nval:], ct[-nval:]
+    sets.append((torch.from_numpy(cx[:-nval]).cuda(), torch.from_numpy(ct[:-nval]).cuda(), dims_c, len(cx) - nval))
+    if not a.no_duct:
+        dx, dt_ = duct_pairs(log=log["data"])
+        log["duct_pairs"] = len(dx)
+        perm = np.random.default_rng(1).permutation(len(dx))
+        dx, dt_ = dx[perm], dt_[perm]
+        sets.append((torch.from_numpy(dx).cuda(), torch.from_numpy(dt_).cuda(), meshgen.duct_grid_dims(), len(dx)))
+    log["data_seconds"] = time.time() - t0
+    del cx, ct
+    net = UNet(device=0, seed=1234)
+    if a.init:
+        net.read(a.init)
+    net.set_loss(1.0, a.w_h1)
+    log["val_loss_init"] = eval_loss(net, vx, vt, dims_c)
+    t1 = time.time()
+    train(net, sets, a.budget, lr0=a.lr, batch=a.batch, log=log)
+    log["train_seconds"] = time.time() - t1
+    log["val_loss"] = eval_loss(net, vx, vt, dims_c)
+    net.save(a.out)
+    # held-out evaluation: the 64^3 benchmark cavity (Re 1000, lid 1) and an
+    # unseen seed, FP64 and mixed, learned vs Jacobi
+    tmp = tempfile.mkdtemp()
+    ev = {}
+    decks = {"c3_re1000": meshgen.write_cavity(os.path.join(tmp, "c3.inp"),
+                                               meshgen.CavitySpec(a.n, re=1000, dt=0.002, steps=100, ngp=8))}
+    re, lid = cavity_params(10_000)
+    decks["seed10000"] = meshgen.write_cavity(os.path.join(tmp, "h.inp"),
+                                              meshgen.CavitySpec(a.n, re=re, dt=0.002, steps=100, ngp=8, lid=lid))
+    for name, deck in decks.items():
+        for prec, pname in ((FP64, "fp64"), (MIXED, "mixed")):
+            ev[f"{name}_{pname}_jacobi"] = fcg_eval(None, deck, a.eval_steps, prec)
+            ev[f"{name}_{pname}_learned"] = fcg_eval(a.out, deck, a.eval_steps, prec, dims_c)
+    log["eval"] = ev
+    with open(a.log or a.out + ".json", "w") as f:
+        json.dump(log, f, indent=1)
+    print(json.dumps(dict(val_loss_init=log["val_loss_init"], val_loss=log["val_loss"],
+                          steps=log["train_steps"], eval=ev), indent=1))
+
+
+if __name__ == "__main__":
+    main()

@@ -305,6 +305,29 @@ def duct_deck(n_cross: int = 24, n_axial: int = 160, re: float = 200.0, dt: floa
     return buf.getvalue()
 
 
+def duct_inlet_profile(mesh, peak: float = 1.0, side: float = 1.0):
+    """Per-node parabolic inlet velocity of a duct deck: the nodes that keep
+    BC 1 (0-based id 0 in ``HostMesh.bcnodes``; wall nodes on the inlet rim
+    belong to BC 2) get
+    u = peak (1 - (2y/side)^2) (1 - (2z/side)^2) along +x, v = w = 0.
+    ``mesh`` is a ``cfdfs.HostMesh`` of the deck.  Returns (nodes, uvw) for
+    ``Solver.set_bc_values``."""
+    bc = mesh.bcnodes()
+    xyz = mesh.coord()
+    nodes = bc[bc[:, 1] == 0, 0].astype(np.int32)
+    y, z = xyz[nodes, 1] / (0.5 * side), xyz[nodes, 2] / (0.5 * side)
+    u = peak * np.clip(1.0 - y * y, 0.0, None) * np.clip(1.0 - z * z, 0.0, None)
+    uvw = np.zeros((len(nodes), 3))
+    uvw[:, 0] = u
+    return nodes, uvw
+
+
+def duct_grid_dims(n_cross: int = 24, n_axial: int = 160):
+    """Pressure-node grid (nx, ny, nz) of ``duct_arrays``: corner nodes are
+    numbered axial index fastest, then across in-plane, then across z."""
+    return (n_axial + 1, n_cross + 1, n_cross + 1)
+
+
 def write_duct(path: str, **kw) -> str:
     text = duct_deck(**kw)
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)

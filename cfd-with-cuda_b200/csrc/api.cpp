@@ -20,7 +20,9 @@
 
 #include "../../include/cfdfs.h"
 #include "cuda/kernels.h"
+#include "cuda/unet.h"
 #include "host/problem.h"
+#include "host/unet_net.h"
 
 namespace cfd {
 int make_basis(int ngp, Basis& B);
@@ -30,6 +32,10 @@ int read_restart(const HostProblem& P, const std::string& path, double* U, doubl
 }  // namespace cfd
 
 using namespace cfd;
+
+struct cfd_unet {
+  UnetNet net;
+};
 
 namespace {
 
@@ -103,6 +109,16 @@ struct cfd_ctx {
   DevBuf<double> upart, ppart, norms, blk;
   int nub = 1, npb = 1;
   double* h_small = nullptr;  // pinned scratch for small readbacks (64 doubles)
+
+  // learned preconditioner: attached network, its grid and flexible-CG state
+  cfd_unet* unet = nullptr;
+  std::unique_ptr<cfd_unet> unet_owned;
+  int udims[3] = {0, 0, 0};
+  DevBuf<int> upmap;  // voxel -> pressure node (empty: identity)
+  DevBuf<double> fcg_sc, fcg_part;
+  DevBuf<int> fcg_done;
+  int fcg_window = 25;
+  double fcg_stall = 0.5;  // minimum residual reduction per window
 
   int timeN = 0;
   double timeT = 0, maxAcc = 0;
@@ -371,6 +387,95 @@ int run_pcg32(cfd_ctx* c, double rtol, int maxit, double* res) {
   return CFD_OK;
 }
 
+// Flexible CG with the attached U-Net.  VT = float: b, x are f_b, f_x and
+// the FP32 SELL values (inner solve of CFD_MIXED); VT = double: b, x are the
+// caller's FP64 vectors.  res = {iterations, ||r||/||b||, status} with the
+// status words of kernels.h (4 = stalled).
+template <class VT>
+int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, double* res) {
+  cudaStream_t s = c->stream;
+  const int n = c->P.NNp;
+  UnetNet& net = c->unet->net;
+  if (net.set_grid(c->udims, false)) return fail(c, CFD_E_NOMEM, "%s", net.err.c_str());
+  if (!c->fcg_sc.p) {
+    CU(c->fcg_sc.alloc(kFcgScalars));
+    CU(c->fcg_part.alloc(4 * (size_t)fcg_blocks(n)));
+    CU(c->fcg_done.alloc(1));
+  }
+  FcgArgs<VT> a{};
+  a.n = n;
+  a.off = c->zs_off.p;
+  a.col = c->zs_col.p;
+  VT* work;
+  if constexpr (sizeof(VT) == 4) {
+    a.val = c->zs_val32.p;
+    work = c->f_work.p;
+  } else {
+    a.val = c->zs_val.p;
+    work = c->cg_work.p;
+  }
+  a.b = b;
+  a.x = x;
+  a.r = work;
+  a.z = work + (size_t)n;
+  a.w = work + 2 * (size_t)n;
+  a.p = work + 3 * (size_t)n;
+  a.q = work + 4 * (size_t)n;
+  a.st.sc = c->fcg_sc.p;
+  a.st.part = c->fcg_part.p;
+  a.st.done = c->fcg_done.p;
+  a.st.rtol = rtol;
+  a.st.stall2 = c->fcg_stall * c->fcg_stall;
+  a.st.maxit = maxit;
+  a.st.window = c->fcg_window;
+  KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
+  c->launches++;
+  const int* pmap = c->upmap.p;
+  // the last layer writes z directly when no conversion or gather is needed
+  float* direct = nullptr;
+  if constexpr (sizeof(VT) == 4)
+    if (!pmap) direct = (float*)a.z;
+  int issued = 0, batch = 2;
+  double rr_prev = -1;
+  for (;;) {
+    for (int k = 0; k < batch; k++) {
+      const long long l0 = net.launches;
+      KL(CFD_K_UNET, ([&]() -> cudaError_t {
+           cudaError_t e = unet_input(n, a.r, pmap, a.st.sc + kFcgRR, 0.0, net.act[0], a.st.done, s);
+           if (e == cudaSuccess) e = net.forward(s, direct, a.st.done);
+           if (e == cudaSuccess && !direct) e = unet_output(n, net.out, pmap, a.z, a.st.done, s);
+           return e;
+         })());
+      c->launches += net.launches - l0 + (direct ? 0 : 1);
+      KL(CFD_K_FCG, launch_fcg_spmv<VT>(a, s));
+      KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
+      c->launches += 2;
+    }
+    issued += batch;
+    CU(cudaMemcpyAsync(c->h_small, c->fcg_sc.p, kFcgScalars * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    const double* h = c->h_small;
+    if (h[kFcgStatus] >= 0 || issued >= maxit) break;
+    // size the next batch from the observed convergence rate
+    const double rr = h[kFcgRR], target = rtol * rtol * h[kFcgBB];
+    int next = 4;
+    if (rr_prev > 0 && rr > 0 && rr < rr_prev) {
+      const double rate = std::log(rr / rr_prev) / batch;  // per iteration, < 0
+      next = (int)std::ceil(std::log(target / rr) / rate);
+    }
+    rr_prev = rr;
+    batch = std::max(1, std::min(next, 16));
+  }
+  const double* h = c->h_small;
+  res[0] = h[kFcgIt];
+  res[1] = h[kFcgBB] > 0 ? std::sqrt(h[kFcgRR] / h[kFcgBB]) : 0.0;
+  res[2] = h[kFcgStatus] < 0 ? 1 : h[kFcgStatus];
+  if (c->prof_on) c->prof[CFD_K_FCG][2] += res[0];
+  return CFD_OK;
+}
+
+bool learned(const cfd_ctx* c) { return c->opt.precond == CFD_PC_LEARNED && c->unet; }
+
 // ||b - Z x||_2 in FP64 (also leaves r in ir_r and (float) r in f_b).
 int residual_norm(cfd_ctx* c, const double* b, const double* x, double* out) {
   cudaStream_t s = c->stream;
@@ -391,9 +496,22 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
   const double rtol = c->opt.cg_rtol;
   if (c->opt.precision == CFD_FP64 || c->opt.precision != CFD_MIXED) {
     double res[4] = {0, 0, 0, 0};
-    int rc = run_pcg64(c, b, x, warm, rtol, c->opt.cg_maxit, res);
-    if (rc) return rc;
-    z.iterations = (int)res[0];
+    int used = 0;
+    if (learned(c)) {
+      int rc = run_fcg<double>(c, b, x, warm, rtol, c->opt.cg_maxit, res);
+      if (rc) return rc;
+      used = (int)res[0];
+      if ((int)res[2] != 0) {
+        // flexible CG stalled, broke down or ran out: Jacobi-PCG from its iterate
+        z.fallback = 1;
+        warm = 1;
+      }
+    }
+    if (!learned(c) || z.fallback) {
+      int rc = run_pcg64(c, b, x, warm, rtol, std::max(1, c->opt.cg_maxit - used), res);
+      if (rc) return rc;
+    }
+    z.iterations = used + (int)res[0];
     z.relres = res[1];
     z.status = (int)res[2];
   } else {
@@ -419,8 +537,16 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
         double res[4] = {0, 0, 0, 0};
         // inner target: inner_rtol relative, but no tighter than needed
         double inner = std::max(c->opt.inner_rtol, 0.5 * rtol * bnorm / rnorm);
-        rc = run_pcg32(c, inner, c->opt.cg_maxit - total, res);
-        if (rc) return rc;
+        if (learned(c) && !z.fallback) {
+          rc = run_fcg<float>(c, c->f_b.p, c->f_x.p, 0, inner, c->opt.cg_maxit - total, res);
+          if (rc) return rc;
+          const int fs = (int)res[2];
+          if (fs == 4 || fs == 2 || (fs == 1 && res[1] > 0.5)) z.fallback = 1;  // Jacobi-PCG from here on
+          if (fs == 2) res[2] = 0;  // the iterate is still finite: the outer residual decides
+        } else {
+          rc = run_pcg32(c, inner, c->opt.cg_maxit - total, res);
+          if (rc) return rc;
+        }
         total += (int)res[0];
         if ((int)res[2] == 3) { z.status = 3; break; }
         KL(CFD_K_OTHER, launch_axpy_f2d(c->P.NNp, c->f_x.p, x, s));
@@ -1036,9 +1162,291 @@ int cfd_selftest_wait_timeout(cfd_ctx* c, int timeout_ms) {
   return CFD_OK;
 }
 
-int cfd_unet_load(cfd_ctx* c, const char* path) {
+int cfd_unet_create(cfd_unet** out, int device, unsigned long long seed) {
+  if (!out) return CFD_E_BADARG;
+  *out = nullptr;
+  if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return CFD_E_CUDA;
+  std::unique_ptr<cfd_unet> u(new cfd_unet());
+  if (u->net.init(seed)) return CFD_E_CUDA;
+  *out = u.release();
+  return CFD_OK;
+}
+
+void cfd_unet_destroy(cfd_unet* u) {
+  if (!u) return;
+  cudaSetDevice(u->net.device);
+  cudaDeviceSynchronize();
+  delete u;
+}
+
+const char* cfd_unet_last_error(const cfd_unet* u) { return u ? u->net.err.c_str() : "null network"; }
+
+long long cfd_unet_param_count(void) { return unet_param_count(); }
+
+int cfd_unet_get_params(cfd_unet* u, float* out, long long n) {
+  if (!u || !out) return CFD_E_BADARG;
+  cudaSetDevice(u->net.device);
+  if (cudaStreamSynchronize(u->net.own_stream) != cudaSuccess) return CFD_E_CUDA;
+  return u->net.get_params(out, n) ? CFD_E_BADARG : CFD_OK;
+}
+
+int cfd_unet_set_params(cfd_unet* u, const float* in, long long n) {
+  if (!u || !in) return CFD_E_BADARG;
+  cudaSetDevice(u->net.device);
+  cudaDeviceSynchronize();
+  return u->net.set_params(in, n) ? CFD_E_BADARG : CFD_OK;
+}
+
+int cfd_unet_save(cfd_unet* u, const char* path) {
+  if (!u || !path) return CFD_E_BADARG;
+  std::vector<float> h((size_t)u->net.nparam);
+  int rc = cfd_unet_get_params(u, h.data(), u->net.nparam);
+  if (rc) return rc;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) {
+    u->net.err = std::string("cannot write ") + path;
+    return CFD_E_IO;
+  }
+  const long long n = u->net.nparam;
+  bool ok = std::fwrite("CFDUNET1", 1, 8, f) == 8 && std::fwrite(&n, sizeof(n), 1, f) == 1 &&
+            std::fwrite(h.data(), sizeof(float), h.size(), f) == h.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) u->net.err = std::string("short write to ") + path;
+  return ok ? CFD_OK : CFD_E_IO;
+}
+
+int cfd_unet_read(cfd_unet* u, const char* path) {
+  if (!u || !path) return CFD_E_BADARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    u->net.err = std::string("cannot open ") + path;
+    return CFD_E_IO;
+  }
+  char tag[8] = {0};
+  long long n = 0;
+  std::vector<float> h;
+  bool ok = std::fread(tag, 1, 8, f) == 8 && std::memcmp(tag, "CFDUNET1", 8) == 0 &&
+            std::fread(&n, sizeof(n), 1, f) == 1 && n == u->net.nparam;
+  if (ok) {
+    h.resize((size_t)n);
+    ok = std::fread(h.data(), sizeof(float), h.size(), f) == h.size();
+  }
+  std::fclose(f);
+  if (!ok) {
+    u->net.err = std::string("not a weight file of this network: ") + path;
+    return CFD_E_BADINPUT;
+  }
+  return cfd_unet_set_params(u, h.data(), n);
+}
+
+namespace {
+
+int unet_prepare(cfd_unet* u, const int* dims, bool train, long long* nv) {
+  if (!dims) return CFD_E_BADARG;
+  cudaSetDevice(u->net.device);
+  if (u->net.set_grid(dims, train)) return CFD_E_BADARG;
+  *nv = u->net.nvox[0];
+  return CFD_OK;
+}
+
+// act[0] <- bf16(x) for sample x (host or device FP32)
+int unet_load_input(cfd_unet* u, const float* x, long long nv, int on_device, float* dev_tmp) {
+  cudaStream_t s = u->net.own_stream;
+  const float* src = x;
+  if (!on_device) {
+    if (cudaMemcpyAsync(dev_tmp, x, nv * sizeof(float), cudaMemcpyHostToDevice, s)) return CFD_E_CUDA;
+    src = dev_tmp;
+  }
+  u->net.launches++;
+  return unet_input((int)nv, src, nullptr, nullptr, 1.0, u->net.act[0], nullptr, s) ? CFD_E_CUDA : CFD_OK;
+}
+
+}  // namespace
+
+int cfd_unet_forward(cfd_unet* u, const int dims[3], const float* x, float* y, int on_device) {
+  if (!u || !x || !y) return CFD_E_BADARG;
+  long long nv = 0;
+  int rc = unet_prepare(u, dims, false, &nv);
+  if (rc) return rc;
+  UnetNet& n = u->net;
+  cudaStream_t s = n.own_stream;
+  DevBuf<float> tmp;
+  if (!on_device && tmp.alloc(2 * (size_t)nv)) return CFD_E_NOMEM;
+  rc = unet_load_input(u, x, nv, on_device, tmp.p);
+  if (rc) return rc;
+  float* dst = on_device ? y : tmp.p + nv;
+  if (n.forward(s, dst) != cudaSuccess) return CFD_E_CUDA;
+  if (!on_device && cudaMemcpyAsync(y, dst, nv * sizeof(float), cudaMemcpyDeviceToHost, s)) return CFD_E_CUDA;
+  return cudaStreamSynchronize(s) == cudaSuccess ? CFD_OK : CFD_E_CUDA;
+}
+
+namespace {
+
+// forward + MSE + backward of one sample; gradients accumulate into G
+int unet_sample(cfd_unet* u, const float* x, const float* t, long long nv, int on_device, float* tmp) {
+  UnetNet& n = u->net;
+  cudaStream_t s = n.own_stream;
+  int rc = unet_load_input(u, x, nv, on_device, tmp);
+  if (rc) return rc;
+  const float* tg = t;
+  if (!on_device) {
+    if (cudaMemcpyAsync(tmp + nv, t, nv * sizeof(float), cudaMemcpyHostToDevice, s)) return CFD_E_CUDA;
+    tg = tmp + nv;
+  }
+  if (n.forward(s, nullptr) != cudaSuccess) return CFD_E_CUDA;
+  n.launches++;
+  if (unet_loss(n.dims[0], n.out, tg, n.grad[kUnetTensors - 1], n.lossv, n.w_l2, n.w_h1, s) != cudaSuccess)
+    return CFD_E_CUDA;
+  return n.backward(s) == cudaSuccess ? CFD_OK : CFD_E_CUDA;
+}
+
+}  // namespace
+
+int cfd_unet_gradient(cfd_unet* u, const int dims[3], const float* x, const float* t, int on_device, float* loss,
+                      float* grad) {
+  if (!u || !x || !t) return CFD_E_BADARG;
+  long long nv = 0;
+  int rc = unet_prepare(u, dims, true, &nv);
+  if (rc) return rc;
+  UnetNet& n = u->net;
+  cudaStream_t s = n.own_stream;
+  DevBuf<float> tmp;
+  if (!on_device && tmp.alloc(2 * (size_t)nv)) return CFD_E_NOMEM;
+  if (cudaMemsetAsync(n.G, 0, n.nparam * sizeof(float), s) || cudaMemsetAsync(n.lossv, 0, sizeof(float), s))
+    return CFD_E_CUDA;
+  rc = unet_sample(u, x, t, nv, on_device, tmp.p);
+  if (rc) return rc;
+  if (cudaMemcpyAsync(n.h_pinned, n.lossv, sizeof(float), cudaMemcpyDeviceToHost, s)) return CFD_E_CUDA;
+  if (grad && cudaMemcpyAsync(grad, n.G, n.nparam * sizeof(float), cudaMemcpyDeviceToHost, s)) return CFD_E_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return CFD_E_CUDA;
+  if (loss) *loss = n.h_pinned[0];
+  return CFD_OK;
+}
+
+int cfd_unet_tensor(cfd_unet* u, int t, float* out, long long n) {
+  if (!u || !out || t < 0 || t >= kUnetTensors) return CFD_E_BADARG;
+  UnetNet& net = u->net;
+  const long long need = net.nvox[kUnetTensor[t].level] * kUnetTensor[t].ch;
+  if (n != need || need == 0) {
+    net.err = "tensor size mismatch (or no forward pass yet)";
+    return CFD_E_BADARG;
+  }
+  cudaSetDevice(net.device);
+  if (cudaStreamSynchronize(net.own_stream) != cudaSuccess) return CFD_E_CUDA;
+  if (t == kUnetTensors - 1)
+    return cudaMemcpy(out, net.out, n * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess ? CFD_OK : CFD_E_CUDA;
+  std::vector<uint16_t> h((size_t)n);
+  if (cudaMemcpy(h.data(), net.act[t], n * sizeof(uint16_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return CFD_E_CUDA;
+  for (long long i = 0; i < n; i++) {
+    const uint32_t b = (uint32_t)h[(size_t)i] << 16;
+    std::memcpy(out + i, &b, sizeof(float));
+  }
+  return CFD_OK;
+}
+
+int cfd_unet_set_loss(cfd_unet* u, float w_l2, float w_h1) {
+  if (!u || !(w_l2 >= 0) || !(w_h1 >= 0) || w_l2 + w_h1 <= 0) return CFD_E_BADARG;
+  u->net.w_l2 = w_l2;
+  u->net.w_h1 = w_h1;
+  return CFD_OK;
+}
+
+int cfd_unet_train_batch(cfd_unet* u, const int dims[3], int nb, const float* x, const float* t, int on_device,
+                         float lr, float* loss) {
+  if (!u || !x || !t || nb < 1 || !(lr > 0)) return CFD_E_BADARG;
+  long long nv = 0;
+  int rc = unet_prepare(u, dims, true, &nv);
+  if (rc) return rc;
+  UnetNet& n = u->net;
+  cudaStream_t s = n.own_stream;
+  DevBuf<float> tmp;
+  if (!on_device && tmp.alloc(2 * (size_t)nv)) return CFD_E_NOMEM;
+  if (cudaMemsetAsync(n.G, 0, n.nparam * sizeof(float), s) || cudaMemsetAsync(n.lossv, 0, sizeof(float), s))
+    return CFD_E_CUDA;
+  for (int i = 0; i < nb; i++) {
+    rc = unet_sample(u, x + (size_t)i * nv, t + (size_t)i * nv, nv, on_device, tmp.p);
+    if (rc) return rc;
+  }
+  if (n.adam(s, lr, 1.0f / nb) != cudaSuccess) return CFD_E_CUDA;
+  if (cudaMemcpyAsync(n.h_pinned, n.lossv, sizeof(float), cudaMemcpyDeviceToHost, s)) return CFD_E_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return CFD_E_CUDA;
+  if (loss) *loss = n.h_pinned[0] / nb;
+  return CFD_OK;
+}
+
+int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_vox) {
+  if (!c) return CFD_E_BADARG;
+  if (!u) {
+    c->unet = nullptr;
+    c->unet_owned.reset();
+    return CFD_OK;
+  }
+  NEED(c->loaded, "cfd_unet_attach before the problem is loaded");
+  NEED(dims, "cfd_unet_attach needs the grid dims");
+  NEED(u->net.device == c->device, "network and context live on different devices");
+  const long long nv = (long long)dims[0] * dims[1] * dims[2];
+  NEED(nv == c->P.NNp, "grid dims do not multiply to the number of pressure nodes");
+  if (u->net.set_grid(dims, false)) return fail(c, CFD_E_BADARG, "%s", u->net.err.c_str());
+  c->upmap.reset();
+  if (p_of_vox) {
+    std::vector<char> seen(nv, 0);
+    for (long long v = 0; v < nv; v++) {
+      NEED(p_of_vox[v] >= 0 && p_of_vox[v] < nv && !seen[p_of_vox[v]], "p_of_vox is not a permutation");
+      seen[p_of_vox[v]] = 1;
+    }
+    CU(c->upmap.alloc(nv));
+    CU(cudaMemcpyAsync(c->upmap.p, p_of_vox, nv * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+  }
+  for (int a = 0; a < 3; a++) c->udims[a] = dims[a];
+  if (c->unet_owned.get() != u) c->unet_owned.reset();
+  c->unet = u;
+  return CFD_OK;
+}
+
+int cfd_unet_load(cfd_ctx* c, const char* path, const int dims[3]) {
   if (!c || !path) return CFD_E_BADARG;
-  return fail(c, CFD_E_BADARG, "learned preconditioner weights are not supported by this build yet");
+  NEED(c->loaded, "cfd_unet_load before the problem is loaded");
+  int d[3];
+  if (dims) {
+    for (int a = 0; a < 3; a++) d[a] = dims[a];
+  } else {
+    int m = (int)std::llround(std::cbrt((double)c->P.NNp));
+    NEED((long long)m * m * m == c->P.NNp, "pressure nodes do not form a cube: pass the grid dims");
+    d[0] = d[1] = d[2] = m;
+  }
+  CU(cudaSetDevice(c->device));
+  cfd_unet* u = nullptr;
+  int rc = cfd_unet_create(&u, c->device, 0);
+  if (rc) return fail(c, rc, "cannot create the network");
+  std::unique_ptr<cfd_unet> own(u);
+  rc = cfd_unet_read(u, path);
+  if (rc) return fail(c, rc, "%s", u->net.err.c_str());
+  c->unet_owned.reset();
+  rc = cfd_unet_attach(c, u, d, nullptr);
+  if (rc) return rc;
+  c->unet_owned = std::move(own);
+  return CFD_OK;
+}
+
+int cfd_pressure_residual(cfd_ctx* c, const double* rhs, const double* x, double* r, double* norm) {
+  if (!c || !rhs || !x || !r) return CFD_E_BADARG;
+  NEED(c->assembled, "cfd_pressure_residual before cfd_step0");
+  cudaStream_t s = c->stream;
+  const size_t NNp = c->P.NNp;
+  DevBuf<double> db, dx;
+  CU(db.alloc(NNp));
+  CU(dx.alloc(NNp));
+  CU(cudaMemcpyAsync(db.p, rhs, NNp * sizeof(double), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(dx.p, x, NNp * sizeof(double), cudaMemcpyHostToDevice, s));
+  double nr = 0;
+  int rc = residual_norm(c, db.p, dx.p, &nr);
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(r, c->ir_r.p, NNp * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (norm) *norm = nr;
+  return CFD_OK;
 }
 
 }  // extern "C"

@@ -152,6 +152,28 @@ struct PcgArgs {
   unsigned long long timeout_ns;
 };
 // Block ranges each PCG block gathers from, for a given grid (host).
+// Flexible CG on the SELL-32 pressure matrix (fcg.cu).  State words in
+// sc[]: indices below; status -1 running, 0 converged, 1 iteration limit,
+// 2 non-finite, 4 stalled (the residual fell by less than sqrt(stall2) over
+// the last window iterations, or the direction broke down).
+enum { kFcgRR = 0, kFcgBB, kFcgPQ, kFcgAlpha, kFcgBeta, kFcgIt, kFcgStatus, kFcgRRMark, kFcgScalars = 8 };
+struct FcgState {
+  double* sc;    // kFcgScalars words
+  double* part;  // 4 x blocks
+  int* done;     // kernels return at once while *done != 0
+  double rtol, stall2;
+  int maxit, window;
+};
+template <class VT> struct FcgArgs {
+  int n; const int *off, *col; const VT* val; const VT* b;
+  VT *x, *r, *z, *w, *p, *q;
+  FcgState st;
+};
+int fcg_blocks(int n);
+template <class VT> cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s);
+template <class VT> cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s);
+template <class VT> cudaError_t launch_fcg_update(const FcgArgs<VT>& a, cudaStream_t s);
+
 void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi);
 template <class VT>
 cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s);

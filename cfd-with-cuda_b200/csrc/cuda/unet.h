@@ -1,0 +1,84 @@
+// Learned pressure preconditioner: a 3-level 3D convolutional U-Net on the
+// structured grid of pressure nodes (hand-written CUDA forward and backward
+// kernels; BF16 weights and activations, FP32 accumulation and gradients).
+//
+// Grid levels: L0 = (nx, ny, nz) pressure nodes, L1 = ((n-1)/2 + 1) per axis
+// (every other node), L2 likewise.  Activations are channels-last
+// (voxel-major, channels contiguous), voxel v = x + nx (y + ny z).
+//
+// The layer list lives in the host network (unet_net.h); these are its
+// building blocks.  Activation: leaky ReLU, slope 0.1.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace cfd {
+
+constexpr float kLeaky = 0.1f;
+
+struct ConvDesc {
+  int in_dims[3], out_dims[3];
+  int stride;                 // 1 or 2
+  const __nv_bfloat16* inA;   // channels-last, ca channels
+  int ca;
+  const __nv_bfloat16* inB;   // optional second input (concatenated channels), cb channels
+  int cb;
+  int cout;
+  const __nv_bfloat16* w;     // [27][ca+cb][cout]
+  const float* bias;          // [cout]
+  __nv_bfloat16* out;         // bf16 output (or null)
+  float* out_f32;             // FP32 output (or null)
+  int act;                    // 1: leaky ReLU
+  const int* skip;            // optional device flag: the kernel does nothing while *skip != 0
+};
+
+cudaError_t conv3_forward(const ConvDesc& d, cudaStream_t s);
+
+// dIn = conv^T(dOut, W): writes FP32 gradients of inA (dA, ca channels) and inB
+// (dB, cb channels); accumulate into existing values when acc* != 0.
+cudaError_t conv3_dgrad(const ConvDesc& d, const float* dout, float* dA, int accA, float* dB, int accB,
+                        cudaStream_t s);
+// dW[k][ci][co] += sum_v in[s v + off_k][ci] dOut[v][co],  db[co] += sum_v dOut[v][co]
+cudaError_t conv3_wgrad(const ConvDesc& d, const float* dout, float* dw, float* db, cudaStream_t s);
+
+// dy *= leaky'(y) (derivative from the sign of the stored output y)
+cudaError_t act_backward(long long n, const __nv_bfloat16* y, float* dy, cudaStream_t s);
+
+// out = P(in) + skip: vertex-centred trilinear prolongation from coarse dims c
+// to fine dims f = 2c - 1 (ch channels), plus an optional fine skip tensor.
+cudaError_t upsample_forward(const int* cdims, const int* fdims, int ch, const __nv_bfloat16* in,
+                             const __nv_bfloat16* skip, __nv_bfloat16* out, const int* skipflag, cudaStream_t s);
+// transpose of upsample_forward: coarse gradient += R(fine gradient)
+cudaError_t upsample_backward(const int* cdims, const int* fdims, int ch, const float* dfine, float* dcoarse,
+                              cudaStream_t s);
+
+// dst += src (FP32)
+cudaError_t add_f32(long long n, const float* src, float* dst, cudaStream_t s);
+
+// Network input x[v] = bf16(r[p(v)] * c), v over the nv grid voxels, p(v) =
+// p_of_vox[v] (identity when null).  c = sqrt(nv / rr[0]) when rr is given
+// (unit-RMS scaling by the residual's squared norm; 0 if rr[0] <= 0), else
+// c = scale.  skipflag as in ConvDesc.
+cudaError_t unet_input(int nv, const double* r, const int* p_of_vox, const double* rr, double scale,
+                       __nv_bfloat16* x, const int* skipflag, cudaStream_t s);
+cudaError_t unet_input(int nv, const float* r, const int* p_of_vox, const double* rr, double scale,
+                       __nv_bfloat16* x, const int* skipflag, cudaStream_t s);
+// z[p(v)] = out[v]
+cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, double* z, const int* skipflag,
+                        cudaStream_t s);
+cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, float* z, const int* skipflag,
+                        cudaStream_t s);
+
+// Training loss of one sample on grid dims, d = out - target:
+//   w_l2 mean(d^2) + w_h1 (1/n) sum over axes of (d[i+e] - d[i])^2
+// (neighbour pairs inside the grid); dout = its gradient, lossv[0] += loss.
+cudaError_t unet_loss(const int* dims, const float* out, const float* target, float* dout, float* lossv, float w_l2,
+                      float w_h1, cudaStream_t s);
+
+// Adam step on FP32 master weights, refreshing the BF16 copy.
+cudaError_t adam_step(long long n, float* w, const float* g, float* m, float* v, __nv_bfloat16* wb, float lr,
+                      float b1, float b2, float eps, int t, float gscale, cudaStream_t s);
+
+cudaError_t f32_to_bf16(long long n, const float* a, __nv_bfloat16* b, cudaStream_t s);
+
+}  // namespace cfd

@@ -197,10 +197,59 @@ int cfd_read_restart(cfd_ctx* ctx, const char* path);
  * (e.g. a parabolic duct inlet): n entries of node ids and 3n values. */
 int cfd_set_bc_values(cfd_ctx* ctx, int n, const int* nodes, const double* uvw);
 
-/* ---- learned preconditioner ----------------------------------------------- */
-
-/* Loads U-Net weights (raw file written by cfd_unet_save / the trainer). */
-int cfd_unet_load(cfd_ctx* ctx, const char* path);
+/* ---- learned preconditioner -------------------------------------------------
+ * No counterpart in the reference.  A 3-level 3D convolutional U-Net on the
+ * structured grid of pressure nodes maps a residual r (scaled to unit RMS)
+ * to an approximation of the error Z^-1 r; with precond = CFD_PC_LEARNED the
+ * pressure solve runs flexible CG with it (inner FP32 solves under
+ * CFD_MIXED, FP64 otherwise) and falls back to Jacobi-PCG for the rest of
+ * the solve when flexible CG stalls (cfd_solve_stats.fallback = 1).
+ * Grids are nx x ny x nz voxels in x-fastest order with (n - 1) % 4 == 0 and
+ * n >= 5 on every axis.  BF16 weights and activations, FP32 accumulation,
+ * FP32 gradients and Adam state. */
+typedef struct cfd_unet cfd_unet;
+/* A network with seeded He-normal weights on the current CUDA device (device
+ * < 0) or the given one. */
+int cfd_unet_create(cfd_unet** out, int device, unsigned long long seed);
+void cfd_unet_destroy(cfd_unet* net);
+const char* cfd_unet_last_error(const cfd_unet* net);
+long long cfd_unet_param_count(void);
+/* FP32 parameters in layer order (weights [27][cin][cout], then bias). */
+int cfd_unet_get_params(cfd_unet* net, float* out, long long n);
+int cfd_unet_set_params(cfd_unet* net, const float* in, long long n);
+/* Weight file: 8-byte tag "CFDUNET1", int64 count, count FP32 values. */
+int cfd_unet_save(cfd_unet* net, const char* path);
+int cfd_unet_read(cfd_unet* net, const char* path);
+/* y = f(x) for one grid (x, y: nx*ny*nz floats; device pointers when
+ * on_device != 0, host otherwise). */
+int cfd_unet_forward(cfd_unet* net, const int dims[3], const float* x, float* y, int on_device);
+/* Training loss of one sample, d = f(x) - t on the grid:
+ *   w_l2 mean(d^2) + w_h1 (1/n) sum over axes of (d[i+e] - d[i])^2
+ * over neighbour pairs (default w_l2 = 1, w_h1 = 0). */
+int cfd_unet_set_loss(cfd_unet* net, float w_l2, float w_h1);
+/* The loss of one sample and, when grad is non-NULL, its gradient with
+ * respect to every parameter (host, cfd_unet_param_count()). */
+int cfd_unet_gradient(cfd_unet* net, const int dims[3], const float* x, const float* t, int on_device,
+                      float* loss, float* grad);
+/* Stored tensor t (0..13) of the last forward pass as floats (n = voxels of
+ * its level x channels, channels fastest); t = 13 is the FP32 output.  For
+ * tests and inspection. */
+int cfd_unet_tensor(cfd_unet* net, int t, float* out, long long n);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on the mean loss of nb samples
+ * stored one grid after another in x and t; *loss receives that mean. */
+int cfd_unet_train_batch(cfd_unet* net, const int dims[3], int nb, const float* x, const float* t,
+                         int on_device, float lr, float* loss);
+/* Uses net as the context's learned preconditioner.  dims: the pressure-node
+ * grid (product = NNp); p_of_vox (NNp entries, may be NULL = identity, i.e.
+ * pressure node x + nx (y + ny z)) names the pressure node of each voxel.
+ * The context keeps the pointer: net must stay alive, on the context's
+ * device, until it is detached (net = NULL) or the context is destroyed. */
+int cfd_unet_attach(cfd_ctx* ctx, cfd_unet* net, const int dims[3], const int* p_of_vox);
+/* Reads a weight file into a network owned by the context and attaches it;
+ * the grid is dims (NULL: a cube, NNp = m^3, identity numbering). */
+int cfd_unet_load(cfd_ctx* ctx, const char* path, const int dims[3]);
+/* r = rhs - Z x in FP64 (host buffers of NNp); *norm (may be NULL) = ||r||_2. */
+int cfd_pressure_residual(cfd_ctx* ctx, const double* rhs, const double* x, double* r, double* norm);
 
 /* ---- timing, counters and self-tests ---------------------------------------- */
 
@@ -211,7 +260,7 @@ long long cfd_launch_count(const cfd_ctx* ctx);
 
 enum cfd_kernel_class {
   CFD_K_CONVECT = 0, CFD_K_STEP1, CFD_K_GT, CFD_K_PCG64, CFD_K_PCG32, CFD_K_RESID64, CFD_K_STEP3,
-  CFD_K_SPMV_K3, CFD_K_PUPDATE, CFD_K_OTHER, CFD_K_COUNT
+  CFD_K_SPMV_K3, CFD_K_PUPDATE, CFD_K_OTHER, CFD_K_UNET, CFD_K_FCG, CFD_K_COUNT
 };
 /* Per-kernel-class CUDA-event timing on the context stream (on = 1 starts
  * and clears, 0 stops).  out receives CFD_K_COUNT triples

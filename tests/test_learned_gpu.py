@@ -1,0 +1,219 @@
+"""The learned pressure preconditioner on the GPU: the CUDA forward pass and
+hand-written backward kernels against the NumPy oracle, training through the
+C ABI, and flexible CG (with its Jacobi-PCG fallback) inside the solver.
+
+Tolerances: the device accumulates in FP32 and stores BF16 activations at the
+same points as the oracle, so a layer recomputed by the oracle from the
+device's own inputs differs only where a BF16 rounding flips (one ulp, under
+1% of values); gradients recomputed by the oracle from the device's stored
+tensors agree to 1e-4 per layer.  End to end, flips cascade through the
+layers (a few percent on small grids), so end-to-end bounds are looser.
+Solver runs with the learned preconditioner converge to the same relative
+residual as Jacobi-PCG, so whole runs keep the FP64 bound of 1e-6 against
+the oracle."""
+import numpy as np
+import pytest
+
+import unet_oracle as U
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = [(9, 9, 9), (13, 5, 9)]  # (nx, ny, nz)
+
+
+def _net(seed=3):
+    import cfdfs
+    net = cfdfs.UNet(device=0, seed=0)
+    theta = U.init_params(seed)
+    net.set_params(theta)
+    return net, theta
+
+
+def _sample(dims, seed):
+    rng = np.random.default_rng(seed)
+    shape = dims[::-1]
+    x = rng.normal(size=shape).astype(np.float32)
+    t = (rng.normal(size=shape) * 0.3).astype(np.float32)
+    return x, t
+
+
+@pytest.mark.parametrize("dims", GRIDS)
+def test_forward_matches_oracle(dims):
+    net, theta = _net()
+    x, _ = _sample(dims, 1)
+    y = net.forward(x, dims)
+    yo, _ = U.forward(theta, x.astype(np.float64))
+    assert rel_l2(y, yo) < 5e-3
+    net.close()
+
+
+def _gpu_tensors(net, dims):
+    return [net.tensor(t, dims).astype(np.float64) for t in range(len(U.TENSORS))]
+
+
+@pytest.mark.parametrize("dims", GRIDS)
+def test_forward_layers_match_oracle(dims):
+    """Each layer of the device forward pass, recomputed by the oracle from
+    the device's own input tensor of that layer: BF16 outputs agree except
+    for rare one-ulp rounding flips (FP32 vs FP64 accumulation)."""
+    net, theta = _net(6)
+    x, _ = _sample(dims, 3)
+    net.forward(x, dims)
+    T = _gpu_tensors(net, dims)
+    layers = U.split_params(theta)
+    lv = U.level_dims(dims)
+    assert np.array_equal(T[0][..., 0], U.bf16(x))
+    for op in U.ORDER:
+        if op >= 0:
+            ti, to, stride, act = U.CONVS[op]
+            W, b = layers[op]
+            y = U.conv(T[ti], U.bf16(W), b.astype(np.float64), stride, lv[U.TENSORS[to][0]][::-1])
+            if act:
+                y = np.where(y < 0, U.LEAKY * y, y)
+        else:
+            ci, si, to = U.UPS[-1 - op]
+            y = U.prolong(T[ci]) + T[si]
+        if to == len(U.TENSORS) - 1:
+            assert rel_l2(T[to], y) < 1e-5, op
+            continue
+        ref = U.bf16(y)
+        diff = T[to] != ref
+        assert diff.mean() < 0.01, (op, diff.mean())
+        # a flip moves a value to the neighbouring BF16 number, or (for values
+        # that come out of cancellation) by the FP32 rounding of the sum
+        bound = np.abs(ref[diff]) * 2.0 ** -7 + 1e-5 * np.abs(ref).max()
+        assert np.all(np.abs(T[to] - ref)[diff] <= bound), op
+
+
+@pytest.mark.parametrize("dims,w_h1", [(GRIDS[0], 0.0), (GRIDS[1], 0.5)])
+def test_gradients_match_oracle(dims, w_h1):
+    """Hand-written backward kernels against the oracle's reverse mode, both
+    starting from the device's stored forward tensors (so BF16 rounding
+    flips of the forward pass cannot mask or fake a difference)."""
+    net, theta = _net(4)
+    net.set_loss(1.0, w_h1)
+    x, t = _sample(dims, 2)
+    loss, g = net.gradient(x, t, dims)
+    T = _gpu_tensors(net, dims)
+    loss_o, g_o = U.backward(theta, T, t.astype(np.float64), 1.0, w_h1)
+    assert abs(loss - loss_o) <= 1e-5 * loss_o
+    offs = np.cumsum([0] + [a + b for (a, b, _, _) in U.layer_shapes()])
+    for layer in range(len(U.CONVS)):
+        sl = slice(offs[layer], offs[layer + 1])
+        assert rel_l2(g[sl], g_o[sl]) < 1e-4, layer
+    # and end to end from the oracle's own forward pass (rounding flips allowed)
+    _, tens = U.forward(theta, x.astype(np.float64))
+    _, g_e = U.backward(theta, tens, t.astype(np.float64), 1.0, w_h1)
+    assert rel_l2(g, g_e) < 0.1
+    net.close()
+
+
+def test_training_reduces_loss(tmp_path):
+    """Adam on the device learns a smoothing map (7-point averages) of
+    random fields; the loss must fall well below its starting value."""
+    import cfdfs
+    net = cfdfs.UNet(device=0, seed=7)
+    dims = (9, 9, 9)
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(64,) + dims[::-1]).astype(np.float32)
+    t = x.copy()
+    for _ in range(3):
+        p = np.pad(t, ((0, 0), (1, 1), (1, 1), (1, 1)), mode="edge")
+        t = (p[:, 1:-1, 1:-1, 1:-1] + p[:, :-2, 1:-1, 1:-1] + p[:, 2:, 1:-1, 1:-1] + p[:, 1:-1, :-2, 1:-1] +
+             p[:, 1:-1, 2:, 1:-1] + p[:, 1:-1, 1:-1, :-2] + p[:, 1:-1, 1:-1, 2:]) / 7.0
+    losses = [net.train_batch(x[i:i + 8], t[i:i + 8], dims, lr=2e-3) for i in range(0, 64, 8) for _ in range(6)]
+    assert losses[-1] < 0.3 * losses[0], losses
+    path = str(tmp_path / "w.bin")
+    net.save(path)
+    net2 = cfdfs.UNet(device=0, seed=1, path=path)
+    assert np.array_equal(net2.params(), net.params())
+    assert np.array_equal(net2.forward(x[0], dims), net.forward(x[0], dims))
+    net.close()
+    net2.close()
+
+
+def _solver(deck, **kw):
+    import cfdfs
+    s = cfdfs.Solver(device=0, **kw)
+    s.load(deck)
+    s.step0()
+    return s
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_flexible_cg_solves_to_tolerance(decks, precision):
+    """Flexible CG with an untrained network reaches the requested relative
+    residual (directly or through its Jacobi-PCG fallback) and agrees with
+    the Jacobi-PCG solution."""
+    import cfdfs
+    s_j = _solver(decks["c1"], precision=precision, cg_rtol=1e-10)
+    s_l = _solver(decks["c1"], precision=precision, cg_rtol=1e-10, precond=cfdfs.PC_LEARNED)
+    net = cfdfs.UNet(device=0, seed=5)
+    s_l.attach_unet(net, (9, 9, 9))
+    rng = np.random.default_rng(3)
+    b = rng.standard_normal(s_l.refresh().NNp)
+    b[s_l.info.zeroPressureNode] = 0.0
+    xj, st_j = s_j.pressure_solve(b)
+    xl, st_l = s_l.pressure_solve(b)
+    assert st_j.status == 0 and st_l.status == 0
+    r, nr = s_j.pressure_residual(b, xl)
+    assert nr <= 1.01e-10 * np.linalg.norm(b)
+    assert rel_l2(xl, xj) < 1e-6
+    s_j.close()
+    s_l.close()
+    net.close()
+
+
+def test_zero_network_falls_back_to_jacobi(decks):
+    """A network that outputs zero gives flexible CG no direction: the solve
+    reports the fallback and still converges through Jacobi-PCG."""
+    import cfdfs
+    s = _solver(decks["c1"], precond=cfdfs.PC_LEARNED)
+    net = cfdfs.UNet(device=0, seed=5)
+    net.set_params(np.zeros(net.nparam, dtype=np.float32))
+    s.attach_unet(net)
+    b = np.random.default_rng(1).standard_normal(s.refresh().NNp)
+    b[s.info.zeroPressureNode] = 0.0
+    x, st = s.pressure_solve(b)
+    assert st.status == 0 and st.fallback == 1
+    _, nr = s.pressure_residual(b, x)
+    assert nr <= 1.01e-8 * np.linalg.norm(b)
+    s.close()
+    net.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_learned_run_matches_oracle(decks, oracle_mod, precision):
+    """Config-1 cavity, 20 steps, with the learned preconditioner: the flow
+    matches the FP64 oracle (Jacobi-PCG) within the run tolerance of its
+    precision (1e-6 FP64, 1e-5 mixed)."""
+    import cfdfs
+    o = oracle_mod.Oracle(decks["c1"])
+    o.step0()
+    o.run(-1)
+    s = _solver(decks["c1"], precision=precision, precond=cfdfs.PC_LEARNED)
+    net = cfdfs.UNet(device=0, seed=9)
+    s.attach_unet(net)
+    st = s.run(-1)
+    assert st.steps == 20
+    Ug, Pg = s.state()
+    tol = 1e-6 if precision == 0 else 1e-5
+    assert rel_l2(Ug, o.vec("Un")) < tol and rel_l2(Pg, o.vec("Pn")) < tol
+    prof_names = cfdfs.Solver.KCLASS
+    assert "unet" in prof_names and "fcg" in prof_names
+    s.close()
+    net.close()
+    o.close()
+
+
+def test_attach_rejects_wrong_grid(decks):
+    import cfdfs
+    s = _solver(decks["c1"], precond=cfdfs.PC_LEARNED)
+    net = cfdfs.UNet(device=0, seed=1)
+    with pytest.raises(cfdfs.CfdError):
+        s.attach_unet(net, (9, 9, 10))
+    with pytest.raises(cfdfs.CfdError):
+        s.attach_unet(net, (9, 9, 9), p_of_vox=np.zeros(729, dtype=np.int32))
+    s.close()
+    net.close()
