@@ -116,6 +116,8 @@ _PROTOS = {
     "cfd_unet_train_batch": (C.c_int, [_vp, _ip, C.c_int, _vp, _vp, C.c_int, C.c_float, _fp]),
     "cfd_unet_set_loss": (C.c_int, [_vp, C.c_float, C.c_float]),
     "cfd_unet_tensor": (C.c_int, [_vp, C.c_int, _fp, C.c_longlong]),
+    "cfd_unet_set_tensor_cores": (C.c_int, [_vp, C.c_int]),
+    "cfd_unet_status": (C.c_int, [_vp]),
     "cfd_unet_attach": (C.c_int, [_vp, _vp, _ip, _ip]),
     "cfd_unet_load": (C.c_int, [_vp, _cp, _ip]),
     "cfd_pressure_residual": (C.c_int, [_vp, _dp, _dp, _dp, _dp]),
@@ -542,6 +544,14 @@ class UNet:
 
     def read(self, path: str):
         self._check(self.L.cfd_unet_read(self.h, path.encode()))
+
+    def set_tensor_cores(self, on: bool):
+        """Forward convolutions on tcgen05 tensor cores (default) or CUDA cores."""
+        self._check(self.L.cfd_unet_set_tensor_cores(self.h, 1 if on else 0))
+
+    def status(self):
+        """Raises if a bounded wait in a tensor-core launch gave up."""
+        self._check(self.L.cfd_unet_status(self.h))
 
     def set_loss(self, w_l2: float = 1.0, w_h1: float = 0.0):
         """Training loss weights (mean squared error, neighbour-difference term)."""

@@ -4,14 +4,16 @@ forward and backward kernels.
 
 Data.  For a right-hand side R2 met during a run, a FP64 Jacobi-PCG solve to
 ||r|| <= 1e-12 ||R2|| gives x*; Jacobi-PCG stopped after k iterations gives
-x_k (x_0 = 0); each pair is (r_k = R2 - Z x_k, e_k = x* - x_k).  Network
-input x = r_k / s and target t = e_k * d / s, with s = RMS(r_k) and d the
-median diagonal entry of Z, so that neither the residual's size nor the
-mesh spacing reaches the network (flexible CG is invariant to the scale of
-the preconditioned vector, so inference needs no rescaling).  Cavity runs
+x_k (x_0 = 0); each pair is (r_k = R2 - Z x_k, e_k = x* - x_k).  The
+preconditioner applies z = D^-1 r + f(r / s) s / d (a Jacobi step plus the
+network's correction), so the network input is x = r_k / s and its target
+t = (e_k - D^-1 r_k) d / s, with s = RMS(r_k), D the diagonal of Z and d its
+median entry: neither the residual's size nor the mesh spacing reaches the
+network, and a network that outputs zero leaves plain Jacobi.  Cavity runs
 draw Re ~ U[100, 1000] and lid speed ~ U[0.5, 1.5] from
-numpy.random.Generator(PCG64(seed)); duct runs use the bent duct with a
-parabolic inlet.
+numpy.random.Generator(PCG64(seed)), with dt = 0.002 / max(1, lid) so that
+the explicit convection step stays within the CFL number of the 64^3
+benchmark case; duct runs use the bent duct with a parabolic inlet.
 
 Run ``python -m cfdfs.learned --out weights.bin`` on a GPU machine; it
 writes the weights and a JSON log of the data, the loss curve and the
@@ -27,7 +29,7 @@ import time
 
 import numpy as np
 
-from . import FP64, MIXED, PC_JACOBI, PC_LEARNED, HostMesh, Solver, UNet, meshgen
+from . import FP64, MIXED, PC_JACOBI, PC_LEARNED, CfdError, HostMesh, Solver, UNet, meshgen
 
 KS = (0, 3, 10, 30, 100)  # Jacobi-PCG iterations of the x_k in each pair
 
@@ -55,6 +57,7 @@ class PairSampler:
         rp, col, val = self.pair.matrix("Z")
         rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
         diag = val[col == rows]
+        self.dinv = 1.0 / diag
         self.dscale = float(np.median(diag))
         self.n = len(rp) - 1
         assert int(np.prod(self.dims)) == self.n
@@ -91,7 +94,7 @@ class PairSampler:
                 continue
             s = nr / np.sqrt(self.n)
             x = (r / s).astype(np.float32).reshape(shape)
-            t = ((xs - xk) * (self.dscale / s)).astype(np.float32).reshape(shape)
+            t = ((xs - xk - self.dinv * r) * (self.dscale / s)).astype(np.float32).reshape(shape)
             out.append((x, t))
         return out
 
@@ -102,19 +105,23 @@ def cavity_pairs(seeds, n=64, dt=0.002, snap_steps=(1, 5, 15, 35, 70, 100), devi
     tmpdir = tmpdir or tempfile.mkdtemp()
     for seed in seeds:
         re, lid = cavity_params(seed)
+        dts = dt / max(1.0, lid)
         deck = meshgen.write_cavity(os.path.join(tmpdir, f"cav_{seed}.inp"),
-                                    meshgen.CavitySpec(n, re=re, dt=dt, steps=max(snap_steps), ngp=8, lid=lid))
+                                    meshgen.CavitySpec(n, re=re, dt=dts, steps=max(snap_steps), ngp=8, lid=lid))
         ps = PairSampler(deck, (n + 1,) * 3, device=device)
-        done = 0
-        for stp in snap_steps:
-            for rhs in ps.advance(stp - done):
-                for x, t in ps.pairs(rhs):
-                    xs.append(x)
-                    ts.append(t)
-            done = stp
+        done, note = 0, "ok"
+        try:
+            for stp in snap_steps:
+                for rhs in ps.advance(stp - done):
+                    for x, t in ps.pairs(rhs):
+                        xs.append(x)
+                        ts.append(t)
+                done = stp
+        except CfdError as e:  # a run that blows up keeps the pairs it gave
+            note = f"stopped after step {done}: {e}"
         ps.close()
         if log is not None:
-            log.append(dict(source="cavity", seed=seed, re=re, lid=lid, pairs=len(xs)))
+            log.append(dict(source="cavity", seed=seed, re=re, lid=lid, dt=dts, pairs=len(xs), note=note))
     return np.stack(xs), np.stack(ts)
 
 

@@ -118,6 +118,7 @@ struct cfd_ctx {
   DevBuf<double> fcg_sc, fcg_part;
   DevBuf<int> fcg_done;
   int fcg_window = 25;
+  double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
 
   int timeN = 0;
@@ -431,10 +432,11 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
   c->launches++;
   const int* pmap = c->upmap.p;
-  // the last layer writes z directly when no conversion or gather is needed
-  float* direct = nullptr;
+  const VT* dinv;
   if constexpr (sizeof(VT) == 4)
-    if (!pmap) direct = (float*)a.z;
+    dinv = c->zdinv32.p;
+  else
+    dinv = c->zdinv.p;
   int issued = 0, batch = 2;
   double rr_prev = -1;
   for (;;) {
@@ -442,11 +444,12 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       const long long l0 = net.launches;
       KL(CFD_K_UNET, ([&]() -> cudaError_t {
            cudaError_t e = unet_input(n, a.r, pmap, a.st.sc + kFcgRR, 0.0, net.act[0], a.st.done, s);
-           if (e == cudaSuccess) e = net.forward(s, direct, a.st.done);
-           if (e == cudaSuccess && !direct) e = unet_output(n, net.out, pmap, a.z, a.st.done, s);
+           if (e == cudaSuccess) e = net.forward(s, nullptr, a.st.done);
+           if (e == cudaSuccess)
+             e = unet_output(n, net.out, pmap, a.st.sc + kFcgRR, c->unet_dscale, dinv, a.r, a.z, a.st.done, s);
            return e;
          })());
-      c->launches += net.launches - l0 + (direct ? 0 : 1);
+      c->launches += net.launches - l0 + 1;
       KL(CFD_K_FCG, launch_fcg_spmv<VT>(a, s));
       KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
       c->launches += 2;
@@ -1274,9 +1277,11 @@ int cfd_unet_forward(cfd_unet* u, const int dims[3], const float* x, float* y, i
   if (!on_device && tmp.alloc(2 * (size_t)nv)) return CFD_E_NOMEM;
   rc = unet_load_input(u, x, nv, on_device, tmp.p);
   if (rc) return rc;
-  float* dst = on_device ? y : tmp.p + nv;
-  if (n.forward(s, dst) != cudaSuccess) return CFD_E_CUDA;
-  if (!on_device && cudaMemcpyAsync(y, dst, nv * sizeof(float), cudaMemcpyDeviceToHost, s)) return CFD_E_CUDA;
+  // the output stays in the network's FP32 buffer too (cfd_unet_tensor)
+  if (n.forward(s, nullptr) != cudaSuccess) return CFD_E_CUDA;
+  if (cudaMemcpyAsync(y, n.out, nv * sizeof(float), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                      s))
+    return CFD_E_CUDA;
   return cudaStreamSynchronize(s) == cudaSuccess ? CFD_OK : CFD_E_CUDA;
 }
 
@@ -1345,6 +1350,26 @@ int cfd_unet_tensor(cfd_unet* u, int t, float* out, long long n) {
   return CFD_OK;
 }
 
+int cfd_unet_set_tensor_cores(cfd_unet* u, int on) {
+  if (!u) return CFD_E_BADARG;
+  u->net.tc_enabled = on != 0;
+  return CFD_OK;
+}
+
+int cfd_unet_status(cfd_unet* u) {
+  if (!u) return CFD_E_BADARG;
+  cudaSetDevice(u->net.device);
+  int h = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess ||
+      cudaMemcpy(&h, u->net.tc_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return CFD_E_CUDA;
+  if (h) {
+    u->net.err = "a bounded wait in a tensor-core convolution gave up";
+    return CFD_E_TIMEOUT;
+  }
+  return CFD_OK;
+}
+
 int cfd_unet_set_loss(cfd_unet* u, float w_l2, float w_h1) {
   if (!u || !(w_l2 >= 0) || !(w_h1 >= 0) || w_l2 + w_h1 <= 0) return CFD_E_BADARG;
   u->net.w_l2 = w_l2;
@@ -1382,7 +1407,7 @@ int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_
     c->unet_owned.reset();
     return CFD_OK;
   }
-  NEED(c->loaded, "cfd_unet_attach before the problem is loaded");
+  NEED(c->assembled, "cfd_unet_attach before cfd_step0");
   NEED(dims, "cfd_unet_attach needs the grid dims");
   NEED(u->net.device == c->device, "network and context live on different devices");
   const long long nv = (long long)dims[0] * dims[1] * dims[2];
@@ -1400,6 +1425,13 @@ int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_
     CU(cudaStreamSynchronize(c->stream));
   }
   for (int a = 0; a < 3; a++) c->udims[a] = dims[a];
+  {
+    std::vector<double> dg(nv);
+    CU(cudaStreamSynchronize(c->stream));
+    CU(cudaMemcpy(dg.data(), c->zdiag.p, nv * sizeof(double), cudaMemcpyDeviceToHost));
+    std::nth_element(dg.begin(), dg.begin() + nv / 2, dg.end());
+    c->unet_dscale = dg[nv / 2] > 0 ? dg[nv / 2] : 1.0;
+  }
   if (c->unet_owned.get() != u) c->unet_owned.reset();
   c->unet = u;
   return CFD_OK;
@@ -1407,7 +1439,7 @@ int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_
 
 int cfd_unet_load(cfd_ctx* c, const char* path, const int dims[3]) {
   if (!c || !path) return CFD_E_BADARG;
-  NEED(c->loaded, "cfd_unet_load before the problem is loaded");
+  NEED(c->assembled, "cfd_unet_load before cfd_step0");
   int d[3];
   if (dims) {
     for (int a = 0; a < 3; a++) d[a] = dims[a];

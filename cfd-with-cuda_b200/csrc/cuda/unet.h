@@ -9,6 +9,7 @@
 // The layer list lives in the host network (unet_net.h); these are its
 // building blocks.  Activation: leaky ReLU, slope 0.1.
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -63,11 +64,14 @@ cudaError_t unet_input(int nv, const double* r, const int* p_of_vox, const doubl
                        __nv_bfloat16* x, const int* skipflag, cudaStream_t s);
 cudaError_t unet_input(int nv, const float* r, const int* p_of_vox, const double* rr, double scale,
                        __nv_bfloat16* x, const int* skipflag, cudaStream_t s);
-// z[p(v)] = out[v]
-cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, double* z, const int* skipflag,
-                        cudaStream_t s);
-cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, float* z, const int* skipflag,
-                        cudaStream_t s);
+// Preconditioned vector of flexible CG: z[p(v)] = out[v] * sqrt(rr[0] / nv)
+// / dscale + dinv[p(v)] r[p(v)] -- the network's correction (trained on
+// unit-RMS residuals and errors scaled by the median diagonal dscale) on top
+// of a Jacobi step.
+cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, const double* rr, double dscale,
+                        const double* dinv, const double* r, double* z, const int* skipflag, cudaStream_t s);
+cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, const double* rr, double dscale,
+                        const float* dinv, const float* r, float* z, const int* skipflag, cudaStream_t s);
 
 // Training loss of one sample on grid dims, d = out - target:
 //   w_l2 mean(d^2) + w_h1 (1/n) sum over axes of (d[i+e] - d[i])^2
@@ -80,5 +84,44 @@ cudaError_t adam_step(long long n, float* w, const float* g, float* m, float* v,
                       float b1, float b2, float eps, int t, float gscale, cudaStream_t s);
 
 cudaError_t f32_to_bf16(long long n, const float* a, __nv_bfloat16* b, cudaStream_t s);
+
+// ---- tensor-core path (unet_tc.cu): stride-1 convolutions, cin in {16, 32,
+// 64}, cout in {16, 32, 64} or 1 with FP32 output ----
+struct ConvTcParams {
+  int dims[3];      // grid (input = output)
+  int brick[3];     // output voxels per CTA along each axis
+  int nb[3];        // bricks per axis
+  int halo[3];      // brick + 2
+  int rows;         // rows reserved per 8-channel plane (halo box plus read slack)
+  int plane_bytes;  // rows * 16 rounded up to 1 KiB
+  int q0, tiles;    // first computed row, 128-row M tiles
+  int cin, N, nslices, cout;
+  const __nv_bfloat16* wpack;  // conv_tc_pack layout
+  const float* bias;
+  __nv_bfloat16* out;
+  float* out_f32;
+  int act;
+  const int* skip;
+  int* err;  // set when a bounded wait gives up
+};
+struct ConvTcPlan {
+  CUtensorMap tmap;  // TMA descriptor of the input tensor
+  ConvTcParams p;
+  int grid_x;
+  size_t smem;
+  int ready;
+};
+bool conv_tc_supported(const ConvDesc& d);
+int conv_tc_slice_width(int cin, int cout);
+long long conv_tc_pack_elems(int cin, int cout);
+// Rearranges [27][cin][cout] BF16 weights into per-tap canonical tensor-core
+// blocks (wpack holds conv_tc_pack_elems values).
+cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, __nv_bfloat16* wpack, cudaStream_t s);
+// Builds the launch plan (bricks, shared-memory layout, TMA descriptor) of a
+// supported convolution; 0 on success.
+int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan);
+// Launches a planned convolution; out_f32 (FP32-output layers) and skip
+// replace the plan's pointers for this launch.
+cudaError_t conv3_forward_tc(const ConvTcPlan& plan, float* out_f32, const int* skip, int* err, cudaStream_t s);
 
 }  // namespace cfd

@@ -2,9 +2,9 @@
 #include "unet_net.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
-#include "../cuda/unet.h"
 
 namespace cfd {
 
@@ -36,8 +36,9 @@ uint64_t splitmix(uint64_t& s) {
 double uniform01(uint64_t& s) { return ((splitmix(s) >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
 
 template <class T>
-cudaError_t grow(T*& p, long long& cap, long long n) {
+cudaError_t grow(T*& p, long long& cap, long long n, int* gen = nullptr) {
   if (n <= cap) return cudaSuccess;
+  if (gen) ++*gen;
   if (p) cudaFree(p);
   p = nullptr;
   cap = 0;
@@ -72,6 +73,8 @@ UnetNet::~UnetNet() {
   }
   cudaFree(out);
   cudaFree(lossv);
+  cudaFree(tc_err);
+  for (int l = 0; l < kUnetConvs; l++) cudaFree(wpack[l]);
   if (h_pinned) cudaFreeHost(h_pinned);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -79,11 +82,14 @@ UnetNet::~UnetNet() {
 int UnetNet::init(unsigned long long seed) {
   nparam = unet_param_count();
   if (cudaGetDevice(&device) != cudaSuccess) return -1;
+  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (const char* e = std::getenv("CFD_UNET_TC")) tc_enabled = std::atoi(e) != 0;
   if (!own_stream && cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
   const size_t b = (size_t)nparam * sizeof(float);
   if (cudaMalloc((void**)&P, b) || cudaMalloc((void**)&G, b) || cudaMalloc((void**)&M1, b) ||
       cudaMalloc((void**)&M2, b) || cudaMalloc((void**)&Pb, (size_t)nparam * sizeof(__nv_bfloat16)) ||
-      cudaMalloc((void**)&lossv, 64 * sizeof(float)) || cudaMallocHost((void**)&h_pinned, 64 * sizeof(float))) {
+      cudaMalloc((void**)&lossv, 64 * sizeof(float)) || cudaMallocHost((void**)&h_pinned, 64 * sizeof(float)) ||
+      cudaMalloc((void**)&tc_err, sizeof(int)) || cudaMemset(tc_err, 0, sizeof(int))) {
     err = "U-Net parameter allocation failed";
     return -1;
   }
@@ -120,6 +126,7 @@ int UnetNet::set_params(const float* h, long long n) {
   }
   launches++;
   adam_t = 0;
+  packs_dirty = true;
   return 0;
 }
 
@@ -148,8 +155,8 @@ int UnetNet::set_grid(const int d[3], bool train) {
   for (int l = 0; l < 3; l++) nvox[l] = (long long)dims[l][0] * dims[l][1] * dims[l][2];
   cudaError_t e = cudaSuccess;
   for (int t = 0; t < kUnetTensors - 1 && e == cudaSuccess; t++)
-    e = grow(act[t], cap[t], nvox[kUnetTensor[t].level] * kUnetTensor[t].ch);
-  if (e == cudaSuccess) e = grow(out, out_cap, nvox[0]);
+    e = grow(act[t], cap[t], nvox[kUnetTensor[t].level] * kUnetTensor[t].ch, &gen);
+  if (e == cudaSuccess) e = grow(out, out_cap, nvox[0], &gen);
   for (int t = 1; train && t < kUnetTensors && e == cudaSuccess; t++)
     e = grow(grad[t], gcap[t], nvox[kUnetTensor[t].level] * kUnetTensor[t].ch);
   if (e != cudaSuccess) {
@@ -191,12 +198,42 @@ ConvDesc conv_desc(const UnetNet& n, int l, float* out_f32, const int* skip = nu
 
 }  // namespace
 
+cudaError_t UnetNet::prepare_tc(cudaStream_t s) {
+  if (packs_dirty) {
+    for (int l = 0; l < kUnetConvs; l++) {
+      const int cin = kUnetTensor[kUnetConv[l].in].ch, cout = kUnetTensor[kUnetConv[l].out].ch;
+      if (cin % 16) continue;
+      cudaError_t e = grow(wpack[l], wpack_cap[l], conv_tc_pack_elems(cin, cout));
+      if (e == cudaSuccess) e = conv_tc_pack(Pb + unet_weight_offset(l), cin, cout, wpack[l], s);
+      launches++;
+      if (e != cudaSuccess) return e;
+    }
+    packs_dirty = false;
+  }
+  if (plan_gen != gen || plan_dims[0] != dims[0][0] || plan_dims[1] != dims[0][1] || plan_dims[2] != dims[0][2]) {
+    for (int l = 0; l < kUnetConvs; l++) {
+      ConvDesc d = conv_desc(*this, l, out);
+      plan_ok[l] = wpack[l] && conv_tc_supported(d) && conv_tc_plan(d, wpack[l], num_sms, plans[l]) == 0;
+    }
+    plan_gen = gen;
+    for (int a = 0; a < 3; a++) plan_dims[a] = dims[0][a];
+  }
+  return cudaSuccess;
+}
+
 cudaError_t UnetNet::forward(cudaStream_t s, float* out_f32, const int* skip) {
   if (!out_f32) out_f32 = out;
+  if (tc_enabled) {
+    cudaError_t e = prepare_tc(s);
+    if (e != cudaSuccess) return e;
+  }
   for (int op : kOrder) {
     cudaError_t e;
     if (op >= 0) {
-      e = conv3_forward(conv_desc(*this, op, out_f32, skip), s);
+      if (tc_enabled && plan_ok[op])
+        e = conv3_forward_tc(plans[op], out_f32, skip, tc_err, s);
+      else
+        e = conv3_forward(conv_desc(*this, op, out_f32, skip), s);
     } else {
       const UnetUpSpec& u = kUnetUp[-1 - op];
       const int lc = kUnetTensor[u.in].level, lf = kUnetTensor[u.out].level;
@@ -244,6 +281,7 @@ cudaError_t UnetNet::backward(cudaStream_t s) {
 
 cudaError_t UnetNet::adam(cudaStream_t s, float lr, float gscale) {
   adam_t++;
+  packs_dirty = true;
   launches++;
   return adam_step(nparam, P, G, M1, M2, Pb, lr, 0.9f, 0.999f, 1e-8f, adam_t, gscale, s);
 }

@@ -25,6 +25,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "../cuda/unet.h"
+
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -74,6 +76,18 @@ struct UnetNet {
   long long gcap[kUnetTensors] = {};
   float* lossv = nullptr;
   float* h_pinned = nullptr;
+  int gen = 0;  // bumped whenever an activation buffer moves
+
+  // tensor-core path: packed weights and launch plans of the stride-1 layers
+  bool tc_enabled = true;
+  int num_sms = 148;
+  __nv_bfloat16* wpack[kUnetConvs] = {};
+  long long wpack_cap[kUnetConvs] = {};
+  bool packs_dirty = true;
+  ConvTcPlan plans[kUnetConvs];
+  bool plan_ok[kUnetConvs] = {};
+  int plan_gen = -1, plan_dims[3] = {0, 0, 0};
+  int* tc_err = nullptr;
 
   ~UnetNet();
   // Allocates parameters on the current device and initialises them from seed.
@@ -83,6 +97,8 @@ struct UnetNet {
   int get_params(float* h, long long n);
   // Sets the grid and (re)allocates activations; train != 0 also gradients.
   int set_grid(const int d[3], bool train);
+  // Packs weights and builds plans for the tensor-core layers when needed.
+  cudaError_t prepare_tc(cudaStream_t s);
   // Forward pass of the grid set by set_grid: act[0] must hold the input;
   // writes the FP32 output to out_f32 (or this->out when null).  Every
   // kernel is a no-op while the device flag *skip is set (skip may be null).

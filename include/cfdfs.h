@@ -231,6 +231,14 @@ int cfd_unet_set_loss(cfd_unet* net, float w_l2, float w_h1);
  * respect to every parameter (host, cfd_unet_param_count()). */
 int cfd_unet_gradient(cfd_unet* net, const int dims[3], const float* x, const float* t, int on_device,
                       float* loss, float* grad);
+/* Forward convolutions on the tensor cores (tcgen05, the default where the
+ * layer shape allows: stride 1, 16/32/64 input channels) or all on the
+ * CUDA-core kernels (on = 0).  The backward pass always uses the CUDA-core
+ * kernels. */
+int cfd_unet_set_tensor_cores(cfd_unet* net, int on);
+/* CFD_E_TIMEOUT if a bounded wait inside a tensor-core convolution gave up
+ * since the network was created (the output of that launch is invalid). */
+int cfd_unet_status(cfd_unet* net);
 /* Stored tensor t (0..13) of the last forward pass as floats (n = voxels of
  * its level x channels, channels fastest); t = 13 is the FP32 output.  For
  * tests and inspection. */

@@ -52,14 +52,18 @@ def _gpu_tensors(net, dims):
     return [net.tensor(t, dims).astype(np.float64) for t in range(len(U.TENSORS))]
 
 
-@pytest.mark.parametrize("dims", GRIDS)
-def test_forward_layers_match_oracle(dims):
-    """Each layer of the device forward pass, recomputed by the oracle from
-    the device's own input tensor of that layer: BF16 outputs agree except
-    for rare one-ulp rounding flips (FP32 vs FP64 accumulation)."""
+@pytest.mark.parametrize("dims,tc", [(GRIDS[0], False), (GRIDS[1], False), (GRIDS[0], True), (GRIDS[1], True),
+                                     ((33, 17, 21), True), ((65, 65, 65), True)])
+def test_forward_layers_match_oracle(dims, tc):
+    """Each layer of the device forward pass (CUDA-core kernels, or the
+    tcgen05 tensor-core convolutions where the layer allows), recomputed by
+    the oracle from the device's own input tensor of that layer: BF16 outputs
+    agree except for rare rounding flips (FP32 vs FP64 accumulation)."""
     net, theta = _net(6)
+    net.set_tensor_cores(tc)
     x, _ = _sample(dims, 3)
     net.forward(x, dims)
+    net.status()
     T = _gpu_tensors(net, dims)
     layers = U.split_params(theta)
     lv = U.level_dims(dims)
@@ -165,13 +169,37 @@ def test_flexible_cg_solves_to_tolerance(decks, precision):
     net.close()
 
 
-def test_zero_network_falls_back_to_jacobi(decks):
-    """A network that outputs zero gives flexible CG no direction: the solve
-    reports the fallback and still converges through Jacobi-PCG."""
+def test_zero_network_is_jacobi_cg(decks):
+    """The preconditioner is a Jacobi step plus the network's correction, so
+    a network that outputs zero turns flexible CG into Jacobi-PCG: same
+    iteration count (within rounding), no fallback."""
     import cfdfs
+    s_j = _solver(decks["c1"])
     s = _solver(decks["c1"], precond=cfdfs.PC_LEARNED)
     net = cfdfs.UNet(device=0, seed=5)
     net.set_params(np.zeros(net.nparam, dtype=np.float32))
+    s.attach_unet(net)
+    b = np.random.default_rng(1).standard_normal(s.refresh().NNp)
+    b[s.info.zeroPressureNode] = 0.0
+    x, st = s.pressure_solve(b)
+    xj, st_j = s_j.pressure_solve(b)
+    assert st.status == 0 and st.fallback == 0
+    assert abs(st.iterations - st_j.iterations) <= 2
+    assert rel_l2(x, xj) < 1e-6
+    s.close()
+    s_j.close()
+    net.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_broken_network_falls_back_to_jacobi(decks, precision):
+    """A network whose output is not finite gives flexible CG no usable
+    direction: the solve reports the fallback and still converges through
+    Jacobi-PCG."""
+    import cfdfs
+    s = _solver(decks["c1"], precision=precision, precond=cfdfs.PC_LEARNED)
+    net = cfdfs.UNet(device=0, seed=5)
+    net.set_params(np.full(net.nparam, np.nan, dtype=np.float32))
     s.attach_unet(net)
     b = np.random.default_rng(1).standard_normal(s.refresh().NNp)
     b[s.info.zeroPressureNode] = 0.0
