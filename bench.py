@@ -34,6 +34,7 @@ sys.path.insert(0, os.path.join(ROOT, "cfd-with-cuda_b200"))
 METRIC = "steps/s at 64³ cavity: mixed+learned-precond vs plain FP64 CG, rel err≤1e-6"
 WORKLOAD = "lid-driven cavity 64x64x64 hex27/hex8 (129^3 velocity, 65^3 pressure nodes), Re=1000, dt=0.002"
 N_ELEM, RE, DT, T_STEPS = 64, 1000.0, 0.002, 100
+WEIGHTS = os.path.join(ROOT, "cfd-with-cuda_b200", "weights", "unet_cavity.bin")
 
 
 def _env_int(name, default):
@@ -56,6 +57,14 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
 
 
 class ClockSampler:
@@ -139,6 +148,18 @@ def algorithmic_bytes(info, klass, iters_per_launch, mixed):
     return 0
 
 
+def unet_flops(dims):
+    """FLOPs of one U-Net application on a pressure grid (multiply-adds of the
+    11 convolutions, counted as 2 flops each)."""
+    d0 = list(dims)
+    lv = [d0, [(v - 1) // 2 + 1 for v in d0]]
+    lv.append([(v - 1) // 2 + 1 for v in lv[1]])
+    vox = [a[0] * a[1] * a[2] for a in lv]
+    convs = [(0, 1, 16), (1, 16, 32), (1, 32, 32), (2, 32, 64), (2, 64, 64), (2, 64, 64), (2, 64, 32),
+             (1, 32, 32), (1, 32, 16), (0, 16, 16), (0, 16, 1)]
+    return sum(2 * 27 * ci * co * vox[l] for (l, ci, co) in convs)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -152,6 +173,7 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     work = tempfile.mkdtemp(prefix=f"cfdbench{rank}_")
     deck = make_deck(os.path.join(work, "cavity64.inp"), args.n)
+    learned = args.precond == "learned"
 
     def barrier():
         if dist is not None:
@@ -164,17 +186,19 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed_solver(precision, steps, warmup, profile_launches=True):
-        s = cfdfs.Solver(device=local_rank, precision=precision, cg_rtol=1e-8, cg_maxit=args.cg_maxit)
+    def timed_solver(precision, use_net, steps, warmup):
+        s = cfdfs.Solver(device=local_rank, precision=precision, cg_rtol=1e-8, cg_maxit=args.cg_maxit,
+                         precond=cfdfs.PC_LEARNED if use_net else cfdfs.PC_JACOBI)
         t0 = time.time()
         s.load(deck)
         s.step0()
+        if use_net:
+            s.load_unet(args.weights)
         setup_s = time.time() - t0
         for _ in range(warmup):
             s.run(1)
         stream = torch.cuda.ExternalStream(s.stream_ptr, device=local_rank)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.profile(True)
         n0 = s.launch_count()
         barrier()
         torch.cuda.synchronize()
@@ -186,15 +210,32 @@ def run_ours(args, rank, world, local_rank):
         barrier()
         ms = ev0.elapsed_time(ev1)
         launches = s.launch_count() - n0
-        prof = s.profile_read()
-        s.profile(False)
-        return s, dict(ms=ms, st=st, launches=launches, prof=prof, clocks=clk.summary(), setup_s=setup_s)
+        return s, dict(ms=ms, st=st, launches=launches, clocks=clk.summary(), setup_s=setup_s)
 
     precision = cfdfs.MIXED if args.precision == "mixed" else cfdfs.FP64
-    s, r = timed_solver(precision, args.steps, args.warmup)
+    s, r = timed_solver(precision, learned, args.steps, args.warmup)
     info = s.refresh()
     ms_max = max_over_ranks(r["ms"])
     value = world * args.steps / (ms_max / 1000.0)
+
+    # the plain FP64 Jacobi-PCG path on the same workload and the same steps
+    # (denominator of the headline target, and the accuracy reference)
+    fp64, acc = None, None
+    if args.fp64_steps and not (precision == cfdfs.FP64 and not learned):
+        s64, r64 = timed_solver(cfdfs.FP64, False, args.steps, args.warmup)
+        ms64 = max_over_ranks(r64["ms"])
+        fp64 = dict(steps=args.steps, steps_per_s=round(world * args.steps / (ms64 / 1000.0), 4),
+                    ms_per_step=round(ms64 / args.steps, 3),
+                    cg_iters_per_step=round(r64["st"].cg_iters / max(1, r64["st"].steps), 1))
+        U1, P1 = s.state()
+        U0, P0 = s64.state()
+        d1, d0 = s.vector("DIV"), s64.vector("DIV")
+        rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+        acc = {"u_rel_l2": rel(U1, U0), "p_rel_l2": rel(P1, P0), "div_max": float(np.abs(d1).max()),
+               "div_max_fp64": float(np.abs(d0).max()),
+               "vs": f"FP64 Jacobi-PCG GPU path after the same {args.warmup + args.steps} steps (that path "
+                     f"matches the FP64 oracle to <= 1e-6 per field in the parity tests)"}
+        s64.close()
 
     # e2e through the C ABI with host buffers: per step the state goes host ->
     # device from pinned memory, one step runs, the new state comes back.
@@ -222,38 +263,44 @@ def run_ours(args, rank, world, local_rank):
     e2e_value = world * n_e2e / (e2e_ms / 1000.0)
     state_bytes = (3 * info.NN + info.NNp) * 8
 
-    # roofline of the dominant kernel class in the timed region
-    prof = r["prof"]
+    # per-kernel-class event timing on a separate short pass (events around
+    # every launch would perturb the timed region), and the roofline of the
+    # dominant class
+    s.profile(True)
+    s.run(args.profile_steps)
+    prof = s.profile_read()
+    s.profile(False)
     top = max(prof, key=lambda k: prof[k]["ms"])
     p = prof[top]
     its_per_launch = (p["iters"] / p["launches"]) if p["launches"] else 0
     avg_ms = p["ms"] / max(1, p["launches"])
-    alg = algorithmic_bytes(info, top, its_per_launch, precision == cfdfs.MIXED)
     peak, peak_kind = peaks()
-    achieved = alg / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else 0.0
+    if top == "unet":
+        m = round(info.NNp ** (1 / 3))
+        alg = unet_flops((m, m, m))
+        tpeak, tkind = tensor_peak()
+        achieved = alg / (avg_ms / 1000.0) / 1e12 if avg_ms > 0 else 0.0
+        roof = {"bound": "tensor", "kernel": top, "achieved": round(achieved, 2), "peak": tpeak, "unit": "TFLOP/s",
+                "frac": round(achieved / tpeak, 4), "peak_kind": f"{tkind} bf16_tflops",
+                "algorithmic_flops_per_launch": int(alg), "avg_launch_ms": round(avg_ms, 4), "traffic": None}
+    else:
+        alg = algorithmic_bytes(info, top, its_per_launch, precision == cfdfs.MIXED)
+        achieved = alg / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else 0.0
+        roof = {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs",
+                "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(avg_ms, 4),
+                "iters_per_launch": round(its_per_launch, 1), "traffic": None}
     total_ms = sum(v["ms"] for v in prof.values())
     kernels = {k: dict(launches=v["launches"], ms=round(v["ms"], 3),
                        share=round(v["ms"] / total_ms, 4) if total_ms else 0.0,
                        iters=v["iters"]) for k, v in prof.items() if v["launches"]}
     s.close()
 
-    # the plain FP64 Jacobi-PCG path on the same workload (denominator of the
-    # headline target), fewer steps
-    fp64 = None
-    if args.fp64_steps > 0 and precision != cfdfs.FP64:
-        s64, r64 = timed_solver(cfdfs.FP64, args.fp64_steps, args.warmup)
-        ms64 = max_over_ranks(r64["ms"])
-        fp64 = dict(steps=args.fp64_steps, steps_per_s=round(world * args.fp64_steps / (ms64 / 1000.0), 4),
-                    ms_per_step=round(ms64 / args.fp64_steps, 3),
-                    cg_iters_per_step=round(r64["st"].cg_iters / max(1, r64["st"].steps), 1))
-        s64.close()
-
     out = None
     if rank == 0:
         cpu = None
         if world == 1 and args.cpu_baseline:
             cpu = cpu_baseline(deck, budget_s=args.cpu_budget)
-        traffic = None
         out = {
             "metric": METRIC,
             "value": round(value, 4),
@@ -265,20 +312,21 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32+f64" if precision == cfdfs.MIXED else "f64",
+            "dtype": ("f32+f64" if precision == cfdfs.MIXED else "f64") + ("+bf16" if learned else ""),
             "data": "synthetic: generated structured cavity deck (no dataset); fluid starts at rest",
             "config": {"workload": WORKLOAD, "elements": args.n ** 3, "precision": args.precision,
-                       "precond": "jacobi", "ngp": 8, "cg_rtol": 1e-8, "cg_x0": "zero",
+                       "precond": "learned U-Net in flexible CG (Jacobi-PCG fallback)" if learned else "jacobi",
+                       "weights": os.path.relpath(args.weights, ROOT) if learned else None,
+                       "ngp": 8, "cg_rtol": 1e-8, "cg_x0": "zero",
                        "timed_steps": f"steps {args.warmup + 1}..{args.warmup + args.steps} of the run from rest",
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush needed)",
                        "setup_s": round(r["setup_s"], 2)},
             "cg_iters_per_step": round(r["st"].cg_iters / max(1, r["st"].steps), 1),
             "subiters_per_step": round(r["st"].subiters / max(1, r["st"].steps), 2),
             "fp64_path": fp64,
-            "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs",
-                         "algorithmic_bytes_per_launch": int(alg), "avg_launch_ms": round(avg_ms, 4),
-                         "iters_per_launch": round(its_per_launch, 1), "traffic": traffic},
+            "speedup_vs_fp64": round(value / fp64["steps_per_s"], 3) if fp64 else None,
+            "accuracy": acc,
+            "roofline": roof,
             "kernels": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 4), "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
@@ -355,13 +403,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--n", type=int, default=N_ELEM, help="elements per side (64 = the headline workload)")
-    ap.add_argument("--fp64-steps", type=int, default=5)
+    ap.add_argument("--precond", default=None, choices=["learned", "jacobi"],
+                    help="default: learned when the weight file exists")
+    ap.add_argument("--weights", default=WEIGHTS)
+    ap.add_argument("--fp64-steps", type=int, default=1, help="0 skips the FP64 Jacobi-PCG comparison run")
+    ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cg-maxit", type=int, default=5000)
     ap.add_argument("--cpu-budget", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.precond is None:
+        args.precond = "learned" if os.path.exists(args.weights) else "jacobi"
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
     local_rank = _env_int("LOCAL_RANK", 0)

@@ -65,7 +65,7 @@ class SolveStats(C.Structure):
 
 class RunStats(C.Structure):
     _fields_ = [("steps", C.c_int), ("subiters", C.c_longlong), ("cg_iters", C.c_longlong), ("steady", C.c_int),
-                ("maxAcc", C.c_double), ("last_iter", C.c_int)]
+                ("maxAcc", C.c_double), ("last_iter", C.c_int), ("fallbacks", C.c_int)]
 
 
 _lib = None

@@ -11,9 +11,9 @@ t = (e_k - D^-1 r_k) d / s, with s = RMS(r_k), D the diagonal of Z and d its
 median entry: neither the residual's size nor the mesh spacing reaches the
 network, and a network that outputs zero leaves plain Jacobi.  Cavity runs
 draw Re ~ U[100, 1000] and lid speed ~ U[0.5, 1.5] from
-numpy.random.Generator(PCG64(seed)), with dt = 0.002 / max(1, lid) so that
-the explicit convection step stays within the CFL number of the 64^3
-benchmark case; duct runs use the bent duct with a parabolic inlet.
+numpy.random.Generator(PCG64(seed)), with dt = 0.002 capped by
+``stable_dt`` (the scheme treats convection and viscosity explicitly); duct
+runs use the bent duct with a parabolic inlet.
 
 Run ``python -m cfdfs.learned --out weights.bin`` on a GPU machine; it
 writes the weights and a JSON log of the data, the loss curve and the
@@ -38,6 +38,16 @@ def cavity_params(seed: int):
     """(Re, lid speed) of a seeded cavity run."""
     rng = np.random.Generator(np.random.PCG64(seed))
     return float(rng.uniform(100.0, 1000.0)), float(rng.uniform(0.5, 1.5))
+
+
+def stable_dt(dt: float, re: float, lid: float, n: int) -> float:
+    """dt capped for the explicit steps of the scheme: the convective number
+    lid dt / h_v stays at or below that of the 64^3, lid-1 benchmark case, and
+    the diffusion number nu dt / h_v^2 at or below 0.08, where h_v = 1/(2n)
+    is the velocity-node spacing and nu = lid / re."""
+    nu = lid / re
+    hv = 1.0 / (2 * n)
+    return min(dt / max(1.0, lid), 0.08 * hv * hv / nu)
 
 
 class PairSampler:
@@ -105,7 +115,7 @@ def cavity_pairs(seeds, n=64, dt=0.002, snap_steps=(1, 5, 15, 35, 70, 100), devi
     tmpdir = tmpdir or tempfile.mkdtemp()
     for seed in seeds:
         re, lid = cavity_params(seed)
-        dts = dt / max(1.0, lid)
+        dts = stable_dt(dt, re, lid, n)
         deck = meshgen.write_cavity(os.path.join(tmpdir, f"cav_{seed}.inp"),
                                     meshgen.CavitySpec(n, re=re, dt=dts, steps=max(snap_steps), ngp=8, lid=lid))
         ps = PairSampler(deck, (n + 1,) * 3, device=device)
@@ -200,24 +210,57 @@ def fcg_eval(net_path: str | None, deck: str, steps: int, precision: int, dims=N
     t0 = time.time()
     st = s.run(steps)
     el = time.time() - t0
-    res = dict(steps=st.steps, cg_iters=int(st.cg_iters), subiters=int(st.subiters),
+    res = dict(steps=st.steps, cg_iters=int(st.cg_iters), subiters=int(st.subiters), fallbacks=int(st.fallbacks),
                its_per_solve=st.cg_iters / max(1, st.subiters), ms_per_step=1e3 * el / max(1, st.steps))
     s.close()
     return res
+
+
+def energy_quality(ps: PairSampler, net: UNet, rhs, ks=(0, 10, 100)):
+    """For pairs from one right-hand side: the relative Z-norm error left by
+    the best multiple of the preconditioned residual, min_a ||e - a B(r)||_Z
+    / ||e||_Z, for B = Jacobi (D^-1 r) and B = the learned preconditioner
+    (D^-1 r + network correction).  Smaller is better; 0 = exact solve."""
+    shape = ps.dims[::-1]
+    out = []
+    zmul = lambda v: -ps.pair.pressure_residual(np.zeros(ps.n), v)[0]
+    ps.pair.set_options(cg_rtol=1e-12, cg_maxit=20000)
+    xs, _ = ps.pair.pressure_solve(rhs)
+    for k in ks:
+        if k == 0:
+            xk = np.zeros(ps.n)
+        else:
+            ps.pair.set_options(cg_maxit=k)
+            xk, _ = ps.pair.pressure_solve(rhs)
+        r, nr = ps.pair.pressure_residual(rhs, xk)
+        e = xs - xk
+        s = nr / np.sqrt(ps.n)
+        bj = ps.dinv * r
+        y = net.forward((r / s).astype(np.float32).reshape(shape), ps.dims).ravel().astype(np.float64)
+        bl = bj + y * (s / ps.dscale)
+        ee = float(e @ zmul(e))
+        res = {}
+        for name, b in (("jacobi", bj), ("learned", bl)):
+            zb = zmul(b)
+            a = float(b @ zmul(e)) / float(b @ zb)
+            d = e - a * b
+            res[name] = float(np.sqrt(max(d @ zmul(d), 0.0) / ee))
+        out.append(dict(k=k, **res))
+    return out
 
 
 def main(argv=None):
     import torch
 
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--out", required=True, help="weight file to write")
+    ap.add_argument("--out", required=True, help="weight file to write (one per variant: <out>.<i>)")
     ap.add_argument("--log", default=None, help="JSON log (default: <out>.json)")
     ap.add_argument("--train-seeds", type=int, default=30)
     ap.add_argument("--n", type=int, default=64)
-    ap.add_argument("--budget", type=float, default=300.0, help="training seconds")
+    ap.add_argument("--budget", type=float, default=300.0, help="training seconds per variant")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--batch", type=int, default=4)
-    ap.add_argument("--w-h1", type=float, default=0.0)
+    ap.add_argument("--variants", default="1,1", help="loss weights 'w_l2,w_h1;w_l2,w_h1;...'")
     ap.add_argument("--no-duct", action="store_true")
     ap.add_argument("--eval-steps", type=int, default=10)
     ap.add_argument("--init", default=None, help="start from these weights")
@@ -242,34 +285,49 @@ def main(argv=None):
         sets.append((torch.from_numpy(dx).cuda(), torch.from_numpy(dt_).cuda(), meshgen.duct_grid_dims(), len(dx)))
     log["data_seconds"] = time.time() - t0
     del cx, ct
-    net = UNet(device=0, seed=1234)
-    if a.init:
-        net.read(a.init)
-    net.set_loss(1.0, a.w_h1)
-    log["val_loss_init"] = eval_loss(net, vx, vt, dims_c)
-    t1 = time.time()
-    train(net, sets, a.budget, lr0=a.lr, batch=a.batch, log=log)
-    log["train_seconds"] = time.time() - t1
-    log["val_loss"] = eval_loss(net, vx, vt, dims_c)
-    net.save(a.out)
-    # held-out evaluation: the 64^3 benchmark cavity (Re 1000, lid 1) and an
-    # unseen seed, FP64 and mixed, learned vs Jacobi
+    # held-out evaluation decks: the 64^3 benchmark cavity (Re 1000, lid 1)
+    # and an unseen seed
     tmp = tempfile.mkdtemp()
-    ev = {}
     decks = {"c3_re1000": meshgen.write_cavity(os.path.join(tmp, "c3.inp"),
                                                meshgen.CavitySpec(a.n, re=1000, dt=0.002, steps=100, ngp=8))}
     re, lid = cavity_params(10_000)
-    decks["seed10000"] = meshgen.write_cavity(os.path.join(tmp, "h.inp"),
-                                              meshgen.CavitySpec(a.n, re=re, dt=0.002, steps=100, ngp=8, lid=lid))
+    decks["seed10000"] = meshgen.write_cavity(
+        os.path.join(tmp, "h.inp"), meshgen.CavitySpec(a.n, re=re, dt=stable_dt(0.002, re, lid, a.n), steps=100,
+                                                       ngp=8, lid=lid))
+    ps = PairSampler(decks["c3_re1000"], dims_c)
+    rhs_eval = ps.advance(20, iters=(1,))[0]
+    log["variants"] = []
+    for i, spec in enumerate(a.variants.split(";")):
+        w_l2, w_h1 = (float(v) for v in spec.split(","))
+        path = f"{a.out}.{i}"
+        net = UNet(device=0, seed=1234)
+        if a.init:
+            net.read(a.init)
+        net.set_loss(w_l2, w_h1)
+        vl = dict(w_l2=w_l2, w_h1=w_h1, weights=path, val_loss_init=eval_loss(net, vx, vt, dims_c))
+        t1 = time.time()
+        train(net, sets, a.budget, lr0=a.lr, batch=a.batch, log=vl)
+        vl["train_seconds"] = time.time() - t1
+        vl["val_loss"] = eval_loss(net, vx, vt, dims_c)
+        vl["energy_quality"] = energy_quality(ps, net, rhs_eval)
+        net.save(path)
+        ev = {}
+        for name, deck in decks.items():
+            for prec, pname in ((FP64, "fp64"), (MIXED, "mixed")):
+                ev[f"{name}_{pname}_learned"] = fcg_eval(path, deck, a.eval_steps, prec, dims_c)
+        vl["eval"] = ev
+        net.close()
+        log["variants"].append(vl)
+    ps.close()
+    base = {}
     for name, deck in decks.items():
         for prec, pname in ((FP64, "fp64"), (MIXED, "mixed")):
-            ev[f"{name}_{pname}_jacobi"] = fcg_eval(None, deck, a.eval_steps, prec)
-            ev[f"{name}_{pname}_learned"] = fcg_eval(a.out, deck, a.eval_steps, prec, dims_c)
-    log["eval"] = ev
+            base[f"{name}_{pname}_jacobi"] = fcg_eval(None, deck, a.eval_steps, prec)
+    log["eval_jacobi"] = base
     with open(a.log or a.out + ".json", "w") as f:
         json.dump(log, f, indent=1)
-    print(json.dumps(dict(val_loss_init=log["val_loss_init"], val_loss=log["val_loss"],
-                          steps=log["train_steps"], eval=ev), indent=1))
+    print(json.dumps(dict(jacobi=base, variants=[{k: v for k, v in vl.items() if k != "train_curve"}
+                                                 for vl in log["variants"]]), indent=1))
 
 
 if __name__ == "__main__":

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -36,6 +37,35 @@ using namespace cfd;
 struct cfd_unet {
   UnetNet net;
 };
+
+namespace {
+constexpr int kFcgBatch = 4;  // flexible-CG iterations per captured graph
+// An instantiated graph of kFcgBatch flexible-CG iterations and the buffers
+// and network state it was captured with.
+struct FcgGraph {
+  struct Key {
+    const void *b, *x, *work;
+    const cfd_unet* net;
+    int gen, plan_gen;
+    bool tc;
+    const int* pmap;
+    const void* dinv;
+    double dscale;
+    int n;
+    bool operator==(const Key& o) const {
+      return b == o.b && x == o.x && work == o.work && net == o.net && gen == o.gen && plan_gen == o.plan_gen &&
+             tc == o.tc && pmap == o.pmap && dinv == o.dinv && dscale == o.dscale && n == o.n;
+    }
+  } key{};
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0;
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+  }
+  ~FcgGraph() { reset(); }
+};
+}  // namespace
 
 namespace {
 
@@ -118,6 +148,8 @@ struct cfd_ctx {
   DevBuf<double> fcg_sc, fcg_part;
   DevBuf<int> fcg_done;
   int fcg_window = 25;
+  bool fcg_use_graph = true;
+  FcgGraph fcg_graph[2];  // FP32 inner solves, FP64 solves
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
 
@@ -437,22 +469,71 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
     dinv = c->zdinv32.p;
   else
     dinv = c->zdinv.p;
+  // one flexible-CG iteration: U-Net apply, SpMV + dots, coefficients, update
+  auto iteration = [&](bool counted) -> int {
+    const long long l0 = net.launches;
+    auto unet = [&]() -> cudaError_t {
+      cudaError_t e = unet_input(n, a.r, pmap, a.st.sc + kFcgRR, 0.0, net.act[0], a.st.done, s);
+      if (e == cudaSuccess) e = net.forward(s, nullptr, a.st.done);
+      if (e == cudaSuccess)
+        e = unet_output(n, net.out, pmap, a.st.sc + kFcgRR, c->unet_dscale, dinv, a.r, a.z, a.st.done, s);
+      return e;
+    };
+    if (counted) {
+      KL(CFD_K_UNET, unet());
+      KL(CFD_K_FCG, launch_fcg_spmv<VT>(a, s));
+      KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
+      c->launches += net.launches - l0 + 1 + 2;
+    } else {
+      CU(unet());
+      CU(launch_fcg_spmv<VT>(a, s));
+      CU(launch_fcg_update<VT>(a, s));
+    }
+    return CFD_OK;
+  };
+  // CUDA graph of kFcgBatch iterations, captured once per buffer / network
+  // configuration and replayed until the done flag stops the kernels
+  FcgGraph* G = nullptr;
+  if (c->fcg_use_graph && !c->prof_on) {
+    CU(net.prepare_tc(s));  // packs and plans outside the capture
+    FcgGraph& g = c->fcg_graph[sizeof(VT) == 4 ? 0 : 1];
+    FcgGraph::Key key{a.b, a.x, a.r, c->unet, net.gen, net.plan_gen, net.tc_enabled, pmap, dinv, c->unet_dscale, n};
+    if (!g.exec || !(g.key == key)) {
+      g.reset();
+      const long long l0 = net.launches;
+      CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+      int rc = CFD_OK;
+      for (int k = 0; k < kFcgBatch && rc == CFD_OK; k++) rc = iteration(false);
+      cudaGraph_t graph = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+      }
+      CU(ce);
+      ce = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      CU(ce);
+      g.key = key;
+      g.launches = (net.launches - l0) + kFcgBatch * 3;
+    }
+    G = &g;
+  }
   int issued = 0, batch = 2;
   double rr_prev = -1;
   for (;;) {
-    for (int k = 0; k < batch; k++) {
-      const long long l0 = net.launches;
-      KL(CFD_K_UNET, ([&]() -> cudaError_t {
-           cudaError_t e = unet_input(n, a.r, pmap, a.st.sc + kFcgRR, 0.0, net.act[0], a.st.done, s);
-           if (e == cudaSuccess) e = net.forward(s, nullptr, a.st.done);
-           if (e == cudaSuccess)
-             e = unet_output(n, net.out, pmap, a.st.sc + kFcgRR, c->unet_dscale, dinv, a.r, a.z, a.st.done, s);
-           return e;
-         })());
-      c->launches += net.launches - l0 + 1;
-      KL(CFD_K_FCG, launch_fcg_spmv<VT>(a, s));
-      KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
-      c->launches += 2;
+    if (G) {
+      const int reps = (batch + kFcgBatch - 1) / kFcgBatch;
+      for (int k = 0; k < reps; k++) {
+        CU(cudaGraphLaunch(G->exec, s));
+        c->launches += G->launches;
+      }
+      batch = reps * kFcgBatch;
+    } else {
+      for (int k = 0; k < batch; k++) {
+        int rc = iteration(true);
+        if (rc) return rc;
+      }
     }
     issued += batch;
     CU(cudaMemcpyAsync(c->h_small, c->fcg_sc.p, kFcgScalars * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -510,11 +591,13 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
         warm = 1;
       }
     }
+    int more = 0;
     if (!learned(c) || z.fallback) {
       int rc = run_pcg64(c, b, x, warm, rtol, std::max(1, c->opt.cg_maxit - used), res);
       if (rc) return rc;
+      more = (int)res[0];
     }
-    z.iterations = used + (int)res[0];
+    z.iterations = used + more;
     z.relres = res[1];
     z.status = (int)res[2];
   } else {
@@ -614,6 +697,7 @@ int cfd_create(cfd_ctx** out, int device) {
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return CFD_E_CUDA;
   if (cudaMallocHost((void**)&c->h_small, 64 * sizeof(double)) != cudaSuccess) return CFD_E_CUDA;
+  if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   *out = c.release();
   return CFD_OK;
 }
@@ -925,6 +1009,7 @@ int cfd_run(cfd_ctx* c, int nsteps, cfd_run_stats* st) {
       if ((rc = cfd_step2(c, iter, &ss))) return rc;
       if ((rc = cfd_step3(c, iter))) return rc;
       r.cg_iters += ss.iterations;
+      r.fallbacks += ss.fallback;
       r.subiters++;
       int conv = 0;
       if ((rc = cfd_check_iter(c, P.tolerance, &conv, nullptr))) return rc;
@@ -1403,6 +1488,8 @@ int cfd_unet_train_batch(cfd_unet* u, const int dims[3], int nb, const float* x,
 int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_vox) {
   if (!c) return CFD_E_BADARG;
   if (!u) {
+    c->fcg_graph[0].reset();
+    c->fcg_graph[1].reset();
     c->unet = nullptr;
     c->unet_owned.reset();
     return CFD_OK;
@@ -1425,6 +1512,8 @@ int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_
     CU(cudaStreamSynchronize(c->stream));
   }
   for (int a = 0; a < 3; a++) c->udims[a] = dims[a];
+  c->fcg_graph[0].reset();
+  c->fcg_graph[1].reset();
   {
     std::vector<double> dg(nv);
     CU(cudaStreamSynchronize(c->stream));

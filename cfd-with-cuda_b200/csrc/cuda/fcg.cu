@@ -74,6 +74,10 @@ __global__ void k_fcg_start2(FcgState st, int nblk) {
     sc[kFcgRRMark] = v[1];
     sc[kFcgIt] = 0;
     sc[kFcgPQ] = 1;
+    sc[kFcgRtol] = st.rtol;
+    sc[kFcgStall2] = st.stall2;
+    sc[kFcgMaxit] = st.maxit;
+    sc[kFcgWindow] = st.window;
     int done = 0;
     double status = -1;
     if (!isfinite(v[0]) || !isfinite(v[1])) {
@@ -162,20 +166,22 @@ __global__ void k_fcg_check(FcgState st, int nblk) {
     double* sc = st.sc;
     const double rr = v[0];
     const double it = sc[kFcgIt] + 1;
+    const double rtol = sc[kFcgRtol], window = sc[kFcgWindow];
     sc[kFcgIt] = it;
     sc[kFcgRR] = rr;
+    const bool mark = window > 0 && fmod(it, window) == 0.0;
     int done = 1;
     if (!isfinite(rr))
       sc[kFcgStatus] = 2;
-    else if (rr <= st.rtol * st.rtol * sc[kFcgBB])
+    else if (rr <= rtol * rtol * sc[kFcgBB])
       sc[kFcgStatus] = 0;
-    else if (it >= st.maxit)
+    else if (it >= sc[kFcgMaxit])
       sc[kFcgStatus] = 1;
-    else if (st.window > 0 && fmod(it, (double)st.window) == 0.0 && rr > st.stall2 * sc[kFcgRRMark])
+    else if (mark && rr > sc[kFcgStall2] * sc[kFcgRRMark])
       sc[kFcgStatus] = 4;
     else
       done = 0;
-    if (!done && st.window > 0 && fmod(it, (double)st.window) == 0.0) sc[kFcgRRMark] = rr;
+    if (!done && mark) sc[kFcgRRMark] = rr;
     st.done[0] = done;
   }
 }

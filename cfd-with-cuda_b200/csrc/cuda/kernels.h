@@ -156,12 +156,17 @@ struct PcgArgs {
 // sc[]: indices below; status -1 running, 0 converged, 1 iteration limit,
 // 2 non-finite, 4 stalled (the residual fell by less than sqrt(stall2) over
 // the last window iterations, or the direction broke down).
-enum { kFcgRR = 0, kFcgBB, kFcgPQ, kFcgAlpha, kFcgBeta, kFcgIt, kFcgStatus, kFcgRRMark, kFcgScalars = 8 };
+enum {
+  kFcgRR = 0, kFcgBB, kFcgPQ, kFcgAlpha, kFcgBeta, kFcgIt, kFcgStatus, kFcgRRMark,
+  kFcgRtol, kFcgStall2, kFcgMaxit, kFcgWindow, kFcgScalars = 12
+};
+// The iteration kernels read the solve's settings from sc[] (written by the
+// start kernel), so a captured sequence of iterations serves every solve.
 struct FcgState {
   double* sc;    // kFcgScalars words
   double* part;  // 4 x blocks
   int* done;     // kernels return at once while *done != 0
-  double rtol, stall2;
+  double rtol, stall2;  // read by the start kernel only
   int maxit, window;
 };
 template <class VT> struct FcgArgs {

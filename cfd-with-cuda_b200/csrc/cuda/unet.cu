@@ -15,6 +15,10 @@ namespace {
 
 __device__ __forceinline__ float bf(const __nv_bfloat16 v) { return __bfloat162float(v); }
 
+struct Dims3 {
+  int c[3], f[3];  // coarse and fine grid dims
+};
+
 __device__ __forceinline__ void vox3(long long v, const int* d, int& x, int& y, int& z) {
   x = (int)(v % d[0]);
   long long t = v / d[0];
@@ -71,6 +75,93 @@ __global__ void __launch_bounds__(128) k_conv_fwd(ConvDesc d) {
       if (d.act && y < 0.f) y *= kLeaky;
       if (d.out) d.out[v * d.cout + co0 + c] = __float2bfloat16(y);
       if (d.out_f32) d.out_f32[v * d.cout + co0 + c] = y;
+    }
+  }
+}
+
+// Single-input-channel convolution (the first layer) with 16 outputs: one
+// thread per output voxel, weights as float4 rows in shared memory, 32-bit
+// index arithmetic, two 16-byte stores per voxel.
+__global__ void __launch_bounds__(256, 3) k_conv_c1to16(ConvDesc d) {
+  __shared__ float4 sw[27 * 4];
+  __shared__ float sb[16];
+  if (d.skip && *d.skip) return;
+  for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) ((float*)sw)[i] = bf(d.w[i]);
+  if (threadIdx.x < 16) sb[threadIdx.x] = d.bias[threadIdx.x];
+  __syncthreads();
+  const int nx = d.out_dims[0], ny = d.out_dims[1], nz = d.out_dims[2];
+  const int nv = nx * ny * nz;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    const int x = v % nx, t = v / nx, y = t % ny, z = t / ny;
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) acc[c] = sb[c];
+#pragma unroll 3
+    for (int k = 0; k < 27; k++) {
+      const int ix = x + k % 3 - 1, iy = y + (k / 3) % 3 - 1, iz = z + k / 9 - 1;
+      if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) continue;
+      const float a = bf(d.inA[ix + nx * (iy + ny * iz)]);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float4 w = sw[4 * k + q];
+        acc[4 * q] += a * w.x;
+        acc[4 * q + 1] += a * w.y;
+        acc[4 * q + 2] += a * w.z;
+        acc[4 * q + 3] += a * w.w;
+      }
+    }
+    __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+    for (int c = 0; c < 16; c++) {
+      float yv = acc[c];
+      if (d.act && yv < 0.f) yv *= kLeaky;
+      o[c] = __float2bfloat16(yv);
+    }
+    uint4* dst = (uint4*)(d.out + (size_t)v * 16);
+    dst[0] = ((const uint4*)o)[0];
+    dst[1] = ((const uint4*)o)[1];
+  }
+}
+
+// Prolongation plus skip for CH channels: one thread per fine voxel, 16-byte
+// vector loads and stores, 32-bit index arithmetic.
+template <int CH>
+__global__ void __launch_bounds__(256) k_up_fwd_v(Dims3 g, const __nv_bfloat16* __restrict__ in,
+                                                  const __nv_bfloat16* __restrict__ skip, __nv_bfloat16* out,
+                                                  const int* skipflag) {
+  if (skipflag && *skipflag) return;
+  const int fx = g.f[0], fy = g.f[1], fz = g.f[2], cx = g.c[0], cy = g.c[1];
+  const int nf = fx * fy * fz;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nf; v += gridDim.x * blockDim.x) {
+    const int X = v % fx, t = v / fx, Y = t % fy, Z = t / fy;
+    float acc[CH];
+#pragma unroll
+    for (int c = 0; c < CH; c++) acc[c] = 0.f;
+    const int nxs = (X & 1) ? 2 : 1, nys = (Y & 1) ? 2 : 1, nzs = (Z & 1) ? 2 : 1;
+    const float w = ((X & 1) ? 0.5f : 1.f) * ((Y & 1) ? 0.5f : 1.f) * ((Z & 1) ? 0.5f : 1.f);
+    for (int zz = 0; zz < nzs; zz++)
+      for (int yy = 0; yy < nys; yy++)
+        for (int xx = 0; xx < nxs; xx++) {
+          const int c0 = ((X >> 1) + xx) + cx * (((Y >> 1) + yy) + cy * ((Z >> 1) + zz));
+          const uint4* src = (const uint4*)(in + (size_t)c0 * CH);
+#pragma unroll
+          for (int q = 0; q < CH / 8; q++) {
+            uint4 u = src[q];
+            const __nv_bfloat16* h = (const __nv_bfloat16*)&u;
+#pragma unroll
+            for (int i = 0; i < 8; i++) acc[8 * q + i] += bf(h[i]);
+          }
+        }
+    const uint4* sk = (const uint4*)(skip + (size_t)v * CH);
+    uint4* dst = (uint4*)(out + (size_t)v * CH);
+#pragma unroll
+    for (int q = 0; q < CH / 8; q++) {
+      uint4 u = sk[q];
+      const __nv_bfloat16* h = (const __nv_bfloat16*)&u;
+      __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) o[i] = __float2bfloat16(acc[8 * q + i] * w + bf(h[i]));
+      dst[q] = *(const uint4*)o;
     }
   }
 }
@@ -209,9 +300,6 @@ __global__ void k_act_bwd(long long n, const __nv_bfloat16* __restrict__ y, floa
     if (bf(y[i]) <= 0.f) dy[i] *= kLeaky;
 }
 
-struct Dims3 {
-  int c[3], f[3];
-};
 
 __global__ void k_up_fwd(Dims3 g, int ch, const __nv_bfloat16* __restrict__ in, const __nv_bfloat16* skip,
                          __nv_bfloat16* out, const int* skipflag) {
@@ -367,6 +455,10 @@ cudaError_t conv3_forward(const ConvDesc& d, cudaStream_t s) {
   const int cin = d.ca + d.cb;
   const long long nv = (long long)d.out_dims[0] * d.out_dims[1] * d.out_dims[2];
   const int gx = grid1(nv, 128);
+  if (cin == 1 && d.cout == 16 && d.stride == 1 && d.out && !d.out_f32 && nv < (1LL << 31)) {
+    k_conv_c1to16<<<grid1(nv, 256), 256, 0, s>>>(d);
+    return cudaGetLastError();
+  }
   if (cin <= 48) {
     const size_t sm = (size_t)27 * cin * 16 * sizeof(float);
     cudaError_t e = with_smem(k_conv_fwd<16>, sm);
@@ -437,7 +529,15 @@ cudaError_t upsample_forward(const int* cdims, const int* fdims, int ch, const _
     g.c[i] = cdims[i];
     g.f[i] = fdims[i];
   }
-  const long long n = (long long)fdims[0] * fdims[1] * fdims[2] * ch;
+  const long long nf = (long long)fdims[0] * fdims[1] * fdims[2];
+  if (skip && nf < (1LL << 31) && (ch == 16 || ch == 32)) {
+    if (ch == 16)
+      k_up_fwd_v<16><<<grid1(nf), 256, 0, s>>>(g, in, skip, out, skipflag);
+    else
+      k_up_fwd_v<32><<<grid1(nf), 256, 0, s>>>(g, in, skip, out, skipflag);
+    return cudaGetLastError();
+  }
+  const long long n = nf * ch;
   k_up_fwd<<<grid1(n), 256, 0, s>>>(g, ch, in, skip, out, skipflag);
   return cudaGetLastError();
 }

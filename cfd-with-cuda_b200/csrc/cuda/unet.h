@@ -85,10 +85,11 @@ cudaError_t adam_step(long long n, float* w, const float* g, float* m, float* v,
 
 cudaError_t f32_to_bf16(long long n, const float* a, __nv_bfloat16* b, cudaStream_t s);
 
-// ---- tensor-core path (unet_tc.cu): stride-1 convolutions, cin in {16, 32,
-// 64}, cout in {16, 32, 64} or 1 with FP32 output ----
+// ---- tensor-core path (unet_tc.cu): stride-1 and stride-2 convolutions,
+// cin in {16, 32, 64}, cout in {16, 32, 64} or 1 with FP32 output ----
 struct ConvTcParams {
-  int dims[3];      // grid (input = output)
+  int dims[3];      // output grid (stride 2: the coarse grid of the input's phases)
+  int stride;       // 1, or 2 (input given as 8 parity phases, conv_tc_space_to_depth)
   int brick[3];     // output voxels per CTA along each axis
   int nb[3];        // bricks per axis
   int halo[3];      // brick + 2
@@ -112,14 +113,20 @@ struct ConvTcPlan {
   int ready;
 };
 bool conv_tc_supported(const ConvDesc& d);
-int conv_tc_slice_width(int cin, int cout);
-long long conv_tc_pack_elems(int cin, int cout);
+int conv_tc_slice_width(int cin, int cout, int stride);
+long long conv_tc_pack_elems(int cin, int cout, int stride);
 // Rearranges [27][cin][cout] BF16 weights into per-tap canonical tensor-core
 // blocks (wpack holds conv_tc_pack_elems values).
-cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, __nv_bfloat16* wpack, cudaStream_t s);
+cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
+                         cudaStream_t s);
+// Stride 2: elements of the parity-phase copy of the input (0 for stride 1)
+// and the pass that writes it (to run before each launch of the plan).
+long long conv_tc_phase_elems(const ConvDesc& d);
+cudaError_t conv_tc_space_to_depth(const ConvDesc& d, __nv_bfloat16* phase, const int* skip, cudaStream_t s);
 // Builds the launch plan (bricks, shared-memory layout, TMA descriptor) of a
-// supported convolution; 0 on success.
-int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan);
+// supported convolution (stride 2 reads the phase buffer); 0 on success.
+int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, const __nv_bfloat16* phase, int num_sms,
+                 ConvTcPlan& plan);
 // Launches a planned convolution; out_f32 (FP32-output layers) and skip
 // replace the plan's pointers for this launch.
 cudaError_t conv3_forward_tc(const ConvTcPlan& plan, float* out_f32, const int* skip, int* err, cudaStream_t s);

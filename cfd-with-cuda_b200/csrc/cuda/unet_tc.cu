@@ -12,6 +12,12 @@
 // all 27 taps for the CTA's slice of output channels are resident in shared
 // memory, pre-packed in the tensor core's canonical K-major layout.
 //
+// Stride 2 (the U-Net's down-sampling layers) runs on the same machinery
+// after a space-to-depth pass splits the fine input into its 8 parity phases
+// (voxel (2i+px, 2j+py, 2k+pz) -> phase px + 2py + 4pz at (i, j, k)): tap d
+// of output X reads phase (d != 0) at coarse index X + (d == -1 ? -1 : 0),
+// again a constant row shift inside that phase's planes (low-side halo only).
+//
 // One thread issues tcgen05.mma (M = 128 rows, N = output channels of the
 // slice, K = 16 input channels) into a 128-column TMEM accumulator; the four
 // warps read it back with tcgen05.ld (warp w owns rows 32w..32w+31), add the
@@ -32,6 +38,10 @@ namespace {
 constexpr int kTcThreads = 128;
 constexpr int kTmemCols = 128;
 constexpr unsigned long long kTcWaitNs = 2000000000ULL;
+
+struct Dims6 {
+  int c[3], f[3];
+};
 
 __device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
   // SWIZZLE_NONE, K-major canonical layout: 8-row core matrices of 16-byte
@@ -87,21 +97,21 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
                                             unsigned long long* bar) {
   asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];" ::"r"(smem_u32(dst)),
-      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+      "[%7];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
       : "memory");
 }
 
 __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ CUtensorMap tmap, ConvTcParams p) {
   if (p.skip && *p.skip) return;
   extern __shared__ __align__(1024) unsigned char smem[];
-  const int nchunk = p.cin >> 3;
+  const int nchunk = p.cin >> 3, nphase = p.stride == 2 ? 8 : 1;
   unsigned char* A = smem;
-  unsigned char* W = smem + (size_t)nchunk * p.plane_bytes;
+  unsigned char* W = smem + (size_t)nphase * nchunk * p.plane_bytes;
   const unsigned wbytes = 27u * p.cin * p.N * 2u;
   unsigned long long* bars = (unsigned long long*)(W + wbytes);  // wbytes is a multiple of 16
   unsigned* tmem_slot = (unsigned*)(bars + 2);
@@ -122,12 +132,19 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
+  float* sbias = (float*)(tmem_slot + 4);  // N floats
+  for (int i = threadIdx.x; i < p.N; i += blockDim.x) {
+    const int co = slice * p.N + i;
+    sbias[i] = co < p.cout ? p.bias[co] : 0.f;
+  }
 
   if (threadIdx.x == 0) {
     const unsigned box = (unsigned)(p.halo[0] * p.halo[1] * p.halo[2]) * 16u;
-    mbar_expect_tx(&bars[0], nchunk * box + wbytes);
-    for (int c = 0; c < nchunk; c++)
-      tma_load_4d(A + (size_t)c * p.plane_bytes, &tmap, c * 8, x0 - 1, y0 - 1, z0 - 1, &bars[0]);
+    mbar_expect_tx(&bars[0], nphase * nchunk * box + wbytes);
+    for (int ph = 0; ph < nphase; ph++)
+      for (int c = 0; c < nchunk; c++)
+        tma_load_5d(A + (size_t)(ph * nchunk + c) * p.plane_bytes, &tmap, c * 8, x0 - 1, y0 - 1, z0 - 1, ph,
+                    &bars[0]);
     bulk_g2s(W, p.wpack + (size_t)slice * 27 * p.cin * p.N, wbytes, &bars[0]);
   }
   bool ok = __syncthreads_and(mbar_wait_bounded(&bars[0], 0, kTcWaitNs));
@@ -135,25 +152,48 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
 
   const unsigned idesc = umma_idesc(p.N);
   const int tpg = kTmemCols / p.N;  // M-tiles per accumulator group
-  const unsigned a0 = smem_u32(A), w0 = smem_u32(W);
-  const unsigned wtap = (unsigned)p.cin * p.N * 2u, wk = (unsigned)(p.N >> 3) * 128u;
+  const int ksteps = p.cin >> 4;
   const int n0 = slice * p.N;
+  // Descriptor bases; per MMA only the start-address field (bits 0-13, in
+  // 16-byte units) changes, by a whole number of rows / weight blocks, so the
+  // issuing thread adds offsets to the 64-bit descriptors (shared addresses
+  // stay below 2^18 bytes, so the field never carries).
+  const unsigned long long da0 = umma_desc(smem_u32(A), (unsigned)p.plane_bytes, 128u);
+  const unsigned long long db0 = umma_desc(smem_u32(W), (unsigned)(p.N >> 3) * 128u, 128u);
+  const unsigned plane16 = (unsigned)p.plane_bytes >> 4;
+  const unsigned wtap16 = (unsigned)(p.cin * p.N * 2) >> 4, wk16 = (unsigned)(p.N >> 3) * 8u;
   int phase = 0;
   for (int g0 = 0; g0 < p.tiles && ok; g0 += tpg) {
     const int g1 = min(p.tiles, g0 + tpg);
     if (threadIdx.x == 0) {
       tc_fence_after();
+      // row offset (16-byte units, including the plane of stride-2 taps) of
+      // every tap
+      int toff[27];
+#pragma unroll
+      for (int k = 0; k < 27; k++) {
+        const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+        int off, plane0;
+        if (p.stride == 2) {
+          off = -(dx < 0) - HX * ((dy < 0) + HY * (dz < 0));
+          plane0 = ((dx != 0) + 2 * (dy != 0) + 4 * (dz != 0)) * nchunk;
+        } else {
+          off = dx + HX * (dy + HY * dz);
+          plane0 = 0;
+        }
+        toff[k] = plane0 * (int)plane16 + off;
+      }
       for (int t = g0; t < g1; t++) {
         const unsigned d = tmem + (unsigned)((t - g0) * p.N);
+        const unsigned long long dat = da0 + (unsigned)(p.q0 + 128 * t);
         unsigned acc = 0;
+#pragma unroll
         for (int k = 0; k < 27; k++) {
-          const int off = (k % 3 - 1) + HX * (((k / 3) % 3 - 1) + HY * (k / 9 - 1));
-          const unsigned row = (unsigned)(p.q0 + 128 * t + off);
-          for (int j = 0; j < (p.cin >> 4); j++) {
-            const unsigned long long da = umma_desc(a0 + (unsigned)(2 * j) * p.plane_bytes + row * 16u,
-                                                    (unsigned)p.plane_bytes, 128u);
-            const unsigned long long db = umma_desc(w0 + (unsigned)k * wtap + (unsigned)(2 * j) * wk, wk, 128u);
-            umma(d, da, db, idesc, acc);
+          const unsigned long long dak = dat + (unsigned long long)(long long)toff[k];
+          const unsigned long long dbk = db0 + (unsigned long long)k * wtap16;
+          for (int j = 0; j < ksteps; j++) {
+            umma(d, dak + (unsigned long long)(2 * j) * plane16, dbk + (unsigned long long)(2 * j) * wk16, idesc,
+                 acc);
             acc = 1;
           }
         }
@@ -181,13 +221,13 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
         tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)((t - g0) * p.N + c), acc);
         if (!valid) continue;
         if (p.out_f32) {
-          if (n0 + c == 0) p.out_f32[v] = acc[0] + p.bias[0];
+          if (n0 + c == 0) p.out_f32[v] = acc[0] + sbias[0];
           continue;
         }
         __align__(16) __nv_bfloat16 o[16];
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-          float y = acc[i] + (n0 + c + i < p.cout ? p.bias[n0 + c + i] : 0.f);
+          float y = acc[i] + sbias[c + i];
           if (p.act && y < 0.f) y *= kLeaky;
           o[i] = __float2bfloat16(y);
         }
@@ -214,6 +254,28 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
   if (warp == 0) {
     tc_fence_after();
     tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+// ph[phase][k][j][i][c] = in[2i+px][2j+py][2k+pz][c] (zero outside the fine
+// grid), phase = px + 2py + 4pz, coarse dims cd; one thread per 8 channels.
+__global__ void k_space_to_depth(const __nv_bfloat16* __restrict__ in, Dims6 g, int ch, __nv_bfloat16* ph,
+                                 const int* skip) {
+  if (skip && *skip) return;
+  const int nc = ch / 8;
+  const long long per = (long long)g.c[0] * g.c[1] * g.c[2];
+  const long long total = 8 * per * nc;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % nc);
+    const long long v = (i / nc) % per;
+    const int phs = (int)(i / (nc * per));
+    const int x = (int)(v % g.c[0]), y = (int)((v / g.c[0]) % g.c[1]), z = (int)(v / ((long long)g.c[0] * g.c[1]));
+    const int fx = 2 * x + (phs & 1), fy = 2 * y + ((phs >> 1) & 1), fz = 2 * z + (phs >> 2);
+    uint4 val = make_uint4(0, 0, 0, 0);
+    if (fx < g.f[0] && fy < g.f[1] && fz < g.f[2])
+      val = *(const uint4*)(in + ((fx + (long long)g.f[0] * (fy + (long long)g.f[1] * fz)) * ch + 8 * c));
+    *(uint4*)(ph + ((phs * per + v) * ch + 8 * c)) = val;
   }
 }
 
@@ -256,48 +318,73 @@ int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
 }  // namespace
 
-int conv_tc_slice_width(int cin, int cout) {
+int conv_tc_slice_width(int cin, int cout, int stride) {
+  // resident weights of a slice: up to 112 KiB next to a stride-1 brick, 56
+  // KiB next to the eight phase planes of a stride-2 brick
+  const long long cap = stride == 2 ? 56 * 1024 : 112 * 1024;
   int N = cout < 16 ? 16 : cout;
-  while (N > 16 && 27LL * cin * N * 2 > 112 * 1024) N /= 2;
+  while (N > 16 && 27LL * cin * N * 2 > cap) N /= 2;
   return N;
 }
 
 bool conv_tc_supported(const ConvDesc& d) {
-  return d.stride == 1 && d.cb == 0 && (d.ca == 16 || d.ca == 32 || d.ca == 64) &&
-         (d.cout == 16 || d.cout == 32 || d.cout == 64 || (d.cout == 1 && d.out_f32 && !d.out)) &&
-         d.in_dims[0] == d.out_dims[0] && d.in_dims[1] == d.out_dims[1] && d.in_dims[2] == d.out_dims[2];
+  bool dims_ok = true;
+  for (int a = 0; a < 3; a++)
+    dims_ok = dims_ok && (d.stride == 1 ? d.in_dims[a] == d.out_dims[a] : d.in_dims[a] == 2 * d.out_dims[a] - 1);
+  return (d.stride == 1 || d.stride == 2) && dims_ok && d.cb == 0 && (d.ca == 16 || d.ca == 32 || d.ca == 64) &&
+         (d.cout == 16 || d.cout == 32 || d.cout == 64 || (d.cout == 1 && d.out_f32 && !d.out));
 }
 
-cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, __nv_bfloat16* wpack, cudaStream_t s) {
-  const int N = conv_tc_slice_width(cin, cout);
+long long conv_tc_phase_elems(const ConvDesc& d) {
+  return d.stride == 2 ? 8LL * d.out_dims[0] * d.out_dims[1] * d.out_dims[2] * d.ca : 0;
+}
+
+cudaError_t conv_tc_space_to_depth(const ConvDesc& d, __nv_bfloat16* phase, const int* skip, cudaStream_t s) {
+  Dims6 g;
+  for (int a = 0; a < 3; a++) {
+    g.c[a] = d.out_dims[a];
+    g.f[a] = d.in_dims[a];
+  }
+  const long long total = conv_tc_phase_elems(d) / 8;
+  k_space_to_depth<<<(int)std::min<long long>((total + 255) / 256, 148 * 16), 256, 0, s>>>(d.inA, g, d.ca, phase,
+                                                                                           skip);
+  return cudaGetLastError();
+}
+
+cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
+                         cudaStream_t s) {
+  const int N = conv_tc_slice_width(cin, cout, stride);
   const int ns = ceil_div(cout < 16 ? 16 : cout, N);
   const long long total = (long long)ns * 27 * cin * N;
   k_pack_tc<<<(int)std::min<long long>((total + 255) / 256, 4096), 256, 0, s>>>(w, cin, cout, N, ns, wpack);
   return cudaGetLastError();
 }
 
-long long conv_tc_pack_elems(int cin, int cout) {
-  const int N = conv_tc_slice_width(cin, cout);
+long long conv_tc_pack_elems(int cin, int cout, int stride) {
+  const int N = conv_tc_slice_width(cin, cout, stride);
   return (long long)ceil_div(cout < 16 ? 16 : cout, N) * 27 * cin * N;
 }
 
-int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan) {
+int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, const __nv_bfloat16* phase, int num_sms,
+                 ConvTcPlan& plan) {
   std::memset(&plan, 0, sizeof(plan));
   if (!conv_tc_supported(d)) return -1;
+  if (d.stride == 2 && !phase) return -1;
   EncodeTiled enc = encoder();
   if (!enc) return -2;
   ConvTcParams& p = plan.p;
   for (int a = 0; a < 3; a++) p.dims[a] = d.out_dims[a];
+  p.stride = d.stride;
   p.cin = d.ca;
   p.cout = d.cout;
-  p.N = conv_tc_slice_width(d.ca, d.cout);
+  p.N = conv_tc_slice_width(d.ca, d.cout, d.stride);
   p.nslices = ceil_div(d.cout < 16 ? 16 : d.cout, p.N);
-  const int nchunk = p.cin / 8;
+  const int nchunk = p.cin / 8, nphase = d.stride == 2 ? 8 : 1, hpad = d.stride == 2 ? 1 : 2;
   const long long wbytes = 27LL * p.cin * p.N * 2;
   for (int a = 0; a < 2; a++) {
     p.nb[a] = ceil_div(p.dims[a], 16);
     p.brick[a] = ceil_div(p.dims[a], p.nb[a]);
-    p.halo[a] = p.brick[a] + 2;
+    p.halo[a] = p.brick[a] + hpad;
   }
   // bricks along z: enough CTAs for two per SM, within the shared-memory budget
   const long long budget = 200 * 1024;
@@ -305,24 +392,25 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
   int tz = std::max(1, ceil_div(p.dims[2], std::max(1, target)));
   for (;; tz--) {
     p.brick[2] = tz;
-    p.halo[2] = tz + 2;
+    p.halo[2] = tz + hpad;
     const int HX = p.halo[0], HY = p.halo[1];
     p.q0 = 1 + HX + HX * HY;
     const int last = p.brick[0] + HX * (p.brick[1] + HY * p.brick[2]);
     p.tiles = ceil_div(last - p.q0 + 1, 128);
-    const int off_max = 1 + HX + HX * HY;
+    const int off_max = d.stride == 2 ? 0 : 1 + HX + HX * HY;
     int rows = std::max(HX * HY * p.halo[2], p.q0 + 128 * p.tiles + off_max);
     p.rows = (rows + 7) & ~7;
     p.plane_bytes = ((p.rows * 16) + 1023) & ~1023;
-    plan.smem = (size_t)nchunk * p.plane_bytes + wbytes + 64;
+    plan.smem = (size_t)nphase * nchunk * p.plane_bytes + wbytes + 64 + 4 * p.N;
     if ((long long)plan.smem <= budget || tz == 1) break;
   }
   if (plan.smem > 227 * 1024) return -3;
   {
     // every shared-memory row the MMAs address lies inside its plane, every
     // TMA box dimension is legal, and a group of tiles fits the TMEM columns
-    const int HX = p.halo[0], HY = p.halo[1], off_max = 1 + HX + HX * HY;
-    if (p.q0 - off_max < 0 || p.q0 + 128 * p.tiles - 1 + off_max >= p.rows || p.rows * 16 > p.plane_bytes ||
+    const int HX = p.halo[0], HY = p.halo[1];
+    const int off_min = 1 + HX + HX * HY, off_max = d.stride == 2 ? 0 : off_min;
+    if (p.q0 - off_min < 0 || p.q0 + 128 * p.tiles - 1 + off_max >= p.rows || p.rows * 16 > p.plane_bytes ||
         p.halo[0] > 256 || p.halo[1] > 256 || p.halo[2] > 256 || p.tiles < 1 || p.N > kTmemCols ||
         p.N % 16 != 0 || p.cin % 16 != 0)
       return -5;
@@ -335,15 +423,19 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
   p.act = d.act;
   p.skip = d.skip;
   plan.grid_x = p.nb[0] * p.nb[1] * p.nb[2];
-  // input tensor [Z][Y][X][C] BF16; box = one 8-channel chunk of the halo brick
-  cuuint64_t gdim[4] = {(cuuint64_t)p.cin, (cuuint64_t)p.dims[0], (cuuint64_t)p.dims[1], (cuuint64_t)p.dims[2]};
-  cuuint64_t gstride[3] = {(cuuint64_t)p.cin * 2, (cuuint64_t)p.cin * 2 * p.dims[0],
-                           (cuuint64_t)p.cin * 2 * p.dims[0] * p.dims[1]};
-  cuuint32_t box[4] = {8, (cuuint32_t)p.halo[0], (cuuint32_t)p.halo[1], (cuuint32_t)p.halo[2]};
-  cuuint32_t estride[4] = {1, 1, 1, 1};
-  CUresult r = enc(&plan.tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void*)d.inA, gdim, gstride, box, estride,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  // input [phase][Z][Y][X][C] BF16 (one phase for stride 1: the tensor
+  // itself; eight coarse-grid phases for stride 2); box = one 8-channel chunk
+  // of the halo brick of one phase
+  const cuuint64_t vox = (cuuint64_t)p.dims[0] * p.dims[1] * p.dims[2];
+  cuuint64_t gdim[5] = {(cuuint64_t)p.cin, (cuuint64_t)p.dims[0], (cuuint64_t)p.dims[1], (cuuint64_t)p.dims[2],
+                        (cuuint64_t)nphase};
+  cuuint64_t gstride[4] = {(cuuint64_t)p.cin * 2, (cuuint64_t)p.cin * 2 * p.dims[0],
+                           (cuuint64_t)p.cin * 2 * p.dims[0] * p.dims[1], (cuuint64_t)p.cin * 2 * vox};
+  cuuint32_t box[5] = {8, (cuuint32_t)p.halo[0], (cuuint32_t)p.halo[1], (cuuint32_t)p.halo[2], 1};
+  cuuint32_t estride[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(&plan.tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(d.stride == 2 ? phase : d.inA), gdim,
+                   gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return -4;
   plan.ready = 1;
   return 0;

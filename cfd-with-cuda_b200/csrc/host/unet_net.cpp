@@ -74,7 +74,10 @@ UnetNet::~UnetNet() {
   cudaFree(out);
   cudaFree(lossv);
   cudaFree(tc_err);
-  for (int l = 0; l < kUnetConvs; l++) cudaFree(wpack[l]);
+  for (int l = 0; l < kUnetConvs; l++) {
+    cudaFree(wpack[l]);
+    cudaFree(phase[l]);
+  }
   if (h_pinned) cudaFreeHost(h_pinned);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -202,9 +205,10 @@ cudaError_t UnetNet::prepare_tc(cudaStream_t s) {
   if (packs_dirty) {
     for (int l = 0; l < kUnetConvs; l++) {
       const int cin = kUnetTensor[kUnetConv[l].in].ch, cout = kUnetTensor[kUnetConv[l].out].ch;
+      const int st = kUnetConv[l].stride;
       if (cin % 16) continue;
-      cudaError_t e = grow(wpack[l], wpack_cap[l], conv_tc_pack_elems(cin, cout));
-      if (e == cudaSuccess) e = conv_tc_pack(Pb + unet_weight_offset(l), cin, cout, wpack[l], s);
+      cudaError_t e = grow(wpack[l], wpack_cap[l], conv_tc_pack_elems(cin, cout, st));
+      if (e == cudaSuccess) e = conv_tc_pack(Pb + unet_weight_offset(l), cin, cout, st, wpack[l], s);
       launches++;
       if (e != cudaSuccess) return e;
     }
@@ -213,7 +217,10 @@ cudaError_t UnetNet::prepare_tc(cudaStream_t s) {
   if (plan_gen != gen || plan_dims[0] != dims[0][0] || plan_dims[1] != dims[0][1] || plan_dims[2] != dims[0][2]) {
     for (int l = 0; l < kUnetConvs; l++) {
       ConvDesc d = conv_desc(*this, l, out);
-      plan_ok[l] = wpack[l] && conv_tc_supported(d) && conv_tc_plan(d, wpack[l], num_sms, plans[l]) == 0;
+      plan_ok[l] = false;
+      if (!wpack[l] || !conv_tc_supported(d)) continue;
+      if (d.stride == 2 && grow(phase[l], phase_cap[l], conv_tc_phase_elems(d)) != cudaSuccess) continue;
+      plan_ok[l] = conv_tc_plan(d, wpack[l], phase[l], num_sms, plans[l]) == 0;
     }
     plan_gen = gen;
     for (int a = 0; a < 3; a++) plan_dims[a] = dims[0][a];
@@ -230,9 +237,14 @@ cudaError_t UnetNet::forward(cudaStream_t s, float* out_f32, const int* skip) {
   for (int op : kOrder) {
     cudaError_t e;
     if (op >= 0) {
-      if (tc_enabled && plan_ok[op])
-        e = conv3_forward_tc(plans[op], out_f32, skip, tc_err, s);
-      else
+      if (tc_enabled && plan_ok[op]) {
+        e = cudaSuccess;
+        if (plans[op].p.stride == 2) {
+          e = conv_tc_space_to_depth(conv_desc(*this, op, out_f32), phase[op], skip, s);
+          launches++;
+        }
+        if (e == cudaSuccess) e = conv3_forward_tc(plans[op], out_f32, skip, tc_err, s);
+      } else
         e = conv3_forward(conv_desc(*this, op, out_f32, skip), s);
     } else {
       const UnetUpSpec& u = kUnetUp[-1 - op];

@@ -89,6 +89,7 @@ typedef struct {
   int steady;            /* 1 if the steady-state test fired */
   double maxAcc;         /* last max |Unp1-Un|/dt */
   int last_iter;         /* iteration index printed by the monitor (maxIter+1 if none converged) */
+  int fallbacks;         /* pressure solves in which the learned preconditioner fell back to Jacobi */
 } cfd_run_stats;
 
 /* ---- context ---------------------------------------------------------- */
