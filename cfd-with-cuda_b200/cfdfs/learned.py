@@ -32,6 +32,7 @@ import numpy as np
 from . import FP64, MIXED, PC_JACOBI, PC_LEARNED, CfdError, HostMesh, Solver, UNet, meshgen
 
 KS = (0, 3, 10, 30, 100)  # Jacobi-PCG iterations of the x_k in each pair
+FCG_KS = (1, 2, 4, 8, 16, 32)  # flexible-CG iterations of the on-policy x_k
 
 
 def cavity_params(seed: int):
@@ -54,8 +55,16 @@ class PairSampler:
     """Two FP64 contexts on one deck: ``run`` advances the flow, ``pair``
     solves for the pairs (so the running state is never disturbed)."""
 
-    def __init__(self, deck: str, dims, device: int = 0, inlet=None):
+    def __init__(self, deck: str, dims, device: int = 0, inlet=None, net=None):
         self.dims = tuple(dims)
+        self.fcg = None
+        if net is not None:
+            # flexible CG with the network being trained: its own iterates
+            # give the on-policy pairs
+            self.fcg = Solver(device=device, precision=FP64, cg_rtol=1e-12, precond=PC_LEARNED)
+            self.fcg.load(deck)
+            self.fcg.step0()
+            self.fcg.attach_unet(net, self.dims)
         self.run = Solver(device=device, precision=FP64)
         self.run.load(deck)
         self.run.step0()
@@ -75,6 +84,8 @@ class PairSampler:
     def close(self):
         self.run.close()
         self.pair.close()
+        if self.fcg is not None:
+            self.fcg.close()
 
     def advance(self, nsteps: int, iters=(1, 2)):
         """Runs nsteps time steps; returns the R2 of the given sub-iterations
@@ -85,20 +96,23 @@ class PairSampler:
         self.run.time_step(after_step2=lambda it: got.append(self.run.vector("R2")) if it in iters else None)
         return got
 
-    def pairs(self, rhs, ks=KS):
-        """Normalised (input, target) pairs, float32 arrays shaped (nz, ny, nx)."""
+    def pairs(self, rhs, ks=KS, onpolicy=False):
+        """Normalised (input, target) pairs, float32 arrays shaped (nz, ny, nx).
+        x_k comes from Jacobi-PCG, or with onpolicy from flexible CG with the
+        attached network (k iterations, then one Jacobi-PCG iteration)."""
         out = []
         if not np.any(rhs):
             return out
         self.pair.set_options(cg_rtol=1e-12, cg_maxit=20000)
         xs, st = self.pair.pressure_solve(rhs)
         shape = self.dims[::-1]
+        it_solver = self.fcg if onpolicy else self.pair
         for k in ks:
             if k == 0:
                 xk = np.zeros(self.n)
             else:
-                self.pair.set_options(cg_maxit=k)
-                xk, _ = self.pair.pressure_solve(rhs)
+                it_solver.set_options(cg_maxit=k)
+                xk, _ = it_solver.pressure_solve(rhs)
             r, nr = self.pair.pressure_residual(rhs, xk)
             if nr == 0.0:
                 continue
@@ -109,8 +123,11 @@ class PairSampler:
         return out
 
 
-def cavity_pairs(seeds, n=64, dt=0.002, snap_steps=(1, 5, 15, 35, 70, 100), device=0, tmpdir=None, log=None):
-    """Pairs from seeded cavity runs; returns (x, t) stacked arrays."""
+def cavity_pairs(seeds, n=64, dt=0.002, snap_steps=(1, 5, 15, 35, 70, 100), device=0, tmpdir=None, log=None,
+                 net=None, ks=KS):
+    """Pairs from seeded cavity runs; returns (x, t) stacked arrays.  With a
+    network, the x_k are flexible-CG iterates with that network (on-policy
+    pairs: the residuals the preconditioner meets inside its own solves)."""
     xs, ts = [], []
     tmpdir = tmpdir or tempfile.mkdtemp()
     for seed in seeds:
@@ -118,12 +135,12 @@ def cavity_pairs(seeds, n=64, dt=0.002, snap_steps=(1, 5, 15, 35, 70, 100), devi
         dts = stable_dt(dt, re, lid, n)
         deck = meshgen.write_cavity(os.path.join(tmpdir, f"cav_{seed}.inp"),
                                     meshgen.CavitySpec(n, re=re, dt=dts, steps=max(snap_steps), ngp=8, lid=lid))
-        ps = PairSampler(deck, (n + 1,) * 3, device=device)
+        ps = PairSampler(deck, (n + 1,) * 3, device=device, net=net)
         done, note = 0, "ok"
         try:
             for stp in snap_steps:
                 for rhs in ps.advance(stp - done):
-                    for x, t in ps.pairs(rhs):
+                    for x, t in ps.pairs(rhs, ks=ks, onpolicy=net is not None):
                         xs.append(x)
                         ts.append(t)
                 done = stp
@@ -131,7 +148,8 @@ def cavity_pairs(seeds, n=64, dt=0.002, snap_steps=(1, 5, 15, 35, 70, 100), devi
             note = f"stopped after step {done}: {e}"
         ps.close()
         if log is not None:
-            log.append(dict(source="cavity", seed=seed, re=re, lid=lid, dt=dts, pairs=len(xs), note=note))
+            log.append(dict(source="cavity-onpolicy" if net is not None else "cavity", seed=seed, re=re, lid=lid,
+                            dt=dts, pairs=len(xs), note=note))
     return np.stack(xs), np.stack(ts)
 
 
@@ -264,6 +282,10 @@ def main(argv=None):
     ap.add_argument("--no-duct", action="store_true")
     ap.add_argument("--eval-steps", type=int, default=10)
     ap.add_argument("--init", default=None, help="start from these weights")
+    ap.add_argument("--onpolicy-rounds", type=int, default=1,
+                    help="rounds of pairs from flexible-CG iterates with the network trained so far")
+    ap.add_argument("--onpolicy-seeds", type=int, default=10)
+    ap.add_argument("--onpolicy-budget", type=float, default=None, help="training seconds per round (default: budget)")
     a = ap.parse_args(argv)
     log = dict(args=vars(a), data=[])
     t0 = time.time()
@@ -307,6 +329,22 @@ def main(argv=None):
         vl = dict(w_l2=w_l2, w_h1=w_h1, weights=path, val_loss_init=eval_loss(net, vx, vt, dims_c))
         t1 = time.time()
         train(net, sets, a.budget, lr0=a.lr, batch=a.batch, log=vl)
+        vsets = list(sets)
+        vl["onpolicy"] = []
+        for rnd in range(a.onpolicy_rounds):
+            # pairs from the network's own flexible-CG solves on fresh seeds,
+            # then more training on everything gathered so far
+            t2 = time.time()
+            seeds = range(1000 * (rnd + 1), 1000 * (rnd + 1) + a.onpolicy_seeds)
+            ox, ot = cavity_pairs(seeds, n=a.n, net=net, ks=FCG_KS, log=log["data"])
+            perm = np.random.default_rng(2 + rnd).permutation(len(ox))
+            vsets.append((torch.from_numpy(ox[perm]).cuda(), torch.from_numpy(ot[perm]).cuda(), dims_c, len(ox)))
+            del ox, ot
+            rl = dict(round=rnd, pairs=vsets[-1][3], data_seconds=time.time() - t2)
+            train(net, vsets, a.onpolicy_budget or a.budget, lr0=0.5 * a.lr, batch=a.batch, seed=1 + rnd, log=rl)
+            rl["energy_quality"] = energy_quality(ps, net, rhs_eval)
+            vl["onpolicy"].append(rl)
+        del vsets
         vl["train_seconds"] = time.time() - t1
         vl["val_loss"] = eval_loss(net, vx, vt, dims_c)
         vl["energy_quality"] = energy_quality(ps, net, rhs_eval)

@@ -145,7 +145,9 @@ struct cfd_ctx {
   std::unique_ptr<cfd_unet> unet_owned;
   int udims[3] = {0, 0, 0};
   DevBuf<int> upmap;  // voxel -> pressure node (empty: identity)
-  DevBuf<double> fcg_sc, fcg_part;
+  DevBuf<double> fcg_sc, fcg_part, fcg_work64;
+  DevBuf<float> fcg_work32;
+  DevBuf<unsigned> fcg_cnt;
   DevBuf<int> fcg_done;
   int fcg_window = 25;
   bool fcg_use_graph = true;
@@ -432,9 +434,13 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   if (net.set_grid(c->udims, false)) return fail(c, CFD_E_NOMEM, "%s", net.err.c_str());
   if (!c->fcg_sc.p) {
     CU(c->fcg_sc.alloc(kFcgScalars));
-    CU(c->fcg_part.alloc(4 * (size_t)fcg_blocks(n)));
+    CU(c->fcg_part.alloc((size_t)fcg_part_words(n)));
+    CU(c->fcg_cnt.alloc(1));
+    CU(cudaMemsetAsync(c->fcg_cnt.p, 0, sizeof(unsigned), s));
     CU(c->fcg_done.alloc(1));
   }
+  // work: r, z, w and kFcgMaxM ring slots each of p and q
+  const size_t nwork = (3 + 2 * (size_t)kFcgMaxM) * n;
   FcgArgs<VT> a{};
   a.n = n;
   a.off = c->zs_off.p;
@@ -442,10 +448,12 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   VT* work;
   if constexpr (sizeof(VT) == 4) {
     a.val = c->zs_val32.p;
-    work = c->f_work.p;
+    if (!c->fcg_work32.p) CU(c->fcg_work32.alloc(nwork));
+    work = c->fcg_work32.p;
   } else {
     a.val = c->zs_val.p;
-    work = c->cg_work.p;
+    if (!c->fcg_work64.p) CU(c->fcg_work64.alloc(nwork));
+    work = c->fcg_work64.p;
   }
   a.b = b;
   a.x = x;
@@ -453,14 +461,16 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   a.z = work + (size_t)n;
   a.w = work + 2 * (size_t)n;
   a.p = work + 3 * (size_t)n;
-  a.q = work + 4 * (size_t)n;
+  a.q = work + (3 + (size_t)kFcgMaxM) * n;
   a.st.sc = c->fcg_sc.p;
   a.st.part = c->fcg_part.p;
+  a.st.cnt = c->fcg_cnt.p;
   a.st.done = c->fcg_done.p;
   a.st.rtol = rtol;
   a.st.stall2 = c->fcg_stall * c->fcg_stall;
   a.st.maxit = maxit;
   a.st.window = c->fcg_window;
+  a.st.m = c->opt.fcg_m;
   KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
   c->launches++;
   const int* pmap = c->upmap.p;
@@ -483,7 +493,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       KL(CFD_K_UNET, unet());
       KL(CFD_K_FCG, launch_fcg_spmv<VT>(a, s));
       KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
-      c->launches += net.launches - l0 + 1 + 2;
+      c->launches += net.launches - l0 + 1 + 1;
     } else {
       CU(unet());
       CU(launch_fcg_spmv<VT>(a, s));
@@ -515,7 +525,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       cudaGraphDestroy(graph);
       CU(ce);
       g.key = key;
-      g.launches = (net.launches - l0) + kFcgBatch * 3;
+      g.launches = (net.launches - l0) + kFcgBatch * 2;
     }
     G = &g;
   }
@@ -681,6 +691,7 @@ void cfd_default_options(cfd_options* o) {
   o->ngp_override = 0;
   o->inner_rtol = 1e-4;
   o->max_outer = 12;
+  o->fcg_m = 4;
 }
 
 int cfd_create(cfd_ctx** out, int device) {
@@ -727,6 +738,8 @@ int cfd_set_options(cfd_ctx* c, const cfd_options* o) {
   c->opt = *o;
   if (c->opt.inner_rtol <= 0 || c->opt.inner_rtol >= 1) c->opt.inner_rtol = 1e-4;
   if (c->opt.max_outer <= 0) c->opt.max_outer = 12;
+  if (c->opt.fcg_m <= 0) c->opt.fcg_m = 4;
+  NEED(c->opt.fcg_m <= kFcgMaxM, "fcg_m must be in 1..8");
   return CFD_OK;
 }
 

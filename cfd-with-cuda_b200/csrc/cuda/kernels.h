@@ -152,29 +152,35 @@ struct PcgArgs {
   unsigned long long timeout_ns;
 };
 // Block ranges each PCG block gathers from, for a given grid (host).
-// Flexible CG on the SELL-32 pressure matrix (fcg.cu).  State words in
-// sc[]: indices below; status -1 running, 0 converged, 1 iteration limit,
-// 2 non-finite, 4 stalled (the residual fell by less than sqrt(stall2) over
-// the last window iterations, or the direction broke down).
+// Truncated flexible CG, FCG(m), on the SELL-32 pressure matrix (fcg.cu).
+// State words in sc[]: indices below; status -1 running, 0 converged, 1
+// iteration limit, 2 non-finite, 4 stalled (the residual fell by less than
+// sqrt(stall2) over the last window iterations, or the direction broke
+// down).  PQ0.. and Beta0.. hold (p_j, q_j) and beta_j per ring slot.
+constexpr int kFcgMaxM = 8;        // directions kept at most
+constexpr int kFcgMaxBlocks = 444;  // grid of the iteration kernels (3 per SM)
 enum {
-  kFcgRR = 0, kFcgBB, kFcgPQ, kFcgAlpha, kFcgBeta, kFcgIt, kFcgStatus, kFcgRRMark,
-  kFcgRtol, kFcgStall2, kFcgMaxit, kFcgWindow, kFcgScalars = 12
+  kFcgRR = 0, kFcgBB, kFcgAlpha, kFcgIt, kFcgStatus, kFcgRRMark, kFcgRtol, kFcgStall2, kFcgMaxit, kFcgWindow,
+  kFcgM, kFcgPQ0 = 12, kFcgBeta0 = kFcgPQ0 + kFcgMaxM, kFcgScalars = kFcgBeta0 + kFcgMaxM
 };
 // The iteration kernels read the solve's settings from sc[] (written by the
 // start kernel), so a captured sequence of iterations serves every solve.
 struct FcgState {
-  double* sc;    // kFcgScalars words
-  double* part;  // 4 x blocks
-  int* done;     // kernels return at once while *done != 0
+  double* sc;     // kFcgScalars words
+  double* part;   // fcg_part_words(n) words
+  unsigned* cnt;  // block arrival counter, zero between kernels (host-zeroed once)
+  int* done;      // kernels return at once while *done != 0
   double rtol, stall2;  // read by the start kernel only
-  int maxit, window;
+  int maxit, window, m;
 };
+// p and q point at m ring slots of n entries each.
 template <class VT> struct FcgArgs {
   int n; const int *off, *col; const VT* val; const VT* b;
   VT *x, *r, *z, *w, *p, *q;
   FcgState st;
 };
 int fcg_blocks(int n);
+int fcg_part_words(int n);
 template <class VT> cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s);
 template <class VT> cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s);
 template <class VT> cudaError_t launch_fcg_update(const FcgArgs<VT>& a, cudaStream_t s);

@@ -88,8 +88,10 @@ cudaError_t f32_to_bf16(long long n, const float* a, __nv_bfloat16* b, cudaStrea
 // ---- tensor-core path (unet_tc.cu): stride-1 and stride-2 convolutions,
 // cin in {16, 32, 64}, cout in {16, 32, 64} or 1 with FP32 output ----
 struct ConvTcParams {
-  int dims[3];      // output grid (stride 2: the coarse grid of the input's phases)
-  int stride;       // 1, or 2 (input given as 8 parity phases, conv_tc_space_to_depth)
+  int dims[3];      // output grid
+  int in_dims[3];   // input grid (stride 2: 2 dims - 1 per axis)
+  const __nv_bfloat16* in;  // input tensor, channels-last, cin channels
+  int stride;       // 1 or 2
   int brick[3];     // output voxels per CTA along each axis
   int nb[3];        // bricks per axis
   int halo[3];      // brick + 2
@@ -106,7 +108,6 @@ struct ConvTcParams {
   int* err;  // set when a bounded wait gives up
 };
 struct ConvTcPlan {
-  CUtensorMap tmap;  // TMA descriptor of the input tensor
   ConvTcParams p;
   int grid_x;
   size_t smem;
@@ -119,14 +120,9 @@ long long conv_tc_pack_elems(int cin, int cout, int stride);
 // blocks (wpack holds conv_tc_pack_elems values).
 cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
                          cudaStream_t s);
-// Stride 2: elements of the parity-phase copy of the input (0 for stride 1)
-// and the pass that writes it (to run before each launch of the plan).
-long long conv_tc_phase_elems(const ConvDesc& d);
-cudaError_t conv_tc_space_to_depth(const ConvDesc& d, __nv_bfloat16* phase, const int* skip, cudaStream_t s);
-// Builds the launch plan (bricks, shared-memory layout, TMA descriptor) of a
-// supported convolution (stride 2 reads the phase buffer); 0 on success.
-int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, const __nv_bfloat16* phase, int num_sms,
-                 ConvTcPlan& plan);
+// Builds the launch plan (bricks, shared-memory layout) of a supported
+// convolution; 0 on success.
+int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan);
 // Launches a planned convolution; out_f32 (FP32-output layers) and skip
 // replace the plan's pointers for this launch.
 cudaError_t conv3_forward_tc(const ConvTcPlan& plan, float* out_f32, const int* skip, int* err, cudaStream_t s);

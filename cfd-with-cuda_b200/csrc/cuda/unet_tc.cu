@@ -1,22 +1,23 @@
-// Tensor-core (tcgen05) 3x3x3 convolution, stride 1, for the U-Net's
+// Tensor-core (tcgen05) 3x3x3 convolution, stride 1 or 2, for the U-Net's
 // inference path.
 //
 // Implicit GEMM without an im2col buffer.  A CTA owns a brick of output
-// voxels; TMA brings the brick plus a one-voxel halo into shared memory, one
+// voxels; its threads gather the brick plus a one-voxel halo into shared
+// memory with 16-byte cp.async copies (zero-filled outside the grid), one
 // plane per 8 input channels, each halo voxel one 16-byte row of the plane
-// (rows numbered hx + HX (hy + HY hz) over the halo box, zero-filled outside
-// the grid).  In that numbering every tap (dx, dy, dz) is a constant row
-// shift, so the A operand of tap k for 128 consecutive rows is the plane
-// itself at a shifted start address: no data is copied per tap.  Rows that
-// fall on the halo ring compute garbage that is never stored.  The weights of
-// all 27 taps for the CTA's slice of output channels are resident in shared
-// memory, pre-packed in the tensor core's canonical K-major layout.
+// (rows numbered hx + HX (hy + HY hz) over the halo box).  In that numbering
+// every tap (dx, dy, dz) is a constant row shift, so the A operand of tap k
+// for 128 consecutive rows is the plane itself at a shifted start address:
+// no data is copied per tap.  Rows that fall on the halo ring compute
+// garbage that is never stored.  The weights of all 27 taps for the CTA's
+// slice of output channels are resident in shared memory, pre-packed in the
+// tensor core's canonical K-major layout and brought in by one bulk copy.
 //
-// Stride 2 (the U-Net's down-sampling layers) runs on the same machinery
-// after a space-to-depth pass splits the fine input into its 8 parity phases
-// (voxel (2i+px, 2j+py, 2k+pz) -> phase px + 2py + 4pz at (i, j, k)): tap d
-// of output X reads phase (d != 0) at coarse index X + (d == -1 ? -1 : 0),
-// again a constant row shift inside that phase's planes (low-side halo only).
+// Stride 2 (the U-Net's down-sampling layers) runs on the same machinery:
+// the gather splits the fine input into its 8 parity phases (voxel (2i+px,
+// 2j+py, 2k+pz) -> phase px + 2py + 4pz at (i, j, k)), and tap d of output X
+// reads phase (d != 0) at coarse index X + (d == -1 ? -1 : 0), again a
+// constant row shift inside that phase's planes (low-side halo only).
 //
 // One thread issues tcgen05.mma (M = 128 rows, N = output channels of the
 // slice, K = 16 input channels) into a 128-column TMEM accumulator; the four
@@ -97,24 +98,66 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
-                                            unsigned long long* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
-      "[%7];" ::"r"(smem_u32(dst)),
-      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
-      : "memory");
+// 16-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, unsigned src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Warp-cooperative gather of the halo brick: one x-run (HX voxels x NCH
+// 16-byte chunks) per warp step, runs (phase, hz, hy) dealt round-robin over
+// the warps, lane constants precomputed, zero fill outside the grid.
+template <int NCH, int STRIDE>
+__device__ __forceinline__ void gather_halo(const ConvTcParams& p, unsigned char* A, int x0, int y0, int z0) {
+  constexpr int NPH = STRIDE == 2 ? 8 : 1;
+  const int HX = p.halo[0], HY = p.halo[1], HZ = p.halo[2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int fx = p.in_dims[0], fy = p.in_dims[1], fz = p.in_dims[2];
+  const int items = HX * NCH;  // per x-run
+  const int runs = NPH * HZ * HY;
+  for (int r = warp; r < runs; r += kTcThreads / 32) {
+    const int hy = r % HY, t = r / HY, hz = t % HZ, ph = t / HZ;
+    int gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+    bool yz_ok = gy >= 0 && gz >= 0;
+    if (STRIDE == 2) {
+      gy = 2 * gy + ((ph >> 1) & 1);
+      gz = 2 * gz + (ph >> 2);
+    }
+    yz_ok = yz_ok && gy < fy && gz < fz;
+    const long long rowbase = (long long)fx * (gy + (long long)fy * gz);
+    const int row0 = HX * (hy + HY * hz);
+    for (int i = lane; i < items; i += 32) {
+      const int c = i % NCH, hx = i / NCH;
+      int gx = x0 - 1 + hx;
+      bool ok = yz_ok && gx >= 0;
+      if (STRIDE == 2) gx = 2 * gx + (ph & 1);
+      ok = ok && gx < fx;
+      const __nv_bfloat16* src = ok ? p.in + ((gx + rowbase) * (NCH * 8) + 8 * c) : p.in;
+      cp_async16(A + (size_t)(ph * NCH + c) * p.plane_bytes + (size_t)(row0 + hx) * 16, src, ok ? 16u : 0u);
+    }
+  }
+  // read slack past the halo box: zeros
+  const int nbox = HX * HY * HZ, slack = p.rows - nbox;
+  for (int i = threadIdx.x; i < NPH * NCH * slack; i += kTcThreads) {
+    const int pl = i / slack, row = nbox + i % slack;
+    *(uint4*)(A + (size_t)pl * p.plane_bytes + (size_t)row * 16) = make_uint4(0, 0, 0, 0);
+  }
 }
 
-__global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ CUtensorMap tmap, ConvTcParams p) {
+template <int CIN, int STRIDE>
+__global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvTcParams p) {
+  constexpr int NCH = CIN / 8, KSTEPS = CIN / 16, NPH = STRIDE == 2 ? 8 : 1;
+  constexpr int NWARP = kTcThreads / 32;
   if (p.skip && *p.skip) return;
   extern __shared__ __align__(1024) unsigned char smem[];
-  const int nchunk = p.cin >> 3, nphase = p.stride == 2 ? 8 : 1;
   unsigned char* A = smem;
-  unsigned char* W = smem + (size_t)nphase * nchunk * p.plane_bytes;
-  const unsigned wbytes = 27u * p.cin * p.N * 2u;
+  unsigned char* W = smem + (size_t)NPH * NCH * p.plane_bytes;
+  const unsigned wbytes = 27u * CIN * p.N * 2u;
+  // barrier 0: weights; barrier 1 + w: MMAs issued by warp w
   unsigned long long* bars = (unsigned long long*)(W + wbytes);  // wbytes is a multiple of 16
-  unsigned* tmem_slot = (unsigned*)(bars + 2);
+  unsigned* tmem_slot = (unsigned*)(bars + 1 + NWARP);
+  float* sbias = (float*)(tmem_slot + 2);  // N floats
 
   const int b = blockIdx.x, slice = blockIdx.y;
   const int bx = b % p.nb[0], by = (b / p.nb[0]) % p.nb[1], bz = b / (p.nb[0] * p.nb[1]);
@@ -123,8 +166,7 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (int i = 0; i <= NWARP; i++) mbar_init(&bars[i], 1);
     mbar_init_fence();
   }
   if (warp == 0) tmem_alloc(tmem_slot, kTmemCols);
@@ -132,75 +174,71 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
   __syncthreads();
   tc_fence_after();
   const unsigned tmem = *tmem_slot;
-  float* sbias = (float*)(tmem_slot + 4);  // N floats
   for (int i = threadIdx.x; i < p.N; i += blockDim.x) {
     const int co = slice * p.N + i;
     sbias[i] = co < p.cout ? p.bias[co] : 0.f;
   }
-
   if (threadIdx.x == 0) {
-    const unsigned box = (unsigned)(p.halo[0] * p.halo[1] * p.halo[2]) * 16u;
-    mbar_expect_tx(&bars[0], nphase * nchunk * box + wbytes);
-    for (int ph = 0; ph < nphase; ph++)
-      for (int c = 0; c < nchunk; c++)
-        tma_load_5d(A + (size_t)(ph * nchunk + c) * p.plane_bytes, &tmap, c * 8, x0 - 1, y0 - 1, z0 - 1, ph,
-                    &bars[0]);
-    bulk_g2s(W, p.wpack + (size_t)slice * 27 * p.cin * p.N, wbytes, &bars[0]);
+    mbar_expect_tx(&bars[0], wbytes);
+    bulk_g2s(W, p.wpack + (size_t)slice * 27 * CIN * p.N, wbytes, &bars[0]);
   }
+  gather_halo<NCH, STRIDE>(p, A, x0, y0, z0);
+  cp_async_wait_all();
+  fence_proxy_async_smem();
   bool ok = __syncthreads_and(mbar_wait_bounded(&bars[0], 0, kTcWaitNs));
   bool loads_done = ok, mma_done = true;
 
   const unsigned idesc = umma_idesc(p.N);
   const int tpg = kTmemCols / p.N;  // M-tiles per accumulator group
-  const int ksteps = p.cin >> 4;
   const int n0 = slice * p.N;
   // Descriptor bases; per MMA only the start-address field (bits 0-13, in
   // 16-byte units) changes, by a whole number of rows / weight blocks, so the
-  // issuing thread adds offsets to the 64-bit descriptors (shared addresses
+  // issuing lanes add offsets to the 64-bit descriptors (shared addresses
   // stay below 2^18 bytes, so the field never carries).
   const unsigned long long da0 = umma_desc(smem_u32(A), (unsigned)p.plane_bytes, 128u);
   const unsigned long long db0 = umma_desc(smem_u32(W), (unsigned)(p.N >> 3) * 128u, 128u);
   const unsigned plane16 = (unsigned)p.plane_bytes >> 4;
-  const unsigned wtap16 = (unsigned)(p.cin * p.N * 2) >> 4, wk16 = (unsigned)(p.N >> 3) * 8u;
+  const unsigned wtap16 = (unsigned)(CIN * p.N * 2) >> 4, wk16 = (unsigned)(p.N >> 3) * 8u;
+  // row offset (16-byte units, including the plane of stride-2 taps) of every tap
+  int toff[27];
+#pragma unroll
+  for (int k = 0; k < 27; k++) {
+    const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+    int off, plane0;
+    if (STRIDE == 2) {
+      off = -(dx < 0) - HX * ((dy < 0) + HY * (dz < 0));
+      plane0 = ((dx != 0) + 2 * (dy != 0) + 4 * (dz != 0)) * NCH;
+    } else {
+      off = dx + HX * (dy + HY * dz);
+      plane0 = 0;
+    }
+    toff[k] = plane0 * (int)plane16 + off;
+  }
   int phase = 0;
   for (int g0 = 0; g0 < p.tiles && ok; g0 += tpg) {
     const int g1 = min(p.tiles, g0 + tpg);
-    if (threadIdx.x == 0) {
+    // every warp's lane 0 issues the MMAs of its tiles (t = g0 + warp + 4j)
+    if (lane == 0) {
       tc_fence_after();
-      // row offset (16-byte units, including the plane of stride-2 taps) of
-      // every tap
-      int toff[27];
-#pragma unroll
-      for (int k = 0; k < 27; k++) {
-        const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
-        int off, plane0;
-        if (p.stride == 2) {
-          off = -(dx < 0) - HX * ((dy < 0) + HY * (dz < 0));
-          plane0 = ((dx != 0) + 2 * (dy != 0) + 4 * (dz != 0)) * nchunk;
-        } else {
-          off = dx + HX * (dy + HY * dz);
-          plane0 = 0;
-        }
-        toff[k] = plane0 * (int)plane16 + off;
-      }
-      for (int t = g0; t < g1; t++) {
+      for (int t = g0 + warp; t < g1; t += NWARP) {
         const unsigned d = tmem + (unsigned)((t - g0) * p.N);
         const unsigned long long dat = da0 + (unsigned)(p.q0 + 128 * t);
-        unsigned acc = 0;
 #pragma unroll
         for (int k = 0; k < 27; k++) {
           const unsigned long long dak = dat + (unsigned long long)(long long)toff[k];
           const unsigned long long dbk = db0 + (unsigned long long)k * wtap16;
-          for (int j = 0; j < ksteps; j++) {
+#pragma unroll
+          for (int j = 0; j < KSTEPS; j++)
             umma(d, dak + (unsigned long long)(2 * j) * plane16, dbk + (unsigned long long)(2 * j) * wk16, idesc,
-                 acc);
-            acc = 1;
-          }
+                 (k | j) != 0);
         }
       }
-      umma_commit(&bars[1]);
+      umma_commit(&bars[1 + warp]);
     }
-    ok = __syncthreads_and(mbar_wait_bounded(&bars[1], phase, kTcWaitNs));
+    __syncwarp();
+    bool w_ok = true;
+    for (int w = 0; w < NWARP; w++) w_ok = w_ok && mbar_wait_bounded(&bars[1 + w], phase, kTcWaitNs);
+    ok = __syncthreads_and(w_ok);
     phase ^= 1;
     tc_fence_after();
     if (!ok) {
@@ -246,36 +284,14 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
     if (threadIdx.x == 0) {
       if (p.err) atomicExch(p.err, 1);
       if (!loads_done) mbar_wait_bounded(&bars[0], 0, kTcWaitNs);
-      if (!mma_done) mbar_wait_bounded(&bars[1], phase ^ 1, kTcWaitNs);
     }
+    if (!mma_done && lane == 0) mbar_wait_bounded(&bars[1 + warp], phase ^ 1, kTcWaitNs);
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
     tmem_dealloc(tmem, kTmemCols);
-  }
-}
-
-// ph[phase][k][j][i][c] = in[2i+px][2j+py][2k+pz][c] (zero outside the fine
-// grid), phase = px + 2py + 4pz, coarse dims cd; one thread per 8 channels.
-__global__ void k_space_to_depth(const __nv_bfloat16* __restrict__ in, Dims6 g, int ch, __nv_bfloat16* ph,
-                                 const int* skip) {
-  if (skip && *skip) return;
-  const int nc = ch / 8;
-  const long long per = (long long)g.c[0] * g.c[1] * g.c[2];
-  const long long total = 8 * per * nc;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % nc);
-    const long long v = (i / nc) % per;
-    const int phs = (int)(i / (nc * per));
-    const int x = (int)(v % g.c[0]), y = (int)((v / g.c[0]) % g.c[1]), z = (int)(v / ((long long)g.c[0] * g.c[1]));
-    const int fx = 2 * x + (phs & 1), fy = 2 * y + ((phs >> 1) & 1), fz = 2 * z + (phs >> 2);
-    uint4 val = make_uint4(0, 0, 0, 0);
-    if (fx < g.f[0] && fy < g.f[1] && fz < g.f[2])
-      val = *(const uint4*)(in + ((fx + (long long)g.f[0] * (fy + (long long)g.f[1] * fz)) * ch + 8 * c));
-    *(uint4*)(ph + ((phs * per + v) * ch + 8 * c)) = val;
   }
 }
 
@@ -296,22 +312,6 @@ __global__ void k_pack_tc(const __nv_bfloat16* __restrict__ w, int cin, int cout
     const int ci = kc * 8 + k8, co = slice * N + ng * 8 + n8;
     wp[i] = co < cout ? w[((size_t)tap * cin + ci) * cout + co] : __float2bfloat16(0.f);
   }
-}
-
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiled encoder() {
-  static EncodeTiled fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiled)p;
-  }
-  return fn;
 }
 
 int ceil_div(int a, int b) { return (a + b - 1) / b; }
@@ -335,22 +335,6 @@ bool conv_tc_supported(const ConvDesc& d) {
          (d.cout == 16 || d.cout == 32 || d.cout == 64 || (d.cout == 1 && d.out_f32 && !d.out));
 }
 
-long long conv_tc_phase_elems(const ConvDesc& d) {
-  return d.stride == 2 ? 8LL * d.out_dims[0] * d.out_dims[1] * d.out_dims[2] * d.ca : 0;
-}
-
-cudaError_t conv_tc_space_to_depth(const ConvDesc& d, __nv_bfloat16* phase, const int* skip, cudaStream_t s) {
-  Dims6 g;
-  for (int a = 0; a < 3; a++) {
-    g.c[a] = d.out_dims[a];
-    g.f[a] = d.in_dims[a];
-  }
-  const long long total = conv_tc_phase_elems(d) / 8;
-  k_space_to_depth<<<(int)std::min<long long>((total + 255) / 256, 148 * 16), 256, 0, s>>>(d.inA, g, d.ca, phase,
-                                                                                           skip);
-  return cudaGetLastError();
-}
-
 cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
                          cudaStream_t s) {
   const int N = conv_tc_slice_width(cin, cout, stride);
@@ -365,15 +349,15 @@ long long conv_tc_pack_elems(int cin, int cout, int stride) {
   return (long long)ceil_div(cout < 16 ? 16 : cout, N) * 27 * cin * N;
 }
 
-int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, const __nv_bfloat16* phase, int num_sms,
-                 ConvTcPlan& plan) {
+int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan) {
   std::memset(&plan, 0, sizeof(plan));
   if (!conv_tc_supported(d)) return -1;
-  if (d.stride == 2 && !phase) return -1;
-  EncodeTiled enc = encoder();
-  if (!enc) return -2;
   ConvTcParams& p = plan.p;
-  for (int a = 0; a < 3; a++) p.dims[a] = d.out_dims[a];
+  for (int a = 0; a < 3; a++) {
+    p.dims[a] = d.out_dims[a];
+    p.in_dims[a] = d.in_dims[a];
+  }
+  p.in = d.inA;
   p.stride = d.stride;
   p.cin = d.ca;
   p.cout = d.cout;
@@ -386,10 +370,27 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, const __nv_bfloa
     p.brick[a] = ceil_div(p.dims[a], p.nb[a]);
     p.halo[a] = p.brick[a] + hpad;
   }
-  // bricks along z: enough CTAs for two per SM, within the shared-memory budget
-  const long long budget = 200 * 1024;
-  const int target = ceil_div(2 * num_sms, p.nb[0] * p.nb[1] * p.nslices);
-  int tz = std::max(1, ceil_div(p.dims[2], std::max(1, target)));
+  // bricks along z: enough CTAs for two per SM when two fit next to each
+  // other in shared memory, else one wave of one CTA per SM with deeper bricks
+  long long budget = 113 * 1024;
+  int per_sm = 2;
+  const auto smem_of = [&](int tz) {
+    const int HX = p.halo[0], HY = p.halo[1], HZ = tz + hpad;
+    const int q0 = 1 + HX + HX * HY, last = p.brick[0] + HX * (p.brick[1] + HY * tz);
+    const int tiles = ceil_div(last - q0 + 1, 128);
+    const int rows = (std::max(HX * HY * HZ, q0 + 128 * tiles + (d.stride == 2 ? 0 : q0)) + 7) & ~7;
+    return (long long)nphase * nchunk * (((rows * 16) + 1023) & ~1023) + wbytes + 64 + 4 * p.N;
+  };
+  {
+    const int target = ceil_div(2 * num_sms, p.nb[0] * p.nb[1] * p.nslices);
+    if (smem_of(std::max(1, ceil_div(p.dims[2], std::max(1, target)))) > budget) {
+      per_sm = 1;
+      budget = 200 * 1024;
+    }
+  }
+  // z-bricks per column: as many as fit in one wave of per_sm CTAs per SM
+  const int target = std::max(1, per_sm * num_sms / (p.nb[0] * p.nb[1] * p.nslices));
+  int tz = std::max(1, ceil_div(p.dims[2], target));
   for (;; tz--) {
     p.brick[2] = tz;
     p.halo[2] = tz + hpad;
@@ -406,8 +407,8 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, const __nv_bfloa
   }
   if (plan.smem > 227 * 1024) return -3;
   {
-    // every shared-memory row the MMAs address lies inside its plane, every
-    // TMA box dimension is legal, and a group of tiles fits the TMEM columns
+    // every shared-memory row the MMAs address lies inside its plane, the
+    // halo box stays small, and a group of tiles fits the TMEM columns
     const int HX = p.halo[0], HY = p.halo[1];
     const int off_min = 1 + HX + HX * HY, off_max = d.stride == 2 ? 0 : off_min;
     if (p.q0 - off_min < 0 || p.q0 + 128 * p.tiles - 1 + off_max >= p.rows || p.rows * 16 > p.plane_bytes ||
@@ -423,32 +424,28 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, const __nv_bfloa
   p.act = d.act;
   p.skip = d.skip;
   plan.grid_x = p.nb[0] * p.nb[1] * p.nb[2];
-  // input [phase][Z][Y][X][C] BF16 (one phase for stride 1: the tensor
-  // itself; eight coarse-grid phases for stride 2); box = one 8-channel chunk
-  // of the halo brick of one phase
-  const cuuint64_t vox = (cuuint64_t)p.dims[0] * p.dims[1] * p.dims[2];
-  cuuint64_t gdim[5] = {(cuuint64_t)p.cin, (cuuint64_t)p.dims[0], (cuuint64_t)p.dims[1], (cuuint64_t)p.dims[2],
-                        (cuuint64_t)nphase};
-  cuuint64_t gstride[4] = {(cuuint64_t)p.cin * 2, (cuuint64_t)p.cin * 2 * p.dims[0],
-                           (cuuint64_t)p.cin * 2 * p.dims[0] * p.dims[1], (cuuint64_t)p.cin * 2 * vox};
-  cuuint32_t box[5] = {8, (cuuint32_t)p.halo[0], (cuuint32_t)p.halo[1], (cuuint32_t)p.halo[2], 1};
-  cuuint32_t estride[5] = {1, 1, 1, 1, 1};
-  CUresult r = enc(&plan.tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(d.stride == 2 ? phase : d.inA), gdim,
-                   gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return -4;
   plan.ready = 1;
   return 0;
 }
 
 cudaError_t conv3_forward_tc(const ConvTcPlan& plan, float* out_f32, const int* skip, int* err, cudaStream_t s) {
-  cudaError_t e = cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem);
-  if (e != cudaSuccess) return e;
   ConvTcParams p = plan.p;
   if (p.out_f32 && out_f32) p.out_f32 = out_f32;
   p.skip = skip;
   p.err = err;
-  k_conv_tc<<<dim3(plan.grid_x, p.nslices), kTcThreads, plan.smem, s>>>(plan.tmap, p);
+  void (*k)(ConvTcParams) = nullptr;
+  switch (p.cin * 4 + p.stride) {
+    case 16 * 4 + 1: k = k_conv_tc<16, 1>; break;
+    case 16 * 4 + 2: k = k_conv_tc<16, 2>; break;
+    case 32 * 4 + 1: k = k_conv_tc<32, 1>; break;
+    case 32 * 4 + 2: k = k_conv_tc<32, 2>; break;
+    case 64 * 4 + 1: k = k_conv_tc<64, 1>; break;
+    case 64 * 4 + 2: k = k_conv_tc<64, 2>; break;
+    default: return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem);
+  if (e != cudaSuccess) return e;
+  k<<<dim3(plan.grid_x, p.nslices), kTcThreads, plan.smem, s>>>(p);
   return cudaGetLastError();
 }
 

@@ -76,7 +76,6 @@ UnetNet::~UnetNet() {
   cudaFree(tc_err);
   for (int l = 0; l < kUnetConvs; l++) {
     cudaFree(wpack[l]);
-    cudaFree(phase[l]);
   }
   if (h_pinned) cudaFreeHost(h_pinned);
   if (own_stream) cudaStreamDestroy(own_stream);
@@ -219,8 +218,7 @@ cudaError_t UnetNet::prepare_tc(cudaStream_t s) {
       ConvDesc d = conv_desc(*this, l, out);
       plan_ok[l] = false;
       if (!wpack[l] || !conv_tc_supported(d)) continue;
-      if (d.stride == 2 && grow(phase[l], phase_cap[l], conv_tc_phase_elems(d)) != cudaSuccess) continue;
-      plan_ok[l] = conv_tc_plan(d, wpack[l], phase[l], num_sms, plans[l]) == 0;
+      plan_ok[l] = conv_tc_plan(d, wpack[l], num_sms, plans[l]) == 0;
     }
     plan_gen = gen;
     for (int a = 0; a < 3; a++) plan_dims[a] = dims[0][a];
@@ -238,12 +236,7 @@ cudaError_t UnetNet::forward(cudaStream_t s, float* out_f32, const int* skip) {
     cudaError_t e;
     if (op >= 0) {
       if (tc_enabled && plan_ok[op]) {
-        e = cudaSuccess;
-        if (plans[op].p.stride == 2) {
-          e = conv_tc_space_to_depth(conv_desc(*this, op, out_f32), phase[op], skip, s);
-          launches++;
-        }
-        if (e == cudaSuccess) e = conv3_forward_tc(plans[op], out_f32, skip, tc_err, s);
+        e = conv3_forward_tc(plans[op], out_f32, skip, tc_err, s);
       } else
         e = conv3_forward(conv_desc(*this, op, out_f32, skip), s);
     } else {

@@ -85,8 +85,6 @@ struct UnetNet {
   long long wpack_cap[kUnetConvs] = {};
   bool packs_dirty = true;
   ConvTcPlan plans[kUnetConvs];
-  __nv_bfloat16* phase[kUnetConvs] = {};  // parity-phase copies of stride-2 inputs
-  long long phase_cap[kUnetConvs] = {};
   bool plan_ok[kUnetConvs] = {};
   int plan_gen = -1, plan_dims[3] = {0, 0, 0};
   int* tc_err = nullptr;

@@ -63,6 +63,8 @@ typedef struct {
   int ngp_override;  /* 0: NGP from the deck; 8 or 27 overrides it */
   double inner_rtol; /* CFD_MIXED: inner FP32 solve tolerance (default 1e-4) */
   int max_outer;     /* CFD_MIXED: refinement sweeps (default 12) */
+  int fcg_m;         /* CFD_PC_LEARNED: flexible-CG directions each new one is
+                        orthogonalised against, 1..8 (default 4) */
 } cfd_options;
 
 typedef struct {
