@@ -145,6 +145,11 @@ def algorithmic_bytes(info, klass, iters_per_launch, mixed):
         return nnzZ * 12 + 4 * (NNp + 1) + 4 * NNp * 8
     if klass == "convect":
         return 3 * 3 * info.NN * 8 + info.NE * (27 * 4 + 8 * 3 * 8)
+    if klass == "spmv_z":
+        # flexible-CG SpMV w = Z z (FP32 inner solve): the Z stream, z
+        # gathered once, w written, r, p, q read for the fused dot products
+        s = 4 if mixed else 8
+        return nnzZ * (s + 4) + 4 * (NNp + 1) + 5 * NNp * s
     return 0
 
 
@@ -174,6 +179,7 @@ def run_ours(args, rank, world, local_rank):
     work = tempfile.mkdtemp(prefix=f"cfdbench{rank}_")
     deck = make_deck(os.path.join(work, "cavity64.inp"), args.n)
     learned = args.precond == "learned"
+    pc_of = {"learned": cfdfs.PC_LEARNED, "twolevel": cfdfs.PC_TWOLEVEL, "jacobi": cfdfs.PC_JACOBI}
 
     def barrier():
         if dist is not None:
@@ -186,14 +192,16 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed_solver(precision, use_net, steps, warmup):
+    def timed_solver(precision, precond, steps, warmup):
         s = cfdfs.Solver(device=local_rank, precision=precision, cg_rtol=1e-8, cg_maxit=args.cg_maxit,
-                         precond=cfdfs.PC_LEARNED if use_net else cfdfs.PC_JACOBI)
+                         precond=pc_of[precond])
         t0 = time.time()
         s.load(deck)
         s.step0()
-        if use_net:
+        if precond == "learned":
             s.load_unet(args.weights)
+        if precond != "jacobi":
+            s.precond_apply(np.zeros(s.refresh().NNp))  # builds the coarse space (set-up)
         setup_s = time.time() - t0
         for _ in range(warmup):
             s.run(1)
@@ -213,16 +221,26 @@ def run_ours(args, rank, world, local_rank):
         return s, dict(ms=ms, st=st, launches=launches, clocks=clk.summary(), setup_s=setup_s)
 
     precision = cfdfs.MIXED if args.precision == "mixed" else cfdfs.FP64
-    s, r = timed_solver(precision, learned, args.steps, args.warmup)
+    s, r = timed_solver(precision, args.precond, args.steps, args.warmup)
     info = s.refresh()
     ms_max = max_over_ranks(r["ms"])
     value = world * args.steps / (ms_max / 1000.0)
 
+    # the same precision with the two-level preconditioner alone (the learned
+    # preconditioner without its network): what the network adds
+    twolevel = None
+    if learned and args.fp64_steps:
+        s2, r2 = timed_solver(precision, "twolevel", args.steps, args.warmup)
+        ms2 = max_over_ranks(r2["ms"])
+        twolevel = dict(steps_per_s=round(world * args.steps / (ms2 / 1000.0), 4), ms_per_step=round(ms2 / args.steps, 3),
+                        cg_iters_per_step=round(r2["st"].cg_iters / max(1, r2["st"].steps), 1))
+        s2.close()
+
     # the plain FP64 Jacobi-PCG path on the same workload and the same steps
     # (denominator of the headline target, and the accuracy reference)
     fp64, acc = None, None
-    if args.fp64_steps and not (precision == cfdfs.FP64 and not learned):
-        s64, r64 = timed_solver(cfdfs.FP64, False, args.steps, args.warmup)
+    if args.fp64_steps and not (precision == cfdfs.FP64 and args.precond == "jacobi"):
+        s64, r64 = timed_solver(cfdfs.FP64, "jacobi", args.steps, args.warmup)
         ms64 = max_over_ranks(r64["ms"])
         fp64 = dict(steps=args.steps, steps_per_s=round(world * args.steps / (ms64 / 1000.0), 4),
                     ms_per_step=round(ms64 / args.steps, 3),
@@ -270,7 +288,9 @@ def run_ours(args, rank, world, local_rank):
     s.run(args.profile_steps)
     prof = s.profile_read()
     s.profile(False)
-    top = max(prof, key=lambda k: prof[k]["ms"])
+    # roofline of the dominant kernel class with a stated byte (or flop) count
+    known = ("pcg32", "pcg64", "spmv_z", "unet", "step1", "spmv_k3", "gt", "step3", "resid64", "convect")
+    top = max((k for k in prof if k in known), key=lambda k: prof[k]["ms"])
     p = prof[top]
     its_per_launch = (p["iters"] / p["launches"]) if p["launches"] else 0
     avg_ms = p["ms"] / max(1, p["launches"])
@@ -315,7 +335,10 @@ def run_ours(args, rank, world, local_rank):
             "dtype": ("f32+f64" if precision == cfdfs.MIXED else "f64") + ("+bf16" if learned else ""),
             "data": "synthetic: generated structured cavity deck (no dataset); fluid starts at rest",
             "config": {"workload": WORKLOAD, "elements": args.n ** 3, "precision": args.precision,
-                       "precond": "learned U-Net in flexible CG (Jacobi-PCG fallback)" if learned else "jacobi",
+                       "precond": {"learned": "Jacobi + coarse space + learned U-Net correction in flexible CG "
+                                   "(Jacobi-PCG fallback)",
+                        "twolevel": "Jacobi + Galerkin coarse-space correction (17^3 lattice) in CG",
+                        "jacobi": "jacobi"}[args.precond],
                        "weights": os.path.relpath(args.weights, ROOT) if learned else None,
                        "ngp": 8, "cg_rtol": 1e-8, "cg_x0": "zero",
                        "timed_steps": f"steps {args.warmup + 1}..{args.warmup + args.steps} of the run from rest",
@@ -324,6 +347,7 @@ def run_ours(args, rank, world, local_rank):
             "cg_iters_per_step": round(r["st"].cg_iters / max(1, r["st"].steps), 1),
             "subiters_per_step": round(r["st"].subiters / max(1, r["st"].steps), 2),
             "fp64_path": fp64,
+            "twolevel_path": twolevel,
             "speedup_vs_fp64": round(value / fp64["steps_per_s"], 3) if fp64 else None,
             "accuracy": acc,
             "roofline": roof,
@@ -403,8 +427,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--n", type=int, default=N_ELEM, help="elements per side (64 = the headline workload)")
-    ap.add_argument("--precond", default=None, choices=["learned", "jacobi"],
-                    help="default: learned when the weight file exists")
+    ap.add_argument("--precond", default=None, choices=["learned", "twolevel", "jacobi"],
+                    help="default: learned when the weight file exists, else twolevel")
     ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--fp64-steps", type=int, default=1, help="0 skips the FP64 Jacobi-PCG comparison run")
     ap.add_argument("--profile-steps", type=int, default=2)
@@ -415,7 +439,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.precond is None:
-        args.precond = "learned" if os.path.exists(args.weights) else "jacobi"
+        args.precond = "learned" if os.path.exists(args.weights) else "twolevel"
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
     local_rank = _env_int("LOCAL_RANK", 0)

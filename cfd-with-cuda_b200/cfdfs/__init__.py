@@ -29,7 +29,7 @@ HEADER = os.path.join(os.path.dirname(ROOT), "include", "cfdfs.h")
 CFD_OK, CFD_E_CUDA, CFD_E_NOCONV, CFD_E_NONFINITE, CFD_E_TIMEOUT, CFD_E_BADARG, CFD_E_BADINPUT, CFD_E_IO, \
     CFD_E_NOMEM = 0, -1, -2, -3, -4, -5, -6, -7, -8
 FP64, MIXED = 0, 1
-PC_JACOBI, PC_LEARNED = 0, 1
+PC_JACOBI, PC_LEARNED, PC_TWOLEVEL = 0, 1, 2
 
 VEC = dict(Un=0, Unp1=1, Unp1_prev=2, UnpHalf=3, UnpHalf_prev=4, Acc=5, Acc_prev=6, Pn=7, Pnp1=8,
            Pnp1_prev=9, Pdot=10, MdInv=11, MdOrigInv=12, KtimesAcc_prev=13, R1=14, R2=15, R3=16, DIV=17)
@@ -121,6 +121,8 @@ _PROTOS = {
     "cfd_unet_attach": (C.c_int, [_vp, _vp, _ip, _ip]),
     "cfd_unet_load": (C.c_int, [_vp, _cp, _ip]),
     "cfd_pressure_residual": (C.c_int, [_vp, _dp, _dp, _dp, _dp]),
+    "cfd_set_pressure_grid": (C.c_int, [_vp, _ip, _ip]),
+    "cfd_precond_apply": (C.c_int, [_vp, _dp, _dp]),
     "cfd_stream": (C.c_void_p, [_vp]),
     "cfd_launch_count": (C.c_longlong, [_vp]),
     "cfd_profile": (C.c_int, [_vp, C.c_int]),
@@ -438,7 +440,22 @@ class Solver:
                                                  _p(r, C.c_double), C.byref(nrm)))
         return r, nrm.value
 
-    # ---- learned preconditioner ----
+    # ---- preconditioners ----
+    def set_pressure_grid(self, dims, p_of_vox=None):
+        """Structured grid of the pressure nodes for the coarse space and the
+        network (dims = (nx, ny, nz); p_of_vox: pressure node of each voxel)."""
+        d = np.ascontiguousarray(dims, dtype=np.int32)
+        pm = None if p_of_vox is None else np.ascontiguousarray(p_of_vox, dtype=np.int32)
+        self._check(self.L.cfd_set_pressure_grid(self.h, _p(d, C.c_int), None if pm is None else _p(pm, C.c_int)))
+
+    def precond_apply(self, r):
+        """Linear part of the configured preconditioner applied to r (FP64)."""
+        i = self.info or self.refresh()
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros(i.NNp)
+        self._check(self.L.cfd_precond_apply(self.h, _p(r, C.c_double), _p(z, C.c_double)))
+        return z
+
     def attach_unet(self, net, dims=None, p_of_vox=None):
         """Use ``net`` (a ``UNet``) as the learned preconditioner on the
         pressure grid ``dims`` (default: a cube); None detaches."""
@@ -461,7 +478,7 @@ class Solver:
 
     # ---- timing / counters ----
     KCLASS = ["convect", "step1", "gt", "pcg64", "pcg32", "resid64", "step3", "spmv_k3", "pupdate", "other",
-              "unet", "fcg"]
+              "unet", "fcg", "coarse", "spmv_z"]
 
     @property
     def stream_ptr(self) -> int:

@@ -2,15 +2,19 @@
 pressure solves, and training of the U-Net on the GPU with the library's
 forward and backward kernels.
 
-Data.  For a right-hand side R2 met during a run, a FP64 Jacobi-PCG solve to
-||r|| <= 1e-12 ||R2|| gives x*; Jacobi-PCG stopped after k iterations gives
-x_k (x_0 = 0); each pair is (r_k = R2 - Z x_k, e_k = x* - x_k).  The
-preconditioner applies z = D^-1 r + f(r / s) s / d (a Jacobi step plus the
-network's correction), so the network input is x = r_k / s and its target
-t = (e_k - D^-1 r_k) d / s, with s = RMS(r_k), D the diagonal of Z and d its
-median entry: neither the residual's size nor the mesh spacing reaches the
-network, and a network that outputs zero leaves plain Jacobi.  Cavity runs
-draw Re ~ U[100, 1000] and lid speed ~ U[0.5, 1.5] from
+The preconditioner is z = L(r) + f(r / s) s / d: the linear two-level part
+L(r) = D^-1 r + P Zc^-1 P^T r (Jacobi step plus the Galerkin coarse-space
+correction) and the network's correction f, evaluated on the residual
+scaled to unit RMS (s = RMS(r)) and brought back by s / d (d = median
+diagonal of Z).  Neither the residual's size nor the mesh spacing reaches
+the network, and a network that outputs zero leaves the two-level method.
+
+Data.  For a right-hand side R2 met during a run, a FP64 two-level CG solve
+to ||r|| <= 1e-12 ||R2|| gives x*; the same solve stopped after k
+iterations gives x_k (x_0 = 0), and flexible CG with the network trained so
+far gives the on-policy x_k; each pair is the input x = r_k / s and the
+target t = (e_k - L(r_k)) d / s with r_k = R2 - Z x_k, e_k = x* - x_k.
+Cavity runs draw Re ~ U[100, 1000] and lid speed ~ U[0.5, 1.5] from
 numpy.random.Generator(PCG64(seed)), with dt = 0.002 capped by
 ``stable_dt`` (the scheme treats convection and viscosity explicitly); duct
 runs use the bent duct with a parabolic inlet.
@@ -29,10 +33,10 @@ import time
 
 import numpy as np
 
-from . import FP64, MIXED, PC_JACOBI, PC_LEARNED, CfdError, HostMesh, Solver, UNet, meshgen
+from . import FP64, MIXED, PC_JACOBI, PC_LEARNED, PC_TWOLEVEL, CfdError, HostMesh, Solver, UNet, meshgen
 
-KS = (0, 3, 10, 30, 100)  # Jacobi-PCG iterations of the x_k in each pair
-FCG_KS = (1, 2, 4, 8, 16, 32)  # flexible-CG iterations of the on-policy x_k
+KS = (0, 2, 5, 10, 20)  # two-level CG iterations of the x_k in each pair
+FCG_KS = (1, 2, 4, 8, 16)  # flexible-CG iterations of the on-policy x_k
 
 
 def cavity_params(seed: int):
@@ -52,11 +56,13 @@ def stable_dt(dt: float, re: float, lid: float, n: int) -> float:
 
 
 class PairSampler:
-    """Two FP64 contexts on one deck: ``run`` advances the flow, ``pair``
-    solves for the pairs (so the running state is never disturbed)."""
+    """FP64 contexts on one deck: ``run`` advances the flow, ``pair`` solves
+    for the pairs with the two-level preconditioner (so the running state is
+    never disturbed), ``fcg`` (with a network) gives on-policy iterates."""
 
     def __init__(self, deck: str, dims, device: int = 0, inlet=None, net=None):
         self.dims = tuple(dims)
+        cube = self.dims[0] == self.dims[1] == self.dims[2]
         self.fcg = None
         if net is not None:
             # flexible CG with the network being trained: its own iterates
@@ -65,14 +71,18 @@ class PairSampler:
             self.fcg.load(deck)
             self.fcg.step0()
             self.fcg.attach_unet(net, self.dims)
-        self.run = Solver(device=device, precision=FP64)
+        self.run = Solver(device=device, precision=FP64, precond=PC_TWOLEVEL)
         self.run.load(deck)
         self.run.step0()
+        if not cube:
+            self.run.set_pressure_grid(self.dims)
         if inlet is not None:
             self.run.set_bc_values(*inlet)
-        self.pair = Solver(device=device, precision=FP64, cg_rtol=1e-12, cg_maxit=20000)
+        self.pair = Solver(device=device, precision=FP64, cg_rtol=1e-12, cg_maxit=20000, precond=PC_TWOLEVEL)
         self.pair.load(deck)
         self.pair.step0()
+        if not cube:
+            self.pair.set_pressure_grid(self.dims)
         rp, col, val = self.pair.matrix("Z")
         rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
         diag = val[col == rows]
@@ -80,6 +90,10 @@ class PairSampler:
         self.dscale = float(np.median(diag))
         self.n = len(rp) - 1
         assert int(np.prod(self.dims)) == self.n
+
+    def linear(self, r):
+        """Linear (two-level) part of the preconditioner applied to r."""
+        return self.pair.precond_apply(r)
 
     def close(self):
         self.run.close()
@@ -98,8 +112,8 @@ class PairSampler:
 
     def pairs(self, rhs, ks=KS, onpolicy=False):
         """Normalised (input, target) pairs, float32 arrays shaped (nz, ny, nx).
-        x_k comes from Jacobi-PCG, or with onpolicy from flexible CG with the
-        attached network (k iterations, then one Jacobi-PCG iteration)."""
+        x_k comes from two-level CG, or with onpolicy from flexible CG with
+        the attached network (k iterations, then one Jacobi-PCG iteration)."""
         out = []
         if not np.any(rhs):
             return out
@@ -118,7 +132,7 @@ class PairSampler:
                 continue
             s = nr / np.sqrt(self.n)
             x = (r / s).astype(np.float32).reshape(shape)
-            t = ((xs - xk - self.dinv * r) * (self.dscale / s)).astype(np.float32).reshape(shape)
+            t = ((xs - xk - self.linear(r)) * (self.dscale / s)).astype(np.float32).reshape(shape)
             out.append((x, t))
         return out
 
@@ -214,12 +228,17 @@ def eval_loss(net: UNet, x, t, dims):
     return tot / max(1, len(x))
 
 
-def fcg_eval(net_path: str | None, deck: str, steps: int, precision: int, dims=None, inlet=None, device=0):
+def fcg_eval(net_path: str | None, deck: str, steps: int, precision: int, dims=None, inlet=None, device=0,
+             precond=None):
     """Pressure-CG iterations and wall time per step of a run, with the
-    learned preconditioner (net_path) or Jacobi-PCG (None)."""
-    s = Solver(device=device, precision=precision, precond=PC_LEARNED if net_path else PC_JACOBI)
+    learned preconditioner (net_path) or, without a network, the given
+    linear preconditioner (default Jacobi-PCG)."""
+    pc = PC_LEARNED if net_path else (PC_JACOBI if precond is None else precond)
+    s = Solver(device=device, precision=precision, precond=pc)
     s.load(deck)
     s.step0()
+    if dims is not None and not (dims[0] == dims[1] == dims[2]):
+        s.set_pressure_grid(dims)
     if inlet is not None:
         s.set_bc_values(*inlet)
     if net_path:
@@ -234,11 +253,12 @@ def fcg_eval(net_path: str | None, deck: str, steps: int, precision: int, dims=N
     return res
 
 
-def energy_quality(ps: PairSampler, net: UNet, rhs, ks=(0, 10, 100)):
+def energy_quality(ps: PairSampler, net: UNet, rhs, ks=(0, 5, 20)):
     """For pairs from one right-hand side: the relative Z-norm error left by
     the best multiple of the preconditioned residual, min_a ||e - a B(r)||_Z
-    / ||e||_Z, for B = Jacobi (D^-1 r) and B = the learned preconditioner
-    (D^-1 r + network correction).  Smaller is better; 0 = exact solve."""
+    / ||e||_Z, for B = Jacobi (D^-1 r), B = two-level (L(r)) and B = the
+    learned preconditioner (L(r) + network correction).  Smaller is better;
+    0 = exact solve."""
     shape = ps.dims[::-1]
     out = []
     zmul = lambda v: -ps.pair.pressure_residual(np.zeros(ps.n), v)[0]
@@ -254,11 +274,12 @@ def energy_quality(ps: PairSampler, net: UNet, rhs, ks=(0, 10, 100)):
         e = xs - xk
         s = nr / np.sqrt(ps.n)
         bj = ps.dinv * r
+        bt = ps.linear(r)
         y = net.forward((r / s).astype(np.float32).reshape(shape), ps.dims).ravel().astype(np.float64)
-        bl = bj + y * (s / ps.dscale)
+        bl = bt + y * (s / ps.dscale)
         ee = float(e @ zmul(e))
         res = {}
-        for name, b in (("jacobi", bj), ("learned", bl)):
+        for name, b in (("jacobi", bj), ("twolevel", bt), ("learned", bl)):
             zb = zmul(b)
             a = float(b @ zmul(e)) / float(b @ zb)
             d = e - a * b
@@ -361,6 +382,7 @@ def main(argv=None):
     for name, deck in decks.items():
         for prec, pname in ((FP64, "fp64"), (MIXED, "mixed")):
             base[f"{name}_{pname}_jacobi"] = fcg_eval(None, deck, a.eval_steps, prec)
+            base[f"{name}_{pname}_twolevel"] = fcg_eval(None, deck, a.eval_steps, prec, precond=PC_TWOLEVEL)
     log["eval_jacobi"] = base
     with open(a.log or a.out + ".json", "w") as f:
         json.dump(log, f, indent=1)

@@ -6,9 +6,11 @@
 // mallocs temporaries in step2GPU and checkConvergenceGPU on every call).
 // State rotation between sub-iterations and time steps swaps buffer
 // pointers instead of copying (blascoCodinaHuerta.cpp:2929-2932, 3070-3071).
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -22,6 +24,7 @@
 #include "../../include/cfdfs.h"
 #include "cuda/kernels.h"
 #include "cuda/unet.h"
+#include "host/coarse.h"
 #include "host/problem.h"
 #include "host/unet_net.h"
 
@@ -52,9 +55,11 @@ struct FcgGraph {
     const void* dinv;
     double dscale;
     int n;
+    int coarse_gen;  // 0: no coarse space
     bool operator==(const Key& o) const {
       return b == o.b && x == o.x && work == o.work && net == o.net && gen == o.gen && plan_gen == o.plan_gen &&
-             tc == o.tc && pmap == o.pmap && dinv == o.dinv && dscale == o.dscale && n == o.n;
+             tc == o.tc && pmap == o.pmap && dinv == o.dinv && dscale == o.dscale && n == o.n &&
+             coarse_gen == o.coarse_gen;
     }
   } key{};
   cudaGraphExec_t exec = nullptr;
@@ -148,12 +153,29 @@ struct cfd_ctx {
   DevBuf<double> fcg_sc, fcg_part, fcg_work64;
   DevBuf<float> fcg_work32;
   DevBuf<unsigned> fcg_cnt;
-  DevBuf<int> fcg_done;
+  DevBuf<int> fcg_done, fcg_err;
   int fcg_window = 25;
   bool fcg_use_graph = true;
   FcgGraph fcg_graph[2];  // FP32 inner solves, FP64 solves
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
+
+  // structured pressure grid (udims, upmap above) and the coarse space of
+  // the two-level preconditioners
+  bool grid_set = false;
+  std::vector<int> h_pmap;  // voxel -> pressure node (empty: identity)
+  bool coarse_ready = false;
+  int coarse_gen = 0;  // bumped on every rebuild (captured graphs key on it)
+  int cs_fd[3] = {0, 0, 0}, cs_cd[3] = {0, 0, 0}, cs_nc = 0;
+  DevBuf<int> cs_i0[3], cs_r[3];
+  DevBuf<double> cs_f[3], cs_e64;
+  DevBuf<float> cs_c32, cs_e32;  // coarse right-hand side (both precisions), FP32 coarse solution
+  DevBuf<__half> cs_inv16;
+  DevBuf<float> zst32;  // Z in structured (125-tap) form for the FP32 inner solves, when it applies
+  bool zst_ok = false;
+  int cs_ld = 0;
+  double cs_scale = 1.0;
+  double coarse_setup_s = 0;
 
   int timeN = 0;
   double timeT = 0, maxAcc = 0;
@@ -216,6 +238,12 @@ int set_device(cfd_ctx* c) {
   CU(cudaSetDevice(c->device));
   return CFD_OK;
 }
+
+double wall_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+bool mixed(const cfd_ctx* c);
 
 cudaEvent_t take_event(cfd_ctx* c) {
   if (!c->ev_pool.empty()) {
@@ -422,22 +450,207 @@ int run_pcg32(cfd_ctx* c, double rtol, int maxit, double* res) {
   return CFD_OK;
 }
 
-// Flexible CG with the attached U-Net.  VT = float: b, x are f_b, f_x and
-// the FP32 SELL values (inner solve of CFD_MIXED); VT = double: b, x are the
-// caller's FP64 vectors.  res = {iterations, ||r||/||b||, status} with the
-// status words of kernels.h (4 = stalled).
+bool learned(const cfd_ctx* c);
+bool twolevel(const cfd_ctx* c);
+
+// Voxel grid of the pressure nodes: dims, voxel -> node map (host and
+// device copies; empty = identity).
+int set_grid(cfd_ctx* c, const int dims[3], const int* p_of_vox) {
+  const long long nv = (long long)dims[0] * dims[1] * dims[2];
+  NEED(dims[0] > 0 && dims[1] > 0 && dims[2] > 0 && nv == c->P.NNp,
+       "grid dims do not multiply to the number of pressure nodes");
+  std::vector<int> pm;
+  if (p_of_vox) {
+    std::vector<char> seen(nv, 0);
+    for (long long v = 0; v < nv; v++) {
+      NEED(p_of_vox[v] >= 0 && p_of_vox[v] < nv && !seen[p_of_vox[v]], "p_of_vox is not a permutation");
+      seen[p_of_vox[v]] = 1;
+    }
+    pm.assign(p_of_vox, p_of_vox + nv);
+  }
+  c->upmap.reset();
+  if (!pm.empty()) {
+    CU(c->upmap.alloc(nv));
+    CU(cudaMemcpyAsync(c->upmap.p, pm.data(), nv * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+  }
+  c->h_pmap = std::move(pm);
+  for (int a = 0; a < 3; a++) c->udims[a] = dims[a];
+  c->grid_set = true;
+  c->coarse_ready = false;
+  c->fcg_graph[0].reset();
+  c->fcg_graph[1].reset();
+  return CFD_OK;
+}
+
+// Without a declared grid: a cube of m^3 pressure nodes numbered x + m (y +
+// m z), accepted only if the node coordinates increase along each index.
+int ensure_grid(cfd_ctx* c) {
+  if (c->grid_set) return CFD_OK;
+  const long long np = c->P.NNp;
+  const int m = (int)std::llround(std::cbrt((double)np));
+  NEED((long long)m * m * m == np && m >= 2,
+       "pressure nodes do not form a cube: declare the grid with cfd_set_pressure_grid");
+  const double* X = c->P.coord.data();
+  for (long long v = 0; v < np; v++) {
+    const int x = (int)(v % m), y = (int)((v / m) % m), z = (int)(v / ((long long)m * m));
+    const bool ok = (x == 0 || X[3 * v] > X[3 * (v - 1)]) && (y == 0 || X[3 * v + 1] > X[3 * (v - m) + 1]) &&
+                    (z == 0 || X[3 * v + 2] > X[3 * (v - (long long)m * m) + 2]);
+    NEED(ok, "pressure nodes are not numbered x + m (y + m z): declare the grid with cfd_set_pressure_grid");
+  }
+  const int d[3] = {m, m, m};
+  return set_grid(c, d, nullptr);
+}
+
+constexpr int kCoarseMaxNodes = 6000;
+
+// Builds the coarse space on the host from the assembled Z and uploads the
+// hat tables and the inverse of P^T Z P (FP64, and FP32 for CFD_MIXED).
+int ensure_coarse(cfd_ctx* c) {
+  if (c->coarse_ready) return CFD_OK;
+  int rc = ensure_grid(c);
+  if (rc) return rc;
+  const double t0 = wall_seconds();
+  const HostProblem& P = c->P;
+  std::vector<double> zv(P.z_col.size());
+  CU(cudaStreamSynchronize(c->stream));
+  CU(cudaMemcpy(zv.data(), c->zval.p, zv.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<int> vox;
+  if (!c->h_pmap.empty()) {
+    vox.assign(c->h_pmap.size(), 0);
+    for (size_t v = 0; v < c->h_pmap.size(); v++) vox[c->h_pmap[v]] = (int)v;
+  }
+  CoarseSpace cs;
+  std::string err;
+  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err))
+    return fail(c, CFD_E_NONFINITE, "%s", err.c_str());
+  const int nc = cs.nc;
+  for (int a = 0; a < 3; a++) {
+    c->cs_fd[a] = cs.fd[a];
+    c->cs_cd[a] = cs.cd[a];
+    const int n = cs.fd[a], ncd = cs.cd[a];
+    std::vector<int> i0(n), rng(2 * (size_t)ncd);
+    std::vector<double> f(n);
+    for (int i = 0; i < ncd; i++) {
+      rng[2 * i] = n;
+      rng[2 * i + 1] = -1;
+    }
+    for (int x = 0; x < n; x++) {
+      int i = 0;
+      double fr = 0.0;
+      if (ncd >= 2) {
+        const double t = x / cs.h[a];
+        i = std::min(std::max((int)std::floor(t), 0), ncd - 2);
+        fr = std::min(std::max(t - i, 0.0), 1.0);
+      }
+      i0[x] = i;
+      f[x] = fr;
+      for (int k = i; k <= std::min(i + 1, ncd - 1); k++) {
+        rng[2 * k] = std::min(rng[2 * k], x);
+        rng[2 * k + 1] = std::max(rng[2 * k + 1], x);
+      }
+    }
+    for (int i = 0; i < ncd; i++)
+      if (rng[2 * i + 1] < rng[2 * i]) rng[2 * i] = rng[2 * i + 1] = 0;
+    CU(c->cs_i0[a].alloc(n));
+    CU(c->cs_f[a].alloc(n));
+    CU(c->cs_r[a].alloc(2 * (size_t)ncd));
+    CU(cudaMemcpy(c->cs_i0[a].p, i0.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(c->cs_f[a].p, f.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(c->cs_r[a].p, rng.data(), rng.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  c->cs_nc = nc;
+  // the inverse goes to the device in FP16 (rows padded to 8 entries),
+  // scaled so its largest entry sits near the top of the FP16 range: the
+  // coarse correction only has to be close, and halving the bytes of the
+  // one dense operand of the iteration matters more
+  const int ld = (nc + 7) & ~7;
+  double amax = 0.0;
+  for (double v : cs.inv) amax = std::max(amax, std::fabs(v));
+  const double scale = amax > 0 ? 16384.0 / amax : 1.0;
+  std::vector<__half> h16((size_t)nc * ld, __float2half(0.f));
+  for (int i = 0; i < nc; i++)
+    for (int j = 0; j < nc; j++) h16[(size_t)i * ld + j] = __float2half((float)(cs.inv[(size_t)i * nc + j] * scale));
+  c->cs_ld = ld;
+  c->cs_scale = scale;
+  CU(c->cs_inv16.alloc(h16.size()));
+  CU(cudaMemcpy(c->cs_inv16.p, h16.data(), h16.size() * sizeof(__half), cudaMemcpyHostToDevice));
+  CU(c->cs_c32.alloc(ld));
+  CU(cudaMemset(c->cs_c32.p, 0, ld * sizeof(float)));
+  CU(c->cs_e64.alloc(nc));
+  if (mixed(c)) CU(c->cs_e32.alloc(nc));
+  // FP32 inner solves on an identity-numbered grid stream Z without column
+  // indices (125 coefficients per row) when every coupling stays within two
+  // grid steps
+  c->zst_ok = false;
+  c->zst32.reset();
+  if (mixed(c) && c->h_pmap.empty()) {
+    DevBuf<int> bad;
+    CU(bad.alloc(1));
+    CU(cudaMemset(bad.p, 0, sizeof(int)));
+    CU(c->zst32.alloc(stencil_elems(P.NNp)));
+    CU(launch_stencil_build<float>(P.NNp, c->udims, c->z_rp.p, c->z_col.p, c->zval.p, c->zst32.p, bad.p, c->stream));
+    int hb = 1;
+    CU(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    c->zst_ok = hb == 0;
+    if (!c->zst_ok) c->zst32.reset();
+  }
+  c->coarse_ready = true;
+  c->coarse_gen++;
+  c->fcg_graph[0].reset();
+  c->fcg_graph[1].reset();
+  c->coarse_setup_s = wall_seconds() - t0;
+  return CFD_OK;
+}
+
+template <class VT>
+CoarseArgs<VT> coarse_args(const cfd_ctx* c, bool with_coarse) {
+  CoarseArgs<VT> a{};
+  for (int k = 0; k < 3; k++) {
+    a.fd[k] = c->udims[k];
+    a.cd[k] = c->cs_cd[k];
+  }
+  a.nc = c->cs_nc;
+  a.ldinv = c->cs_ld;
+  a.inv_scale = c->cs_scale;
+  a.pmap = c->upmap.p;
+  if (with_coarse) {
+    a.i0x = c->cs_i0[0].p;
+    a.i0y = c->cs_i0[1].p;
+    a.i0z = c->cs_i0[2].p;
+    a.fx = c->cs_f[0].p;
+    a.fy = c->cs_f[1].p;
+    a.fz = c->cs_f[2].p;
+    a.rx = c->cs_r[0].p;
+    a.ry = c->cs_r[1].p;
+    a.rz = c->cs_r[2].p;
+    a.inv16 = c->cs_inv16.p;
+  }
+  return a;
+}
+
+// Flexible CG with the two-level preconditioner (Jacobi step + coarse-space
+// correction) and, for CFD_PC_LEARNED, the attached U-Net's correction.
+// VT = float: b, x are f_b, f_x and the FP32 SELL values (inner solve of
+// CFD_MIXED); VT = double: b, x are the caller's FP64 vectors.  The coarse
+// space must be built (ensure_coarse) before.  res = {iterations,
+// ||r||/||b||, status} with the status words of kernels.h (4 = stalled).
 template <class VT>
 int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, double* res) {
   cudaStream_t s = c->stream;
   const int n = c->P.NNp;
-  UnetNet& net = c->unet->net;
-  if (net.set_grid(c->udims, false)) return fail(c, CFD_E_NOMEM, "%s", net.err.c_str());
+  const bool use_net = learned(c);
+  NEED(c->coarse_ready, "coarse space not built");
+  UnetNet* netp = use_net ? &c->unet->net : nullptr;
+  if (netp && netp->set_grid(c->udims, false)) return fail(c, CFD_E_NOMEM, "%s", netp->err.c_str());
   if (!c->fcg_sc.p) {
     CU(c->fcg_sc.alloc(kFcgScalars));
     CU(c->fcg_part.alloc((size_t)fcg_part_words(n)));
     CU(c->fcg_cnt.alloc(1));
     CU(cudaMemsetAsync(c->fcg_cnt.p, 0, sizeof(unsigned), s));
     CU(c->fcg_done.alloc(1));
+    CU(c->fcg_err.alloc(1));
   }
   // work: r, z, w and kFcgMaxM ring slots each of p and q
   const size_t nwork = (3 + 2 * (size_t)kFcgMaxM) * n;
@@ -466,36 +679,61 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   a.st.part = c->fcg_part.p;
   a.st.cnt = c->fcg_cnt.p;
   a.st.done = c->fcg_done.p;
+  a.st.err = c->fcg_err.p;
+  a.st.timeout_ns = 2000000000ULL;
+  a.spmv_grid = std::min(2 * c->num_sms, kFcgMaxBlocks);
+  if constexpr (sizeof(VT) == 4) a.stencil = c->zst_ok ? c->zst32.p : nullptr;
+  for (int k = 0; k < 3; k++) a.fd[k] = c->udims[k];
   a.st.rtol = rtol;
   a.st.stall2 = c->fcg_stall * c->fcg_stall;
   a.st.maxit = maxit;
   a.st.window = c->fcg_window;
-  a.st.m = c->opt.fcg_m;
+  // a nonlinear (network) preconditioner needs the deeper orthogonalisation;
+  // the linear two-level one is symmetric, for which FCG(1) is CG
+  a.st.m = use_net ? c->opt.fcg_m : 1;
   KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
   c->launches++;
   const int* pmap = c->upmap.p;
   const VT* dinv;
-  if constexpr (sizeof(VT) == 4)
+  float* cc = c->cs_c32.p;
+  VT* ce;
+  if constexpr (sizeof(VT) == 4) {
     dinv = c->zdinv32.p;
-  else
+    ce = c->cs_e32.p;
+  } else {
     dinv = c->zdinv.p;
-  // one flexible-CG iteration: U-Net apply, SpMV + dots, coefficients, update
+    ce = c->cs_e64.p;
+  }
+  const CoarseArgs<VT> ca = coarse_args<VT>(c, true);
+  // one flexible-CG iteration: preconditioner (U-Net, coarse restriction
+  // and solve, combination), SpMV + dots + coefficients, update + tests
   auto iteration = [&](bool counted) -> int {
-    const long long l0 = net.launches;
+    const long long l0 = netp ? netp->launches : 0;
     auto unet = [&]() -> cudaError_t {
-      cudaError_t e = unet_input(n, a.r, pmap, a.st.sc + kFcgRR, 0.0, net.act[0], a.st.done, s);
-      if (e == cudaSuccess) e = net.forward(s, nullptr, a.st.done);
-      if (e == cudaSuccess)
-        e = unet_output(n, net.out, pmap, a.st.sc + kFcgRR, c->unet_dscale, dinv, a.r, a.z, a.st.done, s);
+      cudaError_t e = unet_input(n, a.r, pmap, a.st.sc + kFcgRR, 0.0, netp->act[0], a.st.done, s);
+      if (e == cudaSuccess) e = netp->forward(s, nullptr, a.st.done);
       return e;
     };
+    auto coarse = [&]() -> cudaError_t {
+      cudaError_t e = launch_coarse_restrict<VT>(ca, a.r, cc, a.st.done, s);
+      if (e == cudaSuccess) e = launch_coarse_solve<VT>(ca, cc, ce, a.st.done, s);
+      return e;
+    };
+    auto combine = [&]() -> cudaError_t {
+      return launch_precond<VT>(ca, n, a.r, dinv, ce, netp ? netp->out : nullptr, a.st.sc + kFcgRR,
+                                c->unet_dscale, a.z, a.st.done, s);
+    };
     if (counted) {
-      KL(CFD_K_UNET, unet());
-      KL(CFD_K_FCG, launch_fcg_spmv<VT>(a, s));
+      if (netp) KL(CFD_K_UNET, unet());
+      KL(CFD_K_COARSE, coarse());
+      KL(CFD_K_FCG, combine());
+      KL(CFD_K_SPMV_Z, launch_fcg_spmv<VT>(a, s));
       KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
-      c->launches += net.launches - l0 + 1 + 1;
+      c->launches += (netp ? netp->launches - l0 + 1 : 0) + 2 + 3;
     } else {
-      CU(unet());
+      if (netp) CU(unet());
+      CU(coarse());
+      CU(combine());
       CU(launch_fcg_spmv<VT>(a, s));
       CU(launch_fcg_update<VT>(a, s));
     }
@@ -505,12 +743,13 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   // configuration and replayed until the done flag stops the kernels
   FcgGraph* G = nullptr;
   if (c->fcg_use_graph && !c->prof_on) {
-    CU(net.prepare_tc(s));  // packs and plans outside the capture
+    if (netp) CU(netp->prepare_tc(s));  // packs and plans outside the capture
     FcgGraph& g = c->fcg_graph[sizeof(VT) == 4 ? 0 : 1];
-    FcgGraph::Key key{a.b, a.x, a.r, c->unet, net.gen, net.plan_gen, net.tc_enabled, pmap, dinv, c->unet_dscale, n};
+    FcgGraph::Key key{a.b,  a.x, a.r, netp ? c->unet : nullptr, netp ? netp->gen : 0, netp ? netp->plan_gen : 0,
+                      netp ? netp->tc_enabled : false, pmap, dinv, c->unet_dscale, n, c->coarse_gen};
     if (!g.exec || !(g.key == key)) {
       g.reset();
-      const long long l0 = net.launches;
+      const long long l0 = netp ? netp->launches : 0;
       CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
       int rc = CFD_OK;
       for (int k = 0; k < kFcgBatch && rc == CFD_OK; k++) rc = iteration(false);
@@ -525,7 +764,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       cudaGraphDestroy(graph);
       CU(ce);
       g.key = key;
-      g.launches = (net.launches - l0) + kFcgBatch * 2;
+      g.launches = (netp ? netp->launches - l0 + kFcgBatch : 0) + kFcgBatch * 5;
     }
     G = &g;
   }
@@ -564,11 +803,17 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   res[0] = h[kFcgIt];
   res[1] = h[kFcgBB] > 0 ? std::sqrt(h[kFcgRR] / h[kFcgBB]) : 0.0;
   res[2] = h[kFcgStatus] < 0 ? 1 : h[kFcgStatus];
-  if (c->prof_on) c->prof[CFD_K_FCG][2] += res[0];
+  if (c->prof_on) {
+    c->prof[CFD_K_FCG][2] += res[0];
+    c->prof[CFD_K_SPMV_Z][2] += res[0];
+  }
   return CFD_OK;
 }
 
 bool learned(const cfd_ctx* c) { return c->opt.precond == CFD_PC_LEARNED && c->unet; }
+bool twolevel(const cfd_ctx* c) { return c->opt.precond == CFD_PC_TWOLEVEL; }
+// solves that run flexible CG with a coarse space (and, when learned, the network)
+bool fcg_path(const cfd_ctx* c) { return learned(c) || twolevel(c); }
 
 // ||b - Z x||_2 in FP64 (also leaves r in ir_r and (float) r in f_b).
 int residual_norm(cfd_ctx* c, const double* b, const double* x, double* out) {
@@ -591,8 +836,10 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
   if (c->opt.precision == CFD_FP64 || c->opt.precision != CFD_MIXED) {
     double res[4] = {0, 0, 0, 0};
     int used = 0;
-    if (learned(c)) {
-      int rc = run_fcg<double>(c, b, x, warm, rtol, c->opt.cg_maxit, res);
+    if (fcg_path(c)) {
+      int rc = ensure_coarse(c);
+      if (rc) return rc;
+      rc = run_fcg<double>(c, b, x, warm, rtol, c->opt.cg_maxit, res);
       if (rc) return rc;
       used = (int)res[0];
       if ((int)res[2] != 0) {
@@ -602,7 +849,7 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
       }
     }
     int more = 0;
-    if (!learned(c) || z.fallback) {
+    if (!fcg_path(c) || z.fallback) {
       int rc = run_pcg64(c, b, x, warm, rtol, std::max(1, c->opt.cg_maxit - used), res);
       if (rc) return rc;
       more = (int)res[0];
@@ -633,7 +880,9 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
         double res[4] = {0, 0, 0, 0};
         // inner target: inner_rtol relative, but no tighter than needed
         double inner = std::max(c->opt.inner_rtol, 0.5 * rtol * bnorm / rnorm);
-        if (learned(c) && !z.fallback) {
+        if (fcg_path(c) && !z.fallback) {
+          rc = ensure_coarse(c);
+          if (rc) return rc;
           rc = run_fcg<float>(c, c->f_b.p, c->f_x.p, 0, inner, c->opt.cg_maxit - total, res);
           if (rc) return rc;
           const int fs = (int)res[2];
@@ -728,7 +977,8 @@ const char* cfd_last_error(const cfd_ctx* c) { return c ? c->err.c_str() : "null
 int cfd_set_options(cfd_ctx* c, const cfd_options* o) {
   if (!c || !o) return CFD_E_BADARG;
   NEED(o->precision == CFD_FP64 || o->precision == CFD_MIXED, "precision must be CFD_FP64 or CFD_MIXED");
-  NEED(o->precond == CFD_PC_JACOBI || o->precond == CFD_PC_LEARNED, "unknown preconditioner");
+  NEED(o->precond == CFD_PC_JACOBI || o->precond == CFD_PC_LEARNED || o->precond == CFD_PC_TWOLEVEL,
+       "unknown preconditioner");
   NEED(o->cg_rtol > 0 && o->cg_rtol < 1, "cg_rtol must be in (0, 1)");
   NEED(o->cg_maxit > 0, "cg_maxit must be > 0");
   NEED(o->ngp_override == 0 || o->ngp_override == 1 || o->ngp_override == 8 || o->ngp_override == 27,
@@ -852,6 +1102,7 @@ int cfd_step0(cfd_ctx* c) {
   }
   CU(cudaStreamSynchronize(s));
   c->assembled = true;
+  c->coarse_ready = false;  // Z changed
   return CFD_OK;
 }
 
@@ -1513,18 +1764,14 @@ int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_
   const long long nv = (long long)dims[0] * dims[1] * dims[2];
   NEED(nv == c->P.NNp, "grid dims do not multiply to the number of pressure nodes");
   if (u->net.set_grid(dims, false)) return fail(c, CFD_E_BADARG, "%s", u->net.err.c_str());
-  c->upmap.reset();
-  if (p_of_vox) {
-    std::vector<char> seen(nv, 0);
-    for (long long v = 0; v < nv; v++) {
-      NEED(p_of_vox[v] >= 0 && p_of_vox[v] < nv && !seen[p_of_vox[v]], "p_of_vox is not a permutation");
-      seen[p_of_vox[v]] = 1;
-    }
-    CU(c->upmap.alloc(nv));
-    CU(cudaMemcpyAsync(c->upmap.p, p_of_vox, nv * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    CU(cudaStreamSynchronize(c->stream));
+  const bool same = c->grid_set && dims[0] == c->udims[0] && dims[1] == c->udims[1] && dims[2] == c->udims[2] &&
+                    (p_of_vox ? c->h_pmap.size() == (size_t)nv &&
+                                    std::equal(c->h_pmap.begin(), c->h_pmap.end(), p_of_vox)
+                              : c->h_pmap.empty());
+  if (!same) {
+    int rc = set_grid(c, dims, p_of_vox);
+    if (rc) return rc;
   }
-  for (int a = 0; a < 3; a++) c->udims[a] = dims[a];
   c->fcg_graph[0].reset();
   c->fcg_graph[1].reset();
   {
@@ -1580,6 +1827,45 @@ int cfd_pressure_residual(cfd_ctx* c, const double* rhs, const double* x, double
   CU(cudaMemcpyAsync(r, c->ir_r.p, NNp * sizeof(double), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   if (norm) *norm = nr;
+  return CFD_OK;
+}
+
+int cfd_set_pressure_grid(cfd_ctx* c, const int dims[3], const int* p_of_vox) {
+  if (!c || !dims) return CFD_E_BADARG;
+  NEED(c->loaded, "cfd_set_pressure_grid before cfd_load_inp");
+  return set_grid(c, dims, p_of_vox);
+}
+
+int cfd_precond_apply(cfd_ctx* c, const double* r, double* z) {
+  if (!c || !r || !z) return CFD_E_BADARG;
+  NEED(c->assembled, "cfd_precond_apply before cfd_step0");
+  cudaStream_t s = c->stream;
+  const bool with_coarse = c->opt.precond == CFD_PC_TWOLEVEL || c->opt.precond == CFD_PC_LEARNED;
+  if (with_coarse) {
+    int rc = ensure_coarse(c);
+    if (rc) return rc;
+  }
+  const size_t NNp = c->P.NNp;
+  DevBuf<double> dr, dz;
+  CU(dr.alloc(NNp));
+  CU(dz.alloc(NNp));
+  CU(cudaMemcpyAsync(dr.p, r, NNp * sizeof(double), cudaMemcpyHostToDevice, s));
+  CoarseArgs<double> ca{};
+  if (with_coarse) {
+    ca = coarse_args<double>(c, true);
+  } else {  // Jacobi: position-independent, no grid needed
+    ca.fd[0] = (int)NNp;
+    ca.fd[1] = ca.fd[2] = 1;
+  }
+  if (with_coarse) {
+    CU(launch_coarse_restrict<double>(ca, dr.p, c->cs_c32.p, nullptr, s));
+    CU(launch_coarse_solve<double>(ca, c->cs_c32.p, c->cs_e64.p, nullptr, s));
+  }
+  CU(launch_precond<double>(ca, (int)NNp, dr.p, c->zdinv.p, with_coarse ? c->cs_e64.p : nullptr, nullptr, nullptr,
+                            1.0, dz.p, nullptr, s));
+  c->launches += with_coarse ? 3 : 1;
+  CU(cudaMemcpyAsync(z, dz.p, NNp * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
   return CFD_OK;
 }
 

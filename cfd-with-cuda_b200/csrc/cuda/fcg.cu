@@ -19,8 +19,11 @@
 // depend on which block finishes last.  The state words live in device
 // memory, and every kernel returns at once when the done flag is set, so the
 // host can queue several iterations between status reads.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
+#include "sell_stream.cuh"
 
 namespace cfd {
 
@@ -72,80 +75,38 @@ __device__ __forceinline__ void gather_partials(const double* part, int nblk, do
   block_sum<NV>(v);
 }
 
-// r = b - Z x (warm) or r = b, x = 0; partials {(b,b), (r,r)}; the last
-// block initialises the state words.
+// Per-row part of the SpMV kernels: w[i] and the dot products of the
+// iteration (z,w) (z,r) (z,q_j) (p_j,r), accumulated into v.
 template <class VT>
-__global__ void __launch_bounds__(kFcgThreads) k_fcg_start(FcgArgs<VT> a, int warm) {
-  double v[2] = {0, 0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-    const VT bi = a.b[i];
-    VT ri = bi;
-    if (warm)
-      ri = bi - sell_row(a.off, a.col, a.val, a.x, i);
-    else
-      a.x[i] = 0;
-    a.r[i] = ri;
-    v[0] += (double)bi * bi;
-    v[1] += (double)ri * ri;
-  }
-  block_sum<2>(v);
-  if (!post_partials<2>(v, a.st.part, a.st.cnt)) return;
-  gather_partials<2>(a.st.part, gridDim.x, v);
-  if (threadIdx.x == 0) {
-    const FcgState& st = a.st;
-    double* sc = st.sc;
-    sc[kFcgBB] = v[0];
-    sc[kFcgRR] = v[1];
-    sc[kFcgRRMark] = v[1];
-    sc[kFcgIt] = 0;
-    sc[kFcgRtol] = st.rtol;
-    sc[kFcgStall2] = st.stall2;
-    sc[kFcgMaxit] = st.maxit;
-    sc[kFcgWindow] = st.window;
-    sc[kFcgM] = st.m;
-    int done = 0;
-    double status = -1;
-    if (!isfinite(v[0]) || !isfinite(v[1])) {
-      status = 2;
-      done = 1;
-    } else if (v[1] <= st.rtol * st.rtol * v[0]) {
-      status = 0;
-      done = 1;
+__device__ __forceinline__ void fcg_row_dots(const FcgArgs<VT>& a, int i, VT wi, int nd, double (&v)[kFcgParts]) {
+  const size_t n = (size_t)a.n;
+  a.w[i] = wi;
+  const double zi = a.z[i], ri = a.r[i];
+  v[0] += zi * (double)wi;
+  v[1] += zi * ri;
+#pragma unroll
+  for (int j = 0; j < kFcgMaxM; j++) {
+    if (j < nd) {
+      v[2 + j] += zi * (double)a.q[j * n + i];
+      v[2 + kFcgMaxM + j] += (double)a.p[j * n + i] * ri;
     }
-    sc[kFcgStatus] = status;
-    st.done[0] = done;
   }
 }
 
+// Block sums of the SpMV's partials; the last block to finish forms the
+// coefficients beta_j, (p,q) and alpha of the iteration.
 template <class VT>
-__global__ void __launch_bounds__(kFcgThreads) k_fcg_spmv(FcgArgs<VT> a) {
-  if (*a.st.done) return;
-  const double* sc = a.st.sc;
-  const int m = (int)sc[kFcgM], it = (int)sc[kFcgIt];
-  const int nd = it < m ? it : m;
-  const size_t n = (size_t)a.n;
-  double v[kFcgParts];
-#pragma unroll
-  for (int k = 0; k < kFcgParts; k++) v[k] = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-    const VT wi = sell_row(a.off, a.col, a.val, a.z, i);
-    a.w[i] = wi;
-    const double zi = a.z[i], ri = a.r[i];
-    v[0] += zi * wi;
-    v[1] += zi * ri;
-#pragma unroll
-    for (int j = 0; j < kFcgMaxM; j++) {
-      if (j < nd) {
-        v[2 + j] += zi * (double)a.q[j * n + i];
-        v[2 + kFcgMaxM + j] += (double)a.p[j * n + i] * ri;
-      }
-    }
-  }
+__device__ __forceinline__ void fcg_spmv_finish(const FcgArgs<VT>& a, double (&v)[kFcgParts], int nd, int m, int it) {
   block_sum<kFcgParts>(v);
   if (!post_partials<kFcgParts>(v, a.st.part, a.st.cnt)) return;
   gather_partials<kFcgParts>(a.st.part, gridDim.x, v);
   if (threadIdx.x == 0) {
     double* s = a.st.sc;
+    if (ld_volatile_i32(a.st.err)) {
+      s[kFcgStatus] = 3;  // a bounded wait of the matrix stream gave up
+      a.st.done[0] = 1;
+      return;
+    }
     double pq = v[0], pr = v[1];
     double beta[kFcgMaxM];
 #pragma unroll
@@ -172,6 +133,191 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_spmv(FcgArgs<VT> a) {
     s[kFcgAlpha] = alpha;
     s[kFcgPQ0 + it % m] = pq;  // the new direction takes the oldest slot
   }
+}
+
+// r = b - Z x (warm) or r = b, x = 0; partials {(b,b), (r,r)}; the last
+// block initialises the state words.
+template <class VT>
+__global__ void __launch_bounds__(kFcgThreads) k_fcg_start(FcgArgs<VT> a, int warm) {
+  double v[2] = {0, 0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const VT bi = a.b[i];
+    VT ri = bi;
+    if (warm)
+      ri = bi - sell_row(a.off, a.col, a.val, a.x, i);
+    else
+      a.x[i] = 0;
+    a.r[i] = ri;
+    v[0] += (double)bi * bi;
+    v[1] += (double)ri * ri;
+  }
+  block_sum<2>(v);
+  if (!post_partials<2>(v, a.st.part, a.st.cnt)) return;
+  gather_partials<2>(a.st.part, gridDim.x, v);
+  if (threadIdx.x == 0) {
+    const FcgState& st = a.st;
+    double* sc = st.sc;
+    *st.err = 0;
+    sc[kFcgBB] = v[0];
+    sc[kFcgRR] = v[1];
+    sc[kFcgRRMark] = v[1];
+    sc[kFcgIt] = 0;
+    sc[kFcgRtol] = st.rtol;
+    sc[kFcgStall2] = st.stall2;
+    sc[kFcgMaxit] = st.maxit;
+    sc[kFcgWindow] = st.window;
+    sc[kFcgM] = st.m;
+    int done = 0;
+    double status = -1;
+    if (!isfinite(v[0]) || !isfinite(v[1])) {
+      status = 2;
+      done = 1;
+    } else if (v[1] <= st.rtol * st.rtol * v[0]) {
+      status = 0;
+      done = 1;
+    }
+    sc[kFcgStatus] = status;
+    st.done[0] = done;
+  }
+}
+
+// w = Z z with the matrix streamed through shared memory (ChunkStream, as in
+// the persistent PCG): 16 warps per block, each owning a contiguous range of
+// 32-row slices, lane = row.
+template <class VT>
+__global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
+  if (*a.st.done) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const double* sc = a.st.sc;
+  const int m = (int)sc[kFcgM], it = (int)sc[kFcgIt];
+  const int nd = it < m ? it : m;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nslices = (a.n + 31) >> 5;
+  const int W = gridDim.x * kPcgWarps, gw = blockIdx.x * kPcgWarps + wib;
+  Chunk<VT>* chunks = reinterpret_cast<Chunk<VT>*>(smem);
+  unsigned long long* mbars =
+      reinterpret_cast<unsigned long long*>(smem + (size_t)kPcgWarps * kNbuf<VT> * sizeof(Chunk<VT>));
+  ChunkStream<VT> st;
+  st.off = a.off;
+  st.col = a.col;
+  st.val = a.val;
+  st.buf = chunks + wib * kNbuf<VT>;
+  st.mbar = mbars + wib * kNbuf<VT>;
+  st.s_begin = (int)((long long)nslices * gw / W);
+  st.s_end = (int)((long long)nslices * (gw + 1) / W);
+  st.is = st.cs = st.s_begin;
+  st.ik = st.ck = 0;
+  st.nbi = st.nbc = 0;
+  st.parity = 0;
+  st.failed = false;
+  if (lane == 0)
+    for (int k = 0; k < kNbuf<VT>; k++) mbar_init(st.mbar + k, 1);
+  mbar_init_fence();
+  __syncwarp();
+  st.start(lane);
+  double v[kFcgParts];
+#pragma unroll
+  for (int k = 0; k < kFcgParts; k++) v[k] = 0.0;
+  for (int sl = st.s_begin; sl < st.s_end; sl++) {
+    VT acc = 0;
+    const int wd = (__ldg(a.off + sl + 1) - __ldg(a.off + sl)) >> 5;
+    for (int c0 = 0; c0 < wd; c0 += kCh) {
+      if (st.wait(a.st.err, a.st.timeout_ns)) acc += chunk_dot<VT>(st.buf + st.nbc, min(kCh, wd - c0), lane, a.z);
+      st.release(lane);
+    }
+    const int i = sl * 32 + lane;
+    if (i < a.n) fcg_row_dots(a, i, acc, nd, v);
+  }
+  if (!st.failed) st.drain(a.st.timeout_ns);
+  fcg_spmv_finish(a, v, nd, m, it);
+}
+
+// w = Z z on a structured grid of pressure nodes (identity numbering, node
+// x + fx (y + fy z)): Z couples nodes within two grid steps per axis, so a
+// row is 125 coefficients.  They are stored per 32-row slice, tap-major
+// inside the slice (coef[slice][tap][lane], zero for couplings that do not
+// exist): no column indices are streamed, and the gathers of z are
+// contiguous across the warp.  Each warp owns a contiguous range of slices
+// and streams it through shared memory in chunks of 25 taps (one dz plane,
+// 3.2 KB), two chunks in flight per warp on bulk asynchronous copies.  Taps
+// that leave the grid have zero coefficients; their index is clamped.
+constexpr int kStTaps = 25;
+constexpr int kStBuf = 2;
+template <class VT>
+constexpr size_t stencil_smem_bytes() {
+  return (size_t)kPcgWarps * kStBuf * (kStTaps * 32 * sizeof(VT) + sizeof(unsigned long long));
+}
+
+template <class VT>
+__global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT> a) {
+  if (*a.st.done) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const double* sc = a.st.sc;
+  const int m = (int)sc[kFcgM], it = (int)sc[kFcgIt];
+  const int nd = it < m ? it : m;
+  const int n = a.n, fx = a.fd[0], fxy = a.fd[0] * a.fd[1];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int nslices = (n + 31) >> 5;
+  const int W = gridDim.x * kPcgWarps, gw = blockIdx.x * kPcgWarps + wib;
+  const int s0 = (int)((long long)nslices * gw / W), s1 = (int)((long long)nslices * (gw + 1) / W);
+  constexpr unsigned kChunkBytes = kStTaps * 32 * sizeof(VT);
+  VT* buf = reinterpret_cast<VT*>(smem) + (size_t)wib * kStBuf * kStTaps * 32;
+  unsigned long long* mbar =
+      reinterpret_cast<unsigned long long*>(smem + (size_t)kPcgWarps * kStBuf * kChunkBytes) + wib * kStBuf;
+  const int total = (s1 - s0) * 5;  // chunks of this warp
+  if (lane == 0)
+    for (int b = 0; b < kStBuf; b++) mbar_init(mbar + b, 1);
+  mbar_init_fence();
+  __syncwarp();
+  auto issue = [&](int k) {  // chunk k of the warp's range into buffer k % kStBuf
+    if (lane == 0 && k < total) {
+      const int b = k % kStBuf;
+      const VT* src = a.stencil + ((size_t)(s0 + k / 5) * 125 + (k % 5) * kStTaps) * 32;
+      fence_proxy_async_smem();
+      mbar_expect_tx(mbar + b, kChunkBytes);
+      bulk_g2s(buf + (size_t)b * kStTaps * 32, src, kChunkBytes, mbar + b);
+    }
+  };
+  for (int k = 0; k < kStBuf; k++) issue(k);
+  bool ok = true;
+  int kfail = 0;
+  const VT* __restrict__ z = a.z;
+  double v[kFcgParts];
+#pragma unroll
+  for (int k = 0; k < kFcgParts; k++) v[k] = 0.0;
+  int k = 0;
+  for (int sl = s0; sl < s1; sl++) {
+    const int i = sl * 32 + lane;
+    VT acc = 0;
+    for (int dz = -2; dz <= 2; dz++, k++) {
+      const int b = k % kStBuf;
+      if (ok && !mbar_wait_bounded(mbar + b, (unsigned)((k / kStBuf) & 1), a.st.timeout_ns)) {
+        ok = false;
+        kfail = k;
+        if (lane == 0) atomicExch(a.st.err, 1);
+      }
+      if (ok) {
+        const VT* q = buf + (size_t)b * kStTaps * 32 + lane;
+#pragma unroll
+        for (int t = 0; t < kStTaps; t++) {
+          const int dy = t / 5 - 2, dx = t % 5 - 2;
+          int j = i + dx + fx * dy + fxy * dz;
+          j = j < 0 ? 0 : (j >= n ? n - 1 : j);
+          acc += q[t * 32] * __ldg(z + j);
+        }
+      }
+      __syncwarp();
+      if (ok) issue(k + kStBuf);
+    }
+    if (i < n) fcg_row_dots(a, i, acc, nd, v);
+  }
+  if (!ok && lane == 0) {
+    // a bounded wait gave up: give the copies still in flight one more
+    // bounded wait before the block (and its shared memory) ends
+    for (int kk = kfail; kk < kfail + kStBuf && kk < total; kk++)
+      mbar_wait_bounded(mbar + kk % kStBuf, (unsigned)((kk / kStBuf) & 1), a.st.timeout_ns);
+  }
+  fcg_spmv_finish(a, v, nd, m, it);
 }
 
 template <class VT>
@@ -229,6 +375,25 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_update(FcgArgs<VT> a) {
   }
 }
 
+// coef[tap][row] of the structured form of a CSR matrix (identity numbering
+// on the grid fd); *bad = 1 when a coupling reaches beyond two grid steps.
+template <class VT>
+__global__ void k_stencil_build(int n, Int3 fd, const int* __restrict__ rp, const int* __restrict__ col,
+                                const double* __restrict__ val, VT* coef, int* bad) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int x = i % fd.v[0], y = (i / fd.v[0]) % fd.v[1], z = i / (fd.v[0] * fd.v[1]);
+    for (int k = rp[i]; k < rp[i + 1]; k++) {
+      const int j = col[k];
+      const int dx = j % fd.v[0] - x, dy = (j / fd.v[0]) % fd.v[1] - y, dz = j / (fd.v[0] * fd.v[1]) - z;
+      if (dx < -2 || dx > 2 || dy < -2 || dy > 2 || dz < -2 || dz > 2) {
+        atomicExch(bad, 1);
+        continue;
+      }
+      coef[((size_t)(i >> 5) * 125 + (dz + 2) * 25 + (dy + 2) * 5 + (dx + 2)) * 32 + (i & 31)] = (VT)val[k];
+    }
+  }
+}
+
 int nblocks(int n) {
   const int g = (n + kFcgThreads - 1) / kFcgThreads;
   return g < kFcgMaxBlocks ? g : kFcgMaxBlocks;
@@ -237,7 +402,8 @@ int nblocks(int n) {
 }  // namespace
 
 int fcg_blocks(int n) { return nblocks(n); }
-int fcg_part_words(int n) { return kFcgParts * nblocks(n); }
+size_t stencil_elems(int n) { return (size_t)((n + 31) >> 5) * 125 * 32; }
+int fcg_part_words(int n) { return kFcgParts * (nblocks(n) > kFcgMaxBlocks ? nblocks(n) : kFcgMaxBlocks); }
 
 template <class VT>
 cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s) {
@@ -248,7 +414,19 @@ cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s) {
 
 template <class VT>
 cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s) {
-  k_fcg_spmv<VT><<<nblocks(a.n), kFcgThreads, 0, s>>>(a);
+  if (a.spmv_grid < 1 || a.spmv_grid > kFcgMaxBlocks) return cudaErrorInvalidValue;
+  if (a.stencil) {  // one wave of two blocks of 16 warps per SM
+    const size_t smem = stencil_smem_bytes<VT>();
+    cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv_stencil<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    k_fcg_spmv_stencil<VT><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
+    return cudaGetLastError();
+  }
+  const size_t smem = pcg_smem_bytes<VT>();
+  cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_fcg_spmv<VT><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -258,6 +436,19 @@ cudaError_t launch_fcg_update(const FcgArgs<VT>& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <class VT>
+cudaError_t launch_stencil_build(int n, const int fd[3], const int* rp, const int* col, const double* val, VT* coef,
+                                 int* bad, cudaStream_t s) {
+  Int3 g;
+  for (int k = 0; k < 3; k++) g.v[k] = fd[k];
+  cudaError_t e = cudaMemsetAsync(coef, 0, stencil_elems(n) * sizeof(VT), s);
+  if (e != cudaSuccess) return e;
+  k_stencil_build<VT><<<(n + 255) / 256, 256, 0, s>>>(n, g, rp, col, val, coef, bad);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_stencil_build<float>(int, const int*, const int*, const int*, const double*, float*, int*,
+                                                 cudaStream_t);
 template cudaError_t launch_fcg_start<float>(const FcgArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_fcg_start<double>(const FcgArgs<double>&, int, cudaStream_t);
 template cudaError_t launch_fcg_spmv<float>(const FcgArgs<float>&, cudaStream_t);

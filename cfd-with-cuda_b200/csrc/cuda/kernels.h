@@ -13,6 +13,7 @@
 //                           entry j is one contiguous 128/256-byte segment.
 //                           Padding entries hold value 0 and a valid column.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -170,17 +171,61 @@ struct FcgState {
   double* part;   // fcg_part_words(n) words
   unsigned* cnt;  // block arrival counter, zero between kernels (host-zeroed once)
   int* done;      // kernels return at once while *done != 0
+  int* err;       // set when a bounded wait of the matrix stream gives up (status 3)
+  unsigned long long timeout_ns;
   double rtol, stall2;  // read by the start kernel only
   int maxit, window, m;
 };
-// p and q point at m ring slots of n entries each.
+// p and q point at m ring slots of n entries each; spmv_grid: blocks of the
+// SpMV kernel (two per SM, at most kFcgMaxBlocks).  stencil (may be null):
+// the matrix in structured form (launch_stencil_build) on the grid fd, used
+// by the SpMV instead of the SELL arrays.
 template <class VT> struct FcgArgs {
   int n; const int *off, *col; const VT* val; const VT* b;
   VT *x, *r, *z, *w, *p, *q;
+  int spmv_grid;
+  const VT* stencil;
+  int fd[3];
   FcgState st;
 };
+struct Int3 {
+  int v[3];
+};
+// The CSR matrix (rp, col, FP64 val; identity numbering on the grid fd) in
+// structured form: 125 coefficients per row, coef[slice][tap][lane] over
+// 32-row slices (stencil_elems(n) entries); *bad (host-zeroed) is set when a
+// coupling reaches further than two grid steps (the form does not apply).
+size_t stencil_elems(int n);
+template <class VT>
+cudaError_t launch_stencil_build(int n, const int fd[3], const int* rp, const int* col, const double* val, VT* coef,
+                                 int* bad, cudaStream_t s);
 int fcg_blocks(int n);
 int fcg_part_words(int n);
+
+// Two-level preconditioner on the structured pressure grid (coarse.cu): fine
+// voxel grid fd, coarse lattice cd (nc nodes), voxel -> pressure node pmap
+// (null: identity), per-axis hat tables (voxel -> first coarse node i0 and
+// weight f of the second), per coarse node the voxel range [lo, hi] of its
+// hat along each axis, and the dense inverse of P^T Z P stored FP16 as
+// inv16 = inv * inv_scale in rows of ldinv (nc rounded up to 8) entries.
+template <class VT> struct CoarseArgs {
+  int fd[3], cd[3], nc, ldinv;
+  const int* pmap;
+  const int *i0x, *i0y, *i0z;
+  const double *fx, *fy, *fz;
+  const int *rx, *ry, *rz;
+  const __half* inv16;
+  double inv_scale;
+};
+// c = P^T r (FP32 coarse vector), e = Zc^-1 c
+template <class VT>
+cudaError_t launch_coarse_restrict(const CoarseArgs<VT>& a, const VT* r, float* c, const int* done, cudaStream_t s);
+template <class VT>
+cudaError_t launch_coarse_solve(const CoarseArgs<VT>& a, const float* c, VT* e, const int* done, cudaStream_t s);
+// z[p(v)] = dinv r + (P e)[v] (e may be null) + y[v] sqrt(rr / nv) / dscale (y may be null)
+template <class VT>
+cudaError_t launch_precond(const CoarseArgs<VT>& a, int nv, const VT* r, const VT* dinv, const VT* e, const float* y,
+                           const double* rr, double dscale, VT* z, const int* done, cudaStream_t s);
 template <class VT> cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s);
 template <class VT> cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s);
 template <class VT> cudaError_t launch_fcg_update(const FcgArgs<VT>& a, cudaStream_t s);

@@ -365,22 +365,6 @@ __global__ void k_input(int nv, const T* __restrict__ r, const int* __restrict__
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
     x[i] = __float2bfloat16((float)r[pmap ? pmap[i] : i] * cf);
 }
-// z[p(v)] = out[v] * sqrt(rr / nv) / dscale + dinv[p(v)] r[p(v)]: the
-// network's correction, brought back to the residual's scale, on top of a
-// Jacobi step.
-template <class T>
-__global__ void k_output(int nv, const float* __restrict__ out, const int* __restrict__ pmap, const double* rr,
-                         double dscale, const T* __restrict__ dinv, const T* __restrict__ r, T* z,
-                         const int* skipflag) {
-  if (skipflag && *skipflag) return;
-  const double sc = rr[0] > 0.0 ? sqrt(rr[0] / (double)nv) / dscale : 0.0;
-  const T c = (T)sc;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x) {
-    const int p = pmap ? pmap[i] : i;
-    z[p] = (T)out[i] * c + dinv[p] * r[p];
-  }
-}
-
 __global__ void k_add(long long n, const float* __restrict__ a, float* b) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     b[i] += a[i];
@@ -569,17 +553,6 @@ cudaError_t unet_input(int nv, const float* r, const int* pmap, const double* rr
   k_input<float><<<grid1(nv), 256, 0, s>>>(nv, r, pmap, rr, scale, x, skipflag);
   return cudaGetLastError();
 }
-cudaError_t unet_output(int nv, const float* out, const int* pmap, const double* rr, double dscale,
-                        const double* dinv, const double* r, double* z, const int* skipflag, cudaStream_t s) {
-  k_output<double><<<grid1(nv), 256, 0, s>>>(nv, out, pmap, rr, dscale, dinv, r, z, skipflag);
-  return cudaGetLastError();
-}
-cudaError_t unet_output(int nv, const float* out, const int* pmap, const double* rr, double dscale,
-                        const float* dinv, const float* r, float* z, const int* skipflag, cudaStream_t s) {
-  k_output<float><<<grid1(nv), 256, 0, s>>>(nv, out, pmap, rr, dscale, dinv, r, z, skipflag);
-  return cudaGetLastError();
-}
-
 cudaError_t unet_loss(const int* dims, const float* out, const float* target, float* dout, float* lossv, float w_l2,
                       float w_h1, cudaStream_t s) {
   Dims3 g;

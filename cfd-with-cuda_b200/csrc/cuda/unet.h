@@ -64,15 +64,6 @@ cudaError_t unet_input(int nv, const double* r, const int* p_of_vox, const doubl
                        __nv_bfloat16* x, const int* skipflag, cudaStream_t s);
 cudaError_t unet_input(int nv, const float* r, const int* p_of_vox, const double* rr, double scale,
                        __nv_bfloat16* x, const int* skipflag, cudaStream_t s);
-// Preconditioned vector of flexible CG: z[p(v)] = out[v] * sqrt(rr[0] / nv)
-// / dscale + dinv[p(v)] r[p(v)] -- the network's correction (trained on
-// unit-RMS residuals and errors scaled by the median diagonal dscale) on top
-// of a Jacobi step.
-cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, const double* rr, double dscale,
-                        const double* dinv, const double* r, double* z, const int* skipflag, cudaStream_t s);
-cudaError_t unet_output(int nv, const float* out, const int* p_of_vox, const double* rr, double dscale,
-                        const float* dinv, const float* r, float* z, const int* skipflag, cudaStream_t s);
-
 // Training loss of one sample on grid dims, d = out - target:
 //   w_l2 mean(d^2) + w_h1 (1/n) sum over axes of (d[i+e] - d[i])^2
 // (neighbour pairs inside the grid); dout = its gradient, lossv[0] += loss.

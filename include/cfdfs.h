@@ -46,9 +46,14 @@ enum cfd_precision {
 };
 
 enum cfd_precond {
-  CFD_PC_JACOBI = 0,  /* Jacobi-preconditioned CG (reference behaviour) */
-  CFD_PC_LEARNED = 1  /* learned U-Net preconditioner in flexible CG, with
-                         Jacobi-PCG fallback when it stalls */
+  CFD_PC_JACOBI = 0,   /* Jacobi-preconditioned CG (reference behaviour) */
+  CFD_PC_LEARNED = 1,  /* Jacobi step + coarse-space correction + U-Net
+                          correction in flexible CG, with Jacobi-PCG fallback
+                          when it stalls */
+  CFD_PC_TWOLEVEL = 2  /* Jacobi step + coarse-space correction (P Zc^-1 P^T,
+                          Zc = P^T Z P on a coarse lattice of the structured
+                          pressure grid) in CG: the learned preconditioner
+                          without its network */
 };
 
 typedef struct cfd_ctx cfd_ctx;
@@ -261,6 +266,18 @@ int cfd_unet_attach(cfd_ctx* ctx, cfd_unet* net, const int dims[3], const int* p
 int cfd_unet_load(cfd_ctx* ctx, const char* path, const int dims[3]);
 /* r = rhs - Z x in FP64 (host buffers of NNp); *norm (may be NULL) = ||r||_2. */
 int cfd_pressure_residual(cfd_ctx* ctx, const double* rhs, const double* x, double* r, double* norm);
+/* Declares the structured grid of pressure nodes the coarse space and the
+ * network work on: dims (product = NNp) and p_of_vox as in cfd_unet_attach.
+ * Without it, a cube NNp = m^3 whose nodes are numbered x + m (y + m z) (node
+ * coordinates checked) is used.  No counterpart in the reference (new
+ * preconditioners). */
+int cfd_set_pressure_grid(cfd_ctx* ctx, const int dims[3], const int* p_of_vox);
+/* z = linear part of the configured preconditioner applied to r (FP64 host
+ * buffers of NNp): D^-1 r for CFD_PC_JACOBI, D^-1 r + P Zc^-1 P^T r for
+ * CFD_PC_TWOLEVEL and CFD_PC_LEARNED (the network's correction is not
+ * included).  Builds the coarse space on first use.  No counterpart in the
+ * reference (training targets of the network). */
+int cfd_precond_apply(cfd_ctx* ctx, const double* r, double* z);
 
 /* ---- timing, counters and self-tests ---------------------------------------- */
 
@@ -271,7 +288,7 @@ long long cfd_launch_count(const cfd_ctx* ctx);
 
 enum cfd_kernel_class {
   CFD_K_CONVECT = 0, CFD_K_STEP1, CFD_K_GT, CFD_K_PCG64, CFD_K_PCG32, CFD_K_RESID64, CFD_K_STEP3,
-  CFD_K_SPMV_K3, CFD_K_PUPDATE, CFD_K_OTHER, CFD_K_UNET, CFD_K_FCG, CFD_K_COUNT
+  CFD_K_SPMV_K3, CFD_K_PUPDATE, CFD_K_OTHER, CFD_K_UNET, CFD_K_FCG, CFD_K_COARSE, CFD_K_SPMV_Z, CFD_K_COUNT
 };
 /* Per-kernel-class CUDA-event timing on the context stream (on = 1 starts
  * and clears, 0 stops).  out receives CFD_K_COUNT triples

@@ -169,12 +169,13 @@ def test_flexible_cg_solves_to_tolerance(decks, precision):
     net.close()
 
 
-def test_zero_network_is_jacobi_cg(decks):
-    """The preconditioner is a Jacobi step plus the network's correction, so
-    a network that outputs zero turns flexible CG into Jacobi-PCG: same
-    iteration count (within rounding), no fallback."""
+def test_zero_network_is_twolevel_cg(decks):
+    """The preconditioner is a Jacobi step plus the coarse-space correction
+    plus the network's correction, so a network that outputs zero turns
+    flexible CG into CG with the two-level preconditioner: same iteration
+    count (within rounding), no fallback."""
     import cfdfs
-    s_j = _solver(decks["c1"])
+    s_j = _solver(decks["c1"], precond=cfdfs.PC_TWOLEVEL)
     s = _solver(decks["c1"], precond=cfdfs.PC_LEARNED)
     net = cfdfs.UNet(device=0, seed=5)
     net.set_params(np.zeros(net.nparam, dtype=np.float32))
