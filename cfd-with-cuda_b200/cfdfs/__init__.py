@@ -46,7 +46,7 @@ class CfdError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("precond", C.c_int), ("cg_rtol", C.c_double), ("cg_maxit", C.c_int),
                 ("cg_warm", C.c_int), ("ngp_override", C.c_int), ("inner_rtol", C.c_double),
-                ("max_outer", C.c_int), ("fcg_m", C.c_int)]
+                ("max_outer", C.c_int), ("fcg_m", C.c_int), ("fcg_net_iters", C.c_int)]
 
 
 class ProblemInfo(C.Structure):
@@ -233,7 +233,7 @@ class Solver:
 
     def __init__(self, device: int = 0, precision: int = FP64, cg_rtol: float = 1e-8, cg_maxit: int = 1000,
                  cg_warm: int = 0, ngp: int = 0, inner_rtol: float = 1e-4, max_outer: int = 12,
-                 precond: int = PC_JACOBI, fcg_m: int = 4):
+                 precond: int = PC_JACOBI, fcg_m: int = 4, fcg_net_iters: int = 0):
         L = lib()
         h = C.c_void_p()
         rc = L.cfd_create(C.byref(h), device)
@@ -243,6 +243,7 @@ class Solver:
         o = default_options()
         o.precision, o.precond, o.cg_rtol, o.cg_maxit, o.cg_warm = precision, precond, cg_rtol, cg_maxit, cg_warm
         o.ngp_override, o.inner_rtol, o.max_outer, o.fcg_m = ngp, inner_rtol, max_outer, fcg_m
+        o.fcg_net_iters = fcg_net_iters
         self._check(L.cfd_set_options(h, C.byref(o)))
         self.opts = o
         self.info = None
@@ -250,7 +251,8 @@ class Solver:
 
     def set_options(self, **kw):
         """Changes options of a live context (precision and ngp only before
-        load): precond, cg_rtol, cg_maxit, cg_warm, inner_rtol, max_outer, fcg_m."""
+        load): precond, cg_rtol, cg_maxit, cg_warm, inner_rtol, max_outer, fcg_m,
+        fcg_net_iters."""
         o = Options()
         C.memmove(C.byref(o), C.byref(self.opts), C.sizeof(Options))
         for k, v in kw.items():

@@ -56,10 +56,11 @@ struct FcgGraph {
     double dscale;
     int n;
     int coarse_gen;  // 0: no coarse space
+    int iters;       // flexible-CG iterations in the graph
     bool operator==(const Key& o) const {
       return b == o.b && x == o.x && work == o.work && net == o.net && gen == o.gen && plan_gen == o.plan_gen &&
              tc == o.tc && pmap == o.pmap && dinv == o.dinv && dscale == o.dscale && n == o.n &&
-             coarse_gen == o.coarse_gen;
+             coarse_gen == o.coarse_gen && iters == o.iters;
     }
   } key{};
   cudaGraphExec_t exec = nullptr;
@@ -156,7 +157,7 @@ struct cfd_ctx {
   DevBuf<int> fcg_done, fcg_err;
   int fcg_window = 25;
   bool fcg_use_graph = true;
-  FcgGraph fcg_graph[2];  // FP32 inner solves, FP64 solves
+  FcgGraph fcg_graph[2][2];  // [FP32 inner solves, FP64 solves][two-level only, with the network]
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
 
@@ -478,8 +479,8 @@ int set_grid(cfd_ctx* c, const int dims[3], const int* p_of_vox) {
   for (int a = 0; a < 3; a++) c->udims[a] = dims[a];
   c->grid_set = true;
   c->coarse_ready = false;
-  c->fcg_graph[0].reset();
-  c->fcg_graph[1].reset();
+  for (auto& gp : c->fcg_graph)
+    for (auto& g : gp) g.reset();
   return CFD_OK;
 }
 
@@ -598,8 +599,8 @@ int ensure_coarse(cfd_ctx* c) {
   }
   c->coarse_ready = true;
   c->coarse_gen++;
-  c->fcg_graph[0].reset();
-  c->fcg_graph[1].reset();
+  for (auto& gp : c->fcg_graph)
+    for (auto& g : gp) g.reset();
   c->coarse_setup_s = wall_seconds() - t0;
   return CFD_OK;
 }
@@ -707,7 +708,9 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   const CoarseArgs<VT> ca = coarse_args<VT>(c, true);
   // one flexible-CG iteration: preconditioner (U-Net, coarse restriction
   // and solve, combination), SpMV + dots + coefficients, update + tests
-  auto iteration = [&](bool counted) -> int {
+  auto iteration = [&](bool counted, bool with_net) -> int {
+    UnetNet* netp_all = netp;
+    UnetNet* netp = with_net ? netp_all : nullptr;
     const long long l0 = netp ? netp->launches : 0;
     auto unet = [&]() -> cudaError_t {
       cudaError_t e = unet_input(n, a.r, pmap, a.st.sc + kFcgRR, 0.0, netp->act[0], a.st.done, s);
@@ -739,20 +742,25 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
     }
     return CFD_OK;
   };
-  // CUDA graph of kFcgBatch iterations, captured once per buffer / network
-  // configuration and replayed until the done flag stops the kernels
-  FcgGraph* G = nullptr;
-  if (c->fcg_use_graph && !c->prof_on) {
-    if (netp) CU(netp->prepare_tc(s));  // packs and plans outside the capture
-    FcgGraph& g = c->fcg_graph[sizeof(VT) == 4 ? 0 : 1];
-    FcgGraph::Key key{a.b,  a.x, a.r, netp ? c->unet : nullptr, netp ? netp->gen : 0, netp ? netp->plan_gen : 0,
-                      netp ? netp->tc_enabled : false, pmap, dinv, c->unet_dscale, n, c->coarse_gen};
+  // CUDA graphs of kFcgBatch iterations (and, when the network is applied
+  // only in the first fcg_net_iters iterations, one graph of those),
+  // captured once per buffer / network configuration and replayed until the
+  // done flag stops the kernels
+  const int net_iters = !netp ? 0 : (c->opt.fcg_net_iters > 0 ? c->opt.fcg_net_iters : 1 << 30);
+  auto graph_for = [&](bool with_net, int iters, FcgGraph*& out) -> int {
+    out = nullptr;
+    if (!c->fcg_use_graph || c->prof_on) return CFD_OK;
+    if (with_net) CU(netp->prepare_tc(s));  // packs and plans outside the capture
+    FcgGraph& g = c->fcg_graph[sizeof(VT) == 4 ? 0 : 1][with_net ? 1 : 0];
+    FcgGraph::Key key{a.b, a.x, a.r, with_net ? c->unet : nullptr, with_net ? netp->gen : 0,
+                      with_net ? netp->plan_gen : 0, with_net ? netp->tc_enabled : false, pmap, dinv,
+                      c->unet_dscale, n, c->coarse_gen, iters};
     if (!g.exec || !(g.key == key)) {
       g.reset();
-      const long long l0 = netp ? netp->launches : 0;
+      const long long l0 = with_net ? netp->launches : 0;
       CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
       int rc = CFD_OK;
-      for (int k = 0; k < kFcgBatch && rc == CFD_OK; k++) rc = iteration(false);
+      for (int k = 0; k < iters && rc == CFD_OK; k++) rc = iteration(false, with_net);
       cudaGraph_t graph = nullptr;
       cudaError_t ce = cudaStreamEndCapture(s, &graph);
       if (rc) {
@@ -764,12 +772,40 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       cudaGraphDestroy(graph);
       CU(ce);
       g.key = key;
-      g.launches = (netp ? netp->launches - l0 + kFcgBatch : 0) + kFcgBatch * 5;
+      g.launches = (with_net ? netp->launches - l0 + iters : 0) + iters * 5;
     }
-    G = &g;
+    out = &g;
+    return CFD_OK;
+  };
+  const bool net_all = net_iters >= (1 << 30);
+  const int head = net_all ? 0 : net_iters;  // iterations of the network-only head
+  FcgGraph *G = nullptr, *GH = nullptr;
+  {
+    int rc = graph_for(net_all, kFcgBatch, G);
+    if (rc) return rc;
+    if (head > 0) {
+      rc = graph_for(true, std::min(head, kFcgBatch), GH);
+      if (rc) return rc;
+    }
   }
   int issued = 0, batch = 2;
   double rr_prev = -1;
+  if (head > 0) {
+    // the network's iterations first, then the two-level part alone
+    const int hb = std::min(head, kFcgBatch);
+    for (int done_h = 0; done_h < head; done_h += hb) {
+      if (GH) {
+        CU(cudaGraphLaunch(GH->exec, s));
+        c->launches += GH->launches;
+      } else {
+        for (int k = 0; k < hb; k++) {
+          int rc = iteration(true, true);
+          if (rc) return rc;
+        }
+      }
+      issued += hb;
+    }
+  }
   for (;;) {
     if (G) {
       const int reps = (batch + kFcgBatch - 1) / kFcgBatch;
@@ -780,7 +816,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       batch = reps * kFcgBatch;
     } else {
       for (int k = 0; k < batch; k++) {
-        int rc = iteration(true);
+        int rc = iteration(true, net_all);
         if (rc) return rc;
       }
     }
@@ -861,7 +897,8 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
     cudaStream_t s = c->stream;
     if (!warm) CU(cudaMemsetAsync(x, 0, c->P.NNp * sizeof(double), s));
     double bnorm = 0, rnorm = 0;
-    int rc = residual_norm(c, b, c->pzero, &bnorm);
+    // ||b|| (x = 0: the residual is b itself, and f_b = b for the first inner solve)
+    int rc = residual_norm(c, b, nullptr, &bnorm);
     if (rc) return rc;
     if (!std::isfinite(bnorm)) {
       z.status = 2;
@@ -869,7 +906,8 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
       CU(cudaMemsetAsync(x, 0, c->P.NNp * sizeof(double), s));
       z.status = 0;
     } else {
-      rc = residual_norm(c, b, x, &rnorm);
+      rnorm = bnorm;
+      if (warm) rc = residual_norm(c, b, x, &rnorm);
       if (rc) return rc;
       z.status = 1;
       int total = 0;
@@ -990,6 +1028,7 @@ int cfd_set_options(cfd_ctx* c, const cfd_options* o) {
   if (c->opt.max_outer <= 0) c->opt.max_outer = 12;
   if (c->opt.fcg_m <= 0) c->opt.fcg_m = 4;
   NEED(c->opt.fcg_m <= kFcgMaxM, "fcg_m must be in 1..8");
+  NEED(c->opt.fcg_net_iters >= 0, "fcg_net_iters must be >= 0");
   return CFD_OK;
 }
 
@@ -1752,8 +1791,8 @@ int cfd_unet_train_batch(cfd_unet* u, const int dims[3], int nb, const float* x,
 int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_vox) {
   if (!c) return CFD_E_BADARG;
   if (!u) {
-    c->fcg_graph[0].reset();
-    c->fcg_graph[1].reset();
+    for (auto& gp : c->fcg_graph)
+      for (auto& g : gp) g.reset();
     c->unet = nullptr;
     c->unet_owned.reset();
     return CFD_OK;
@@ -1772,8 +1811,8 @@ int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_
     int rc = set_grid(c, dims, p_of_vox);
     if (rc) return rc;
   }
-  c->fcg_graph[0].reset();
-  c->fcg_graph[1].reset();
+  for (auto& gp : c->fcg_graph)
+    for (auto& g : gp) g.reset();
   {
     std::vector<double> dg(nv);
     CU(cudaStreamSynchronize(c->stream));

@@ -237,6 +237,7 @@ template <class VT>
 int pcg_max_grid(int n, int device);
 
 // r = b - Z x (FP64, SELL-32 Z) and the partial sum of r^2 per block; rf = (float) r.
+// x == null stands for x = 0 (r = b, Z is not read).
 cudaError_t launch_residual64(int n, const int* off, const int* col, const double* val, const double* b,
                               const double* x, double* r, float* rf, double* part, int nblocks,
                               cudaStream_t s);

@@ -338,11 +338,13 @@ __global__ void __launch_bounds__(kResThreads) k_residual64(int n, const int* __
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double acc[1] = {0};
   if (i < n) {
-    const int s = i >> 5, l = i & 31;
-    const int bb = __ldg(off + s) + l, w = (__ldg(off + s + 1) - __ldg(off + s)) >> 5;
     double q = 0;
+    if (x) {  // x == null: x = 0, r = b without touching Z
+      const int s = i >> 5, l = i & 31;
+      const int bb = __ldg(off + s) + l, w = (__ldg(off + s + 1) - __ldg(off + s)) >> 5;
 #pragma unroll 4
-    for (int j = 0; j < w; j++) q += __ldcs(val + bb + 32 * j) * __ldg(x + __ldcs(col + bb + 32 * j));
+      for (int j = 0; j < w; j++) q += __ldcs(val + bb + 32 * j) * __ldg(x + __ldcs(col + bb + 32 * j));
+    }
     const double ri = b[i] - q;
     r[i] = ri;
     if (rf) rf[i] = (float)ri;

@@ -79,10 +79,47 @@ __global__ void __launch_bounds__(128) k_conv_fwd(ConvDesc d) {
   }
 }
 
+// Sixteen-input-channel convolution with a single FP32 output (the last
+// layer): one thread per output voxel, the 27 x 16 weights as float4 rows in
+// shared memory, two 16-byte loads per neighbour voxel.
+__global__ void __launch_bounds__(256) k_conv_16to1(ConvDesc d) {
+  __shared__ float4 sw[27 * 4];
+  if (d.skip && *d.skip) return;
+  for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) ((float*)sw)[i] = bf(d.w[i]);
+  const float b0 = d.bias[0];
+  __syncthreads();
+  const int nx = d.out_dims[0], ny = d.out_dims[1], nz = d.out_dims[2];
+  const int nv = nx * ny * nz;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    const int x = v % nx, t = v / nx, y = t % ny, z = t / ny;
+    float acc = b0;
+#pragma unroll 3
+    for (int k = 0; k < 27; k++) {
+      const int ix = x + k % 3 - 1, iy = y + (k / 3) % 3 - 1, iz = z + k / 9 - 1;
+      if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) continue;
+      const uint4* src = reinterpret_cast<const uint4*>(d.inA + (size_t)(ix + nx * (iy + ny * iz)) * 16);
+      const uint4 u0 = __ldg(src), u1 = __ldg(src + 1);
+      const __nv_bfloat162* h0 = reinterpret_cast<const __nv_bfloat162*>(&u0);
+      const __nv_bfloat162* h1 = reinterpret_cast<const __nv_bfloat162*>(&u1);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float4 w = sw[4 * k + q];
+        const float2 a = __bfloat1622float2(q < 2 ? h0[2 * q] : h1[2 * (q - 2)]);
+        const float2 b = __bfloat1622float2(q < 2 ? h0[2 * q + 1] : h1[2 * (q - 2) + 1]);
+        acc += a.x * w.x + a.y * w.y + b.x * w.z + b.y * w.w;
+      }
+    }
+    if (d.act && acc < 0.f) acc *= kLeaky;
+    d.out_f32[v] = acc;
+  }
+}
+
 // Single-input-channel convolution (the first layer) with 16 outputs: one
-// thread per output voxel, weights as float4 rows in shared memory, 32-bit
-// index arithmetic, two 16-byte stores per voxel.
-__global__ void __launch_bounds__(256, 3) k_conv_c1to16(ConvDesc d) {
+// thread per four consecutive output voxels along x (each weight row and
+// input value serves four voxels), weights as float4 rows in shared memory,
+// two 16-byte stores per voxel.
+__global__ void __launch_bounds__(256, 2) k_conv_c1to16(ConvDesc d) {
+  constexpr int XB = 4;  // consecutive voxels along x per thread: weights and inputs reused
   __shared__ float4 sw[27 * 4];
   __shared__ float sb[16];
   if (d.skip && *d.skip) return;
@@ -90,36 +127,60 @@ __global__ void __launch_bounds__(256, 3) k_conv_c1to16(ConvDesc d) {
   if (threadIdx.x < 16) sb[threadIdx.x] = d.bias[threadIdx.x];
   __syncthreads();
   const int nx = d.out_dims[0], ny = d.out_dims[1], nz = d.out_dims[2];
-  const int nv = nx * ny * nz;
-  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
-    const int x = v % nx, t = v / nx, y = t % ny, z = t / ny;
-    float acc[16];
+  const int gx = (nx + XB - 1) / XB;
+  const int ng = gx * ny * nz;
+  for (int gidx = blockIdx.x * blockDim.x + threadIdx.x; gidx < ng; gidx += gridDim.x * blockDim.x) {
+    const int xg = gidx % gx, t = gidx / gx, y = t % ny, z = t / ny;
+    const int x0 = xg * XB;
+    float acc[XB][16];
 #pragma unroll
-    for (int c = 0; c < 16; c++) acc[c] = sb[c];
-#pragma unroll 3
-    for (int k = 0; k < 27; k++) {
-      const int ix = x + k % 3 - 1, iy = y + (k / 3) % 3 - 1, iz = z + k / 9 - 1;
-      if (ix < 0 || iy < 0 || iz < 0 || ix >= nx || iy >= ny || iz >= nz) continue;
-      const float a = bf(d.inA[ix + nx * (iy + ny * iz)]);
+    for (int u = 0; u < XB; u++)
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const float4 w = sw[4 * k + q];
-        acc[4 * q] += a * w.x;
-        acc[4 * q + 1] += a * w.y;
-        acc[4 * q + 2] += a * w.z;
-        acc[4 * q + 3] += a * w.w;
+      for (int c = 0; c < 16; c++) acc[u][c] = sb[c];
+#pragma unroll 1
+    for (int dzy = 0; dzy < 9; dzy++) {
+      const int iy = y + dzy % 3 - 1, iz = z + dzy / 3 - 1;
+      if (iy < 0 || iz < 0 || iy >= ny || iz >= nz) continue;
+      // inputs x0-1 .. x0+XB (zero outside the grid)
+      float in[XB + 2];
+      const __nv_bfloat16* row = d.inA + (size_t)nx * (iy + (size_t)ny * iz);
+#pragma unroll
+      for (int k = 0; k < XB + 2; k++) {
+        const int ix = x0 - 1 + k;
+        in[k] = (ix >= 0 && ix < nx) ? bf(row[ix]) : 0.f;
+      }
+#pragma unroll
+      for (int dx = 0; dx < 3; dx++) {
+        const int tap = dx + 3 * dzy;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const float4 w = sw[4 * tap + q];
+#pragma unroll
+          for (int u = 0; u < XB; u++) {
+            const float a = in[u + dx];
+            acc[u][4 * q] += a * w.x;
+            acc[u][4 * q + 1] += a * w.y;
+            acc[u][4 * q + 2] += a * w.z;
+            acc[u][4 * q + 3] += a * w.w;
+          }
+        }
       }
     }
-    __align__(16) __nv_bfloat16 o[16];
 #pragma unroll
-    for (int c = 0; c < 16; c++) {
-      float yv = acc[c];
-      if (d.act && yv < 0.f) yv *= kLeaky;
-      o[c] = __float2bfloat16(yv);
+    for (int u = 0; u < XB; u++) {
+      if (x0 + u >= nx) break;
+      __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+      for (int c = 0; c < 16; c++) {
+        float yv = acc[u][c];
+        if (d.act && yv < 0.f) yv *= kLeaky;
+        o[c] = __float2bfloat16(yv);
+      }
+      const size_t v = (size_t)(x0 + u) + (size_t)nx * (y + (size_t)ny * z);
+      uint4* dst = (uint4*)(d.out + v * 16);
+      dst[0] = ((const uint4*)o)[0];
+      dst[1] = ((const uint4*)o)[1];
     }
-    uint4* dst = (uint4*)(d.out + (size_t)v * 16);
-    dst[0] = ((const uint4*)o)[0];
-    dst[1] = ((const uint4*)o)[1];
   }
 }
 
@@ -427,9 +488,13 @@ int grid1(long long n, int t = 256) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// Raises the kernel's dynamic shared-memory limit to the largest a block may
+// have when a launch needs more than the default: the limit belongs to the
+// kernel, and launches of other layers (or recorded in a CUDA graph) must
+// stay valid.
 template <class F>
 cudaError_t with_smem(F kernel, size_t bytes) {
-  if (bytes > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (bytes > 48 * 1024) return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   return cudaSuccess;
 }
 
@@ -440,7 +505,12 @@ cudaError_t conv3_forward(const ConvDesc& d, cudaStream_t s) {
   const long long nv = (long long)d.out_dims[0] * d.out_dims[1] * d.out_dims[2];
   const int gx = grid1(nv, 128);
   if (cin == 1 && d.cout == 16 && d.stride == 1 && d.out && !d.out_f32 && nv < (1LL << 31)) {
-    k_conv_c1to16<<<grid1(nv, 256), 256, 0, s>>>(d);
+    const long long ng = (long long)((d.out_dims[0] + 3) / 4) * d.out_dims[1] * d.out_dims[2];
+    k_conv_c1to16<<<grid1(ng, 256), 256, 0, s>>>(d);
+    return cudaGetLastError();
+  }
+  if (d.ca == 16 && d.cb == 0 && d.cout == 1 && d.stride == 1 && d.out_f32 && !d.out && nv < (1LL << 31)) {
+    k_conv_16to1<<<grid1(nv, 256), 256, 0, s>>>(d);
     return cudaGetLastError();
   }
   if (cin <= 48) {

@@ -77,7 +77,7 @@ cudaError_t adam_step(long long n, float* w, const float* g, float* m, float* v,
 cudaError_t f32_to_bf16(long long n, const float* a, __nv_bfloat16* b, cudaStream_t s);
 
 // ---- tensor-core path (unet_tc.cu): stride-1 and stride-2 convolutions,
-// cin in {16, 32, 64}, cout in {16, 32, 64} or 1 with FP32 output ----
+// cin in {16, 32, 64}, cout in {16, 32, 64} ----
 struct ConvTcParams {
   int dims[3];      // output grid
   int in_dims[3];   // input grid (stride 2: 2 dims - 1 per axis)

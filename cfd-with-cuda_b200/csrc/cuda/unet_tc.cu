@@ -216,21 +216,41 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvTcParams p) {
   }
   int phase = 0;
   for (int g0 = 0; g0 < p.tiles && ok; g0 += tpg) {
-    const int g1 = min(p.tiles, g0 + tpg);
-    // every warp's lane 0 issues the MMAs of its tiles (t = g0 + warp + 4j)
+    const int g1 = min(p.tiles, g0 + tpg), ntg = g1 - g0;
+    // Groups with fewer tiles than warps split the taps of a tile over S
+    // warps, each into its own accumulator columns (summed in the
+    // epilogue), so every warp issues MMAs.
+    int S = 1;
+    while (S * 2 * ntg <= NWARP && S * 2 * ntg * p.N <= kTmemCols) S *= 2;
     if (lane == 0) {
       tc_fence_after();
-      for (int t = g0 + warp; t < g1; t += NWARP) {
-        const unsigned d = tmem + (unsigned)((t - g0) * p.N);
-        const unsigned long long dat = da0 + (unsigned)(p.q0 + 128 * t);
+      if (S == 1) {
+        // every warp's lane 0 issues the MMAs of its tiles (t = g0 + warp + 4j)
+        for (int t = g0 + warp; t < g1; t += NWARP) {
+          const unsigned d = tmem + (unsigned)((t - g0) * p.N);
+          const unsigned long long dat = da0 + (unsigned)(p.q0 + 128 * t);
 #pragma unroll
-        for (int k = 0; k < 27; k++) {
+          for (int k = 0; k < 27; k++) {
+            const unsigned long long dak = dat + (unsigned long long)(long long)toff[k];
+            const unsigned long long dbk = db0 + (unsigned long long)k * wtap16;
+#pragma unroll
+            for (int j = 0; j < KSTEPS; j++)
+              umma(d, dak + (unsigned long long)(2 * j) * plane16, dbk + (unsigned long long)(2 * j) * wk16, idesc,
+                   (k | j) != 0);
+          }
+        }
+      } else if (warp < ntg * S) {
+        // warp = (tile, split): taps k = split, split + S, ...
+        const int t = g0 + warp / S, sp = warp % S;
+        const unsigned d = tmem + (unsigned)(((t - g0) * S + sp) * p.N);
+        const unsigned long long dat = da0 + (unsigned)(p.q0 + 128 * t);
+        for (int k = sp; k < 27; k += S) {
           const unsigned long long dak = dat + (unsigned long long)(long long)toff[k];
           const unsigned long long dbk = db0 + (unsigned long long)k * wtap16;
 #pragma unroll
           for (int j = 0; j < KSTEPS; j++)
             umma(d, dak + (unsigned long long)(2 * j) * plane16, dbk + (unsigned long long)(2 * j) * wk16, idesc,
-                 (k | j) != 0);
+                 (k != sp || j != 0) ? 1u : 0u);
         }
       }
       umma_commit(&bars[1 + warp]);
@@ -256,7 +276,13 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvTcParams p) {
       const long long v = X + (long long)p.dims[0] * (Y + (long long)p.dims[1] * Z);
       for (int c = 0; c < p.N; c += 16) {
         float acc[16];
-        tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)((t - g0) * p.N + c), acc);
+        tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)((t - g0) * S * p.N + c), acc);
+        for (int sp = 1; sp < S; sp++) {
+          float part[16];
+          tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + (unsigned)(((t - g0) * S + sp) * p.N + c), part);
+#pragma unroll
+          for (int i = 0; i < 16; i++) acc[i] += part[i];
+        }
         if (!valid) continue;
         if (p.out_f32) {
           if (n0 + c == 0) p.out_f32[v] = acc[0] + sbias[0];
@@ -331,8 +357,10 @@ bool conv_tc_supported(const ConvDesc& d) {
   bool dims_ok = true;
   for (int a = 0; a < 3; a++)
     dims_ok = dims_ok && (d.stride == 1 ? d.in_dims[a] == d.out_dims[a] : d.in_dims[a] == 2 * d.out_dims[a] - 1);
+  // (the single-output last layer runs on CUDA cores: a 16-column MMA would
+  // compute 15 unused channels)
   return (d.stride == 1 || d.stride == 2) && dims_ok && d.cb == 0 && (d.ca == 16 || d.ca == 32 || d.ca == 64) &&
-         (d.cout == 16 || d.cout == 32 || d.cout == 64 || (d.cout == 1 && d.out_f32 && !d.out));
+         (d.cout == 16 || d.cout == 32 || d.cout == 64);
 }
 
 cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
@@ -370,40 +398,28 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
     p.brick[a] = ceil_div(p.dims[a], p.nb[a]);
     p.halo[a] = p.brick[a] + hpad;
   }
-  // bricks along z: enough CTAs for two per SM when two fit next to each
+  // bricks along z: one wave of two CTAs per SM when two fit next to each
   // other in shared memory, else one wave of one CTA per SM with deeper bricks
-  long long budget = 113 * 1024;
-  int per_sm = 2;
-  const auto smem_of = [&](int tz) {
-    const int HX = p.halo[0], HY = p.halo[1], HZ = tz + hpad;
-    const int q0 = 1 + HX + HX * HY, last = p.brick[0] + HX * (p.brick[1] + HY * tz);
-    const int tiles = ceil_div(last - q0 + 1, 128);
-    const int rows = (std::max(HX * HY * HZ, q0 + 128 * tiles + (d.stride == 2 ? 0 : q0)) + 7) & ~7;
-    return (long long)nphase * nchunk * (((rows * 16) + 1023) & ~1023) + wbytes + 64 + 4 * p.N;
-  };
-  {
-    const int target = ceil_div(2 * num_sms, p.nb[0] * p.nb[1] * p.nslices);
-    if (smem_of(std::max(1, ceil_div(p.dims[2], std::max(1, target)))) > budget) {
-      per_sm = 1;
-      budget = 200 * 1024;
+  for (int per_sm = 2; per_sm >= 1; per_sm--) {
+    const long long budget = per_sm == 2 ? 113 * 1024 : 220 * 1024;
+    const int target = std::max(1, per_sm * num_sms / (p.nb[0] * p.nb[1] * p.nslices));
+    int tz = std::max(1, ceil_div(p.dims[2], target));
+    for (;; tz--) {
+      p.brick[2] = tz;
+      p.halo[2] = tz + hpad;
+      const int HX = p.halo[0], HY = p.halo[1];
+      p.q0 = 1 + HX + HX * HY;
+      const int last = p.brick[0] + HX * (p.brick[1] + HY * p.brick[2]);
+      p.tiles = ceil_div(last - p.q0 + 1, 128);
+      const int off_max = d.stride == 2 ? 0 : 1 + HX + HX * HY;
+      int rows = std::max(HX * HY * p.halo[2], p.q0 + 128 * p.tiles + off_max);
+      p.rows = (rows + 7) & ~7;
+      p.plane_bytes = ((p.rows * 16) + 1023) & ~1023;
+      plan.smem = (size_t)nphase * nchunk * p.plane_bytes + wbytes + 64 + 4 * p.N;
+      if ((long long)plan.smem <= budget || tz == 1) break;
     }
-  }
-  // z-bricks per column: as many as fit in one wave of per_sm CTAs per SM
-  const int target = std::max(1, per_sm * num_sms / (p.nb[0] * p.nb[1] * p.nslices));
-  int tz = std::max(1, ceil_div(p.dims[2], target));
-  for (;; tz--) {
-    p.brick[2] = tz;
-    p.halo[2] = tz + hpad;
-    const int HX = p.halo[0], HY = p.halo[1];
-    p.q0 = 1 + HX + HX * HY;
-    const int last = p.brick[0] + HX * (p.brick[1] + HY * p.brick[2]);
-    p.tiles = ceil_div(last - p.q0 + 1, 128);
-    const int off_max = d.stride == 2 ? 0 : 1 + HX + HX * HY;
-    int rows = std::max(HX * HY * p.halo[2], p.q0 + 128 * p.tiles + off_max);
-    p.rows = (rows + 7) & ~7;
-    p.plane_bytes = ((p.rows * 16) + 1023) & ~1023;
-    plan.smem = (size_t)nphase * nchunk * p.plane_bytes + wbytes + 64 + 4 * p.N;
-    if ((long long)plan.smem <= budget || tz == 1) break;
+    const int ctas = p.nb[0] * p.nb[1] * ceil_div(p.dims[2], p.brick[2]) * p.nslices;
+    if ((long long)plan.smem <= budget && ctas <= per_sm * num_sms) break;  // fits one wave
   }
   if (plan.smem > 227 * 1024) return -3;
   {
@@ -443,7 +459,11 @@ cudaError_t conv3_forward_tc(const ConvTcPlan& plan, float* out_f32, const int* 
     case 64 * 4 + 2: k = k_conv_tc<64, 2>; break;
     default: return cudaErrorInvalidValue;
   }
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem);
+  // The limit is a property of the kernel, not of the launch: layers of one
+  // instantiation need different amounts, and a launch recorded in a CUDA
+  // graph must stay valid after a later layer's launch, so the limit is
+  // always the largest a block may have.
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return e;
   k<<<dim3(plan.grid_x, p.nslices), kTcThreads, plan.smem, s>>>(p);
   return cudaGetLastError();

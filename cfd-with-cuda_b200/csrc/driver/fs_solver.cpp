@@ -56,6 +56,7 @@ int main(int argc, char** argv) {
   if (const char* p = std::getenv("CFD_CG_RTOL")) o.cg_rtol = std::atof(p);
   if (const char* p = std::getenv("CFD_CG_WARM")) o.cg_warm = std::atoi(p);
   if (const char* p = std::getenv("CFD_NGP")) o.ngp_override = std::atoi(p);
+  if (const char* p = std::getenv("CFD_PRECOND")) o.precond = std::strcmp(p, "twolevel") == 0 ? CFD_PC_TWOLEVEL : CFD_PC_JACOBI;
   long maxsteps = -1;
   if (const char* p = std::getenv("CFD_MAXSTEPS")) maxsteps = std::atol(p);
   check(c, cfd_set_options(c, &o), "cfd_set_options");
