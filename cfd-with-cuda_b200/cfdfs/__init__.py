@@ -138,6 +138,7 @@ _PROTOS = {
     "cfdh_get_bcnodes": (C.c_int, [_vp, _ip]),
     "cfdh_get_pattern": (C.c_int, [_vp, C.c_int, _ip, _ip]),
     "cfdh_write_tecplot": (C.c_int, [_vp, _dp, _dp, _cp, _cp]),
+    "cfdh_coarse_inverse": (C.c_int, [_ip, _ip, _ip, _dp, _ip, _dp]),
 }
 
 
@@ -630,6 +631,28 @@ class UNet:
             self._check(self.L.cfd_unet_train_batch(self.h, _p(d, C.c_int), x.shape[0], x.ctypes.data,
                                                     t.ctypes.data, 0, lr, C.byref(loss)))
         return float(loss.value)
+
+
+def coarse_inverse(dims, rowptr, col, val):
+    """Host-only coarse space of the two-level preconditioner for the CSR
+    matrix Z on the grid dims: (coarse nodes per axis, inverse of P^T Z P)."""
+    L = lib()
+    d = np.ascontiguousarray(dims, dtype=np.int32)
+    rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    vl = np.ascontiguousarray(val, dtype=np.float64)
+    cd = np.zeros(3, dtype=np.int32)
+    rc = L.cfdh_coarse_inverse(_p(d, C.c_int), _p(rp, C.c_int), _p(cl, C.c_int), _p(vl, C.c_double),
+                               _p(cd, C.c_int), None)
+    if rc != CFD_OK:
+        raise CfdError(rc, "cfdh_coarse_inverse: bad arguments")
+    nc = int(np.prod(cd))
+    inv = np.zeros((nc, nc))
+    rc = L.cfdh_coarse_inverse(_p(d, C.c_int), _p(rp, C.c_int), _p(cl, C.c_int), _p(vl, C.c_double),
+                               _p(cd, C.c_int), _p(inv, C.c_double))
+    if rc != CFD_OK:
+        raise CfdError(rc, "cfdh_coarse_inverse: the coarse matrix is not positive definite")
+    return tuple(int(v) for v in cd), inv
 
 
 NOALLOC_MAX_N = 524288

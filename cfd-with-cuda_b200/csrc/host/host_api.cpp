@@ -4,8 +4,10 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../../include/cfdfs.h"
+#include "coarse.h"
 #include "problem.h"
 
 namespace cfd {
@@ -81,6 +83,28 @@ int cfdh_get_pattern(const cfd_host* h, int which, int* rowptr, int* col) {
 int cfdh_write_tecplot(const cfd_host* h, const double* U, const double* Pv, const char* path, const char* title) {
   if (!h || !U || !Pv || !path) return CFD_E_BADARG;
   return cfd::write_tecplot(h->P, U, Pv, path, title ? title : "");
+}
+
+int cfdh_coarse_inverse(const int dims[3], const int* rowptr, const int* col, const double* val, int* cd,
+                        double* inv) {
+  if (!dims || !rowptr || !col || !val || !cd) return CFD_E_BADARG;
+  const long long n = (long long)dims[0] * dims[1] * dims[2];
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || n > (1LL << 30)) return CFD_E_BADARG;
+  const int kMaxNodes = 6000;
+  if (!inv) {
+    double h[3];
+    cfd::coarse_lattice(dims, kMaxNodes, cd, h);
+    return CFD_OK;
+  }
+  std::vector<int> rp(rowptr, rowptr + n + 1);
+  std::vector<int> cl(col, col + rp[n]);
+  std::vector<double> vl(val, val + rp[n]);
+  cfd::CoarseSpace cs;
+  std::string err;
+  if (cfd::coarse_build(dims, kMaxNodes, std::vector<int>(), rp, cl, vl, cs, err)) return CFD_E_NONFINITE;
+  for (int a = 0; a < 3; a++) cd[a] = cs.cd[a];
+  std::copy(cs.inv.begin(), cs.inv.end(), inv);
+  return CFD_OK;
 }
 
 }  // extern "C"

@@ -338,6 +338,13 @@ int cfdh_sizes(const cfd_host* h, long long* out12);
 int cfdh_get_ltog(const cfd_host* h, int* out);     /* NE x 27 */
 int cfdh_get_coord(const cfd_host* h, double* out); /* NN x 3 */
 int cfdh_get_bcnodes(const cfd_host* h, int* out);  /* nBCnodes x 2 (node, bc) */
+/* Coarse space of the two-level preconditioner for a CSR matrix Z (n rows,
+ * FP64 values) on a structured grid dims (product = n, identity numbering
+ * x + nx (y + ny z)): cd receives the coarse nodes per axis; inv (NULL: only
+ * the sizes) receives the nc x nc inverse of P^T Z P, nc = cd[0] cd[1] cd[2]
+ * (at most 6000).  Host only; no counterpart in the reference. */
+int cfdh_coarse_inverse(const int dims[3], const int* rowptr, const int* col, const double* val, int* cd,
+                        double* inv);
 /* which: 0 K (NN x NN), 1 G (NN x NNp), 2 G^T (NNp x NN), 3 Z (NNp x NNp) */
 int cfdh_get_pattern(const cfd_host* h, int which, int* rowptr, int* col);
 /* createTecplot layout (blascoCodinaHuerta.cpp:4249-4482) for given state. */

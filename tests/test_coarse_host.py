@@ -1,0 +1,62 @@
+"""Host construction of the two-level preconditioner's coarse space (no GPU):
+the coarse lattice sizes and the inverse of P^T Z P from the library's
+Cholesky against NumPy, with Z taken from the CPU oracle on generated
+cavity and duct decks.  FP64 throughout: relative 1e-10."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import rel_l2
+
+
+def _hats(n, s=4.0):
+    if n < 2:
+        return sp.csr_matrix(np.ones((n, 1)))
+    cd = max(2, min(int(np.ceil((n - 1) / s - 1e-9)) + 1, n))
+    h = (n - 1) / (cd - 1)
+    x = np.arange(n)
+    i = np.clip(np.floor(x / h).astype(int), 0, cd - 2)
+    f = np.clip(x / h - i, 0.0, 1.0)
+    return sp.csr_matrix((np.concatenate([1 - f, f]), (np.concatenate([x, x]), np.concatenate([i, i + 1]))),
+                         shape=(n, cd))
+
+
+@pytest.mark.parametrize("case", ["cavity", "duct"])
+def test_coarse_inverse_matches_numpy(case, tmp_path, oracle_mod):
+    import cfdfs
+    from cfdfs import meshgen
+    if case == "cavity":
+        deck = meshgen.write_cavity(str(tmp_path / "c.inp"), meshgen.CavitySpec(12, re=100, dt=0.01, steps=2, ngp=8))
+        dims = (13, 13, 13)
+    else:
+        deck = meshgen.write_duct(str(tmp_path / "d.inp"), n_cross=4, n_axial=24, steps=2, dt=0.01)
+        dims = meshgen.duct_grid_dims(4, 24)
+    o = oracle_mod.Oracle(deck)
+    o.step0()
+    Z = o.csr("Z").tocsr()
+    o.close()
+    cd, inv = cfdfs.coarse_inverse(dims, Z.indptr, Z.indices, Z.data)
+    P = sp.kron(_hats(dims[2]), sp.kron(_hats(dims[1]), _hats(dims[0]))).tocsr()
+    assert cd == tuple(_hats(n).shape[1] for n in dims)
+    ref = np.linalg.inv((P.T @ Z @ P).toarray())
+    assert rel_l2(inv, ref) < 1e-10
+    assert np.allclose(inv, inv.T, rtol=0, atol=1e-12 * np.abs(inv).max())
+
+
+def test_coarse_lattice_limits():
+    import cfdfs
+    # spacing 4 voxels where the axis allows; widened beyond 6000 nodes
+    rp = np.zeros(1, dtype=np.int32)
+    L = cfdfs.lib()
+    import ctypes as C
+    for dims, want in (((65, 65, 65), (17, 17, 17)), ((161, 25, 25), (41, 7, 7)), ((9, 9, 9), (3, 3, 3))):
+        d = np.array(dims, dtype=np.int32)
+        cd = np.zeros(3, dtype=np.int32)
+        assert L.cfdh_coarse_inverse(cfdfs._p(d, C.c_int), cfdfs._p(rp, C.c_int), cfdfs._p(rp, C.c_int),
+                                     cfdfs._p(np.zeros(1), C.c_double), cfdfs._p(cd, C.c_int), None) == 0
+        assert tuple(cd) == want
+    d = np.array((257, 257, 257), dtype=np.int32)
+    cd = np.zeros(3, dtype=np.int32)
+    L.cfdh_coarse_inverse(cfdfs._p(d, C.c_int), cfdfs._p(rp, C.c_int), cfdfs._p(rp, C.c_int),
+                          cfdfs._p(np.zeros(1), C.c_double), cfdfs._p(cd, C.c_int), None)
+    assert int(np.prod(cd)) <= 6000
