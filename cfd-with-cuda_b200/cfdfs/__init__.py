@@ -389,9 +389,16 @@ class Solver:
         self._check(self.L.cfd_get_monitor(self.h, node, _p(out, C.c_double)))
         return out
 
-    def state(self):
+    def state(self, out=None):
+        """(U, P) in the reference layout; out = (U, P) writes into the
+        caller's arrays (e.g. pinned host buffers) instead of new ones."""
         i = self.info or self.refresh()
-        U, P = np.zeros(3 * i.NN), np.zeros(i.NNp)
+        if out is None:
+            U, P = np.zeros(3 * i.NN), np.zeros(i.NNp)
+        else:
+            U, P = out
+            assert U.dtype == np.float64 and P.dtype == np.float64 and U.flags.c_contiguous and P.flags.c_contiguous
+            assert U.size == 3 * i.NN and P.size == i.NNp
         self._check(self.L.cfd_download_state(self.h, _p(U, C.c_double), _p(P, C.c_double)))
         return U, P
 

@@ -638,10 +638,13 @@ CoarseArgs<VT> coarse_args(const cfd_ctx* c, bool with_coarse) {
 // space must be built (ensure_coarse) before.  res = {iterations,
 // ||r||/||b||, status} with the status words of kernels.h (4 = stalled).
 template <class VT>
-int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, double* res) {
+int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, double* res, bool first_solve) {
   cudaStream_t s = c->stream;
   const int n = c->P.NNp;
-  const bool use_net = learned(c);
+  // with fcg_net_iters > 0 the network serves the head of the first inner
+  // solve of a pressure solve only; refinement sweeps solve for corrections
+  // of a solution already accurate to the inner tolerance
+  const bool use_net = learned(c) && (first_solve || c->opt.fcg_net_iters == 0);
   NEED(c->coarse_ready, "coarse space not built");
   UnetNet* netp = use_net ? &c->unet->net : nullptr;
   if (netp && netp->set_grid(c->udims, false)) return fail(c, CFD_E_NOMEM, "%s", netp->err.c_str());
@@ -875,7 +878,7 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
     if (fcg_path(c)) {
       int rc = ensure_coarse(c);
       if (rc) return rc;
-      rc = run_fcg<double>(c, b, x, warm, rtol, c->opt.cg_maxit, res);
+      rc = run_fcg<double>(c, b, x, warm, rtol, c->opt.cg_maxit, res, true);
       if (rc) return rc;
       used = (int)res[0];
       if ((int)res[2] != 0) {
@@ -921,7 +924,7 @@ int pressure_solve(cfd_ctx* c, const double* b, double* x, int warm, cfd_solve_s
         if (fcg_path(c) && !z.fallback) {
           rc = ensure_coarse(c);
           if (rc) return rc;
-          rc = run_fcg<float>(c, c->f_b.p, c->f_x.p, 0, inner, c->opt.cg_maxit - total, res);
+          rc = run_fcg<float>(c, c->f_b.p, c->f_x.p, 0, inner, c->opt.cg_maxit - total, res, outer == 0);
           if (rc) return rc;
           const int fs = (int)res[2];
           if (fs == 4 || fs == 2 || (fs == 1 && res[1] > 0.5)) z.fallback = 1;  // Jacobi-PCG from here on

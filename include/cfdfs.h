@@ -71,7 +71,8 @@ typedef struct {
   int fcg_m;         /* CFD_PC_LEARNED: flexible-CG directions each new one is
                         orthogonalised against, 1..8 (default 4) */
   int fcg_net_iters; /* CFD_PC_LEARNED: the network's correction is applied in
-                        the first fcg_net_iters iterations of each solve, the
+                        the first fcg_net_iters iterations of each pressure
+                        solve (of its first inner solve in CFD_MIXED), the
                         two-level part alone after them (0 = every iteration) */
 } cfd_options;
 
