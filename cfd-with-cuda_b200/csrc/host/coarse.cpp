@@ -55,6 +55,7 @@ bool cholesky(std::vector<double>& A, int n) {
       for (int i = j + 1; i < k1; i++) {
         double* ri = a + (size_t)i * n;
         double s = ri[j];
+#pragma omp simd reduction(- : s)
         for (int k = k0; k < j; k++) s -= ri[k] * rj[k];
         ri[j] = s / rj[j];
       }
@@ -66,6 +67,7 @@ bool cholesky(std::vector<double>& A, int n) {
       for (int j = k0; j < k1; j++) {
         const double* rj = a + (size_t)j * n;
         double s = ri[j];
+#pragma omp simd reduction(- : s)
         for (int k = k0; k < j; k++) s -= ri[k] * rj[k];
         ri[j] = s / rj[j];
       }
@@ -101,6 +103,7 @@ void cholesky_inverse(std::vector<double>& A, int n, std::vector<double>& inv) {
     for (int i = j + 1; i < n; i++) {
       const double* li = a + (size_t)i * n;
       double s = li[j] * ud[j];
+#pragma omp simd reduction(+ : s)
       for (int k = j + 1; k < i; k++) s += li[k] * uj[k];
       uj[i] = -s / ld[i];
     }
