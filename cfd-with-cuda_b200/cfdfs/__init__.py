@@ -46,7 +46,8 @@ class CfdError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("precond", C.c_int), ("cg_rtol", C.c_double), ("cg_maxit", C.c_int),
                 ("cg_warm", C.c_int), ("ngp_override", C.c_int), ("inner_rtol", C.c_double),
-                ("max_outer", C.c_int), ("fcg_m", C.c_int), ("fcg_net_iters", C.c_int)]
+                ("max_outer", C.c_int), ("fcg_m", C.c_int), ("fcg_net_iters", C.c_int),
+                ("deterministic", C.c_int)]
 
 
 class ProblemInfo(C.Structure):
@@ -139,6 +140,7 @@ _PROTOS = {
     "cfdh_get_pattern": (C.c_int, [_vp, C.c_int, _ip, _ip]),
     "cfdh_write_tecplot": (C.c_int, [_vp, _dp, _dp, _cp, _cp]),
     "cfdh_coarse_inverse": (C.c_int, [_ip, _ip, _ip, _dp, _ip, _dp]),
+    "cfdh_element_colors": (C.c_int, [_vp, _ip, _ip]),
 }
 
 
@@ -221,6 +223,17 @@ class HostMesh:
         self.L.cfdh_get_pattern(self.h, w, _p(rp, C.c_int), _p(col, C.c_int))
         return rp, col
 
+    def element_colors(self):
+        """(order, off): the deterministic mode's element colouring, colour c
+        owning order[off[c]:off[c+1]]."""
+        nc = self.L.cfdh_element_colors(self.h, None, None)
+        if nc < 0:
+            raise CfdError(nc, "more than 64 element colours")
+        order = np.zeros(self.NE, dtype=np.int32)
+        off = np.zeros(nc + 1, dtype=np.int32)
+        self.L.cfdh_element_colors(self.h, _p(order, C.c_int), _p(off, C.c_int))
+        return order, off
+
     def write_tecplot(self, U, P, path: str, title: str):
         U = np.ascontiguousarray(U, dtype=np.float64)
         P = np.ascontiguousarray(P, dtype=np.float64)
@@ -234,7 +247,7 @@ class Solver:
 
     def __init__(self, device: int = 0, precision: int = FP64, cg_rtol: float = 1e-8, cg_maxit: int = 1000,
                  cg_warm: int = 0, ngp: int = 0, inner_rtol: float = 1e-4, max_outer: int = 12,
-                 precond: int = PC_JACOBI, fcg_m: int = 4, fcg_net_iters: int = 0):
+                 precond: int = PC_JACOBI, fcg_m: int = 4, fcg_net_iters: int = 0, deterministic: int = 0):
         L = lib()
         h = C.c_void_p()
         rc = L.cfd_create(C.byref(h), device)
@@ -244,7 +257,7 @@ class Solver:
         o = default_options()
         o.precision, o.precond, o.cg_rtol, o.cg_maxit, o.cg_warm = precision, precond, cg_rtol, cg_maxit, cg_warm
         o.ngp_override, o.inner_rtol, o.max_outer, o.fcg_m = ngp, inner_rtol, max_outer, fcg_m
-        o.fcg_net_iters = fcg_net_iters
+        o.fcg_net_iters, o.deterministic = fcg_net_iters, deterministic
         self._check(L.cfd_set_options(h, C.byref(o)))
         self.opts = o
         self.info = None
@@ -253,7 +266,7 @@ class Solver:
     def set_options(self, **kw):
         """Changes options of a live context (precision and ngp only before
         load): precond, cg_rtol, cg_maxit, cg_warm, inner_rtol, max_outer, fcg_m,
-        fcg_net_iters."""
+        fcg_net_iters, deterministic."""
         o = Options()
         C.memmove(C.byref(o), C.byref(self.opts), C.sizeof(Options))
         for k, v in kw.items():

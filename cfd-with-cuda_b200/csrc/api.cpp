@@ -57,10 +57,11 @@ struct FcgGraph {
     int n;
     int coarse_gen;  // 0: no coarse space
     int iters;       // flexible-CG iterations in the graph
+    int m;           // directions kept (selects the SpMV's instantiation)
     bool operator==(const Key& o) const {
       return b == o.b && x == o.x && work == o.work && net == o.net && gen == o.gen && plan_gen == o.plan_gen &&
              tc == o.tc && pmap == o.pmap && dinv == o.dinv && dscale == o.dscale && n == o.n &&
-             coarse_gen == o.coarse_gen && iters == o.iters;
+             coarse_gen == o.coarse_gen && iters == o.iters && m == o.m;
     }
   } key{};
   cudaGraphExec_t exec = nullptr;
@@ -114,6 +115,8 @@ struct cfd_ctx {
 
   // mesh
   DevBuf<int> ltog, bcnodes;
+  DevBuf<int> elist;           // elements colour by colour (deterministic mode)
+  std::vector<int> color_off;  // colour c owns elist[color_off[c] .. color_off[c+1]); empty: > 64 colours
   DevBuf<double> coord, bcvals;
   DevBuf<Basis> basis;
   DevBuf<unsigned char> bcmask;
@@ -312,6 +315,15 @@ int upload_problem(cfd_ctx* c) {
   CU(cudaMemcpyAsync(c->basis.p, &hb, sizeof(Basis), cudaMemcpyHostToDevice, s));
   CU(upload(c->ltog, P.ltog, s));
   CU(upload(c->coord, P.coord, s));
+  {
+    std::vector<int> order;
+    c->color_off.clear();
+    if (color_elements(P, order, c->color_off) == 0) {
+      CU(upload(c->elist, order, s));
+    } else {
+      c->color_off.clear();
+    }
+  }
   CU(upload(c->k_rp, P.k_rp, s));
   CU(upload(c->k_col, P.k_col, s));
   CU(upload(c->g_rp, P.g_rp, s));
@@ -757,7 +769,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
     FcgGraph& g = c->fcg_graph[sizeof(VT) == 4 ? 0 : 1][with_net ? 1 : 0];
     FcgGraph::Key key{a.b, a.x, a.r, with_net ? c->unet : nullptr, with_net ? netp->gen : 0,
                       with_net ? netp->plan_gen : 0, with_net ? netp->tc_enabled : false, pmap, dinv,
-                      c->unet_dscale, n, c->coarse_gen, iters};
+                      c->unet_dscale, n, c->coarse_gen, iters, a.st.m};
     if (!g.exec || !(g.key == key)) {
       g.reset();
       const long long l0 = with_net ? netp->launches : 0;
@@ -1111,7 +1123,20 @@ int cfd_step0(cfd_ctx* c) {
   a.k_rp = c->k_rp.p; a.k_col = c->k_col.p; a.kval = c->kval.p;
   a.g_rp = c->g_rp.p; a.g_col = c->g_col.p; a.g1 = c->g1.p; a.g2 = c->g2.p; a.g3 = c->g3.p;
   a.msum = c->msum.p;
-  CU(launch_assemble(a, c->num_sms, s));
+  if (c->opt.deterministic) {
+    NEED(!c->color_off.empty(), "deterministic mode: the mesh needs more than 64 element colours");
+    a.elist = c->elist.p;
+    a.plain = 1;
+    for (size_t k = 0; k + 1 < c->color_off.size(); k++) {
+      a.e_begin = c->color_off[k];
+      a.e_end = c->color_off[k + 1];
+      CU(launch_assemble(a, c->num_sms, s));
+    }
+  } else {
+    a.e_begin = 0;
+    a.e_end = P.NE;
+    CU(launch_assemble(a, c->num_sms, s));
+  }
   CU(launch_fill_gt((long long)P.gt_col.size(), c->gt_pos.p, c->g1.p, c->g2.p, c->g3.p, c->gt1.p, c->gt2.p,
                     c->gt3.p, s));
   CU(launch_md_finalize(P.NN, c->msum.p, c->bcmask.p, c->minv_orig.p, c->minv_free.p, s));
@@ -1166,14 +1191,30 @@ int cfd_convect(cfd_ctx* c) {
   NEED(c->assembled, "cfd_convect before cfd_step0");
   cudaStream_t s = c->stream;
   CU(cudaMemsetAsync(c->r1conv, 0, c->P.NN * sizeof(double4), s));
+  NEED(!c->opt.deterministic || !c->color_off.empty(),
+       "deterministic mode: the mesh needs more than 64 element colours");
+  auto run = [&](auto a, auto launch) -> int {
+    if (c->opt.deterministic) {  // one colour per launch, plain adds
+      a.elist = c->elist.p;
+      a.plain = 1;
+      for (size_t k = 0; k + 1 < c->color_off.size(); k++) {
+        a.e_begin = c->color_off[k];
+        a.e_end = c->color_off[k + 1];
+        KL(CFD_K_CONVECT, launch(a));
+      }
+    } else {
+      a.e_begin = 0;
+      a.e_end = c->P.NE;
+      KL(CFD_K_CONVECT, launch(a));
+    }
+    return CFD_OK;
+  };
   if (mixed(c)) {
     ConvArgs<float> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
-    KL(CFD_K_CONVECT, launch_convect<float>(a, c->num_sms, s));
-  } else {
-    ConvArgs<double> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
-    KL(CFD_K_CONVECT, launch_convect<double>(a, c->num_sms, s));
+    return run(a, [&](const ConvArgs<float>& x) { return launch_convect<float>(x, c->num_sms, s); });
   }
-  return CFD_OK;
+  ConvArgs<double> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
+  return run(a, [&](const ConvArgs<double>& x) { return launch_convect<double>(x, c->num_sms, s); });
 }
 
 int cfd_step1(cfd_ctx* c, int iter) {

@@ -8,6 +8,9 @@
 //   blocks Ke (27x27), Ge_d (27x8) and the row sums of Me are added into
 //   their CSR slots with FP64 atomics; the slot is found by binary search in
 //   the sorted CSR row, so no element colouring and no slot map is needed.
+//   In deterministic mode the host launches one colour at a time (no two
+//   elements of a colour share a node) and the blocks add without atomics,
+//   in the same order every run.
 // k_build_z: Z = sum_d G_d^T diag(MdOrigInv) G_d in gather form, one warp
 //   per Z row: for every velocity node v of G^T row p (ascending), the lanes
 //   take the columns q of G row v and add (G_d[v][q]*Minv[v]) * G_d[v][p] to
@@ -64,7 +67,8 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
   const Basis* B = a.basis;
   for (int i = t; i < ngp * 27; i += blockDim.x) sSv[i / 27][i % 27] = B->Sv[i / 27][i % 27];
   for (int i = t; i < ngp * 8; i += blockDim.x) sSp[i / 8][i % 8] = B->Sp[i / 8][i % 8];
-  for (int e = blockIdx.x; e < a.NE; e += gridDim.x) {
+  for (int pos = a.e_begin + blockIdx.x; pos < a.e_end; pos += gridDim.x) {
+    const int e = a.elist ? a.elist[pos] : pos;
     __syncthreads();
     if (t < 27) lt[t] = a.ltog[(size_t)e * 27 + t];
     __syncthreads();
@@ -94,7 +98,12 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
                wd[k];
         int row = lt[i], col = lt[j];
         int slot = bsearch_slot(a.k_col, a.k_rp[row], a.k_rp[row + 1], col);
-        if (slot >= 0) atomicAdd(a.kval + slot, s);
+        if (slot >= 0) {
+          if (a.plain)
+            a.kval[slot] += s;
+          else
+            atomicAdd(a.kval + slot, s);
+        }
       } else {
         int i = idx - 729;
         double s = 0;
@@ -103,7 +112,10 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
           for (int k = 0; k < ngp; k++) mij += sSv[k][i] * sSv[k][j] * wd[k];
           s += mij;
         }
-        atomicAdd(a.msum + lt[i], s);
+        if (a.plain)
+          a.msum[lt[i]] += s;
+        else
+          atomicAdd(a.msum + lt[i], s);
       }
     }
     // Ge_d[i][m] = -(1/rho) sum_k Sp[k][m] dSv_i/dx_d detJ w
@@ -119,9 +131,15 @@ __global__ void __launch_bounds__(kAsmThreads) k_assemble(AsmArgs a) {
       int row = lt[i], col = lt[m];
       int slot = bsearch_slot(a.g_col, a.g_rp[row], a.g_rp[row + 1], col);
       if (slot >= 0) {
-        atomicAdd(a.g1 + slot, s0);
-        atomicAdd(a.g2 + slot, s1);
-        atomicAdd(a.g3 + slot, s2);
+        if (a.plain) {
+          a.g1[slot] += s0;
+          a.g2[slot] += s1;
+          a.g3[slot] += s2;
+        } else {
+          atomicAdd(a.g1 + slot, s0);
+          atomicAdd(a.g2 + slot, s1);
+          atomicAdd(a.g3 + slot, s2);
+        }
       }
     }
   }
@@ -224,7 +242,9 @@ inline int grid_for(long long n, int threads, int cap = 148 * 32) {
 }  // namespace
 
 cudaError_t launch_assemble(const AsmArgs& a, int num_sms, cudaStream_t s) {
-  int grid = a.NE < num_sms * 16 ? a.NE : num_sms * 16;
+  const int ne = a.e_end - a.e_begin;
+  if (ne <= 0) return cudaSuccess;
+  int grid = ne < num_sms * 16 ? ne : num_sms * 16;
   k_assemble<<<grid, kAsmThreads, 0, s>>>(a);
   return cudaGetLastError();
 }

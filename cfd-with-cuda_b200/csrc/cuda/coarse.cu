@@ -85,7 +85,9 @@ __device__ __forceinline__ float dot8(const uint4& q, const float* c) {
 
 // e = inv c: one block of four warps per row, every thread with its share
 // of the row's 16-byte loads (8 FP16 entries each) in flight at once, FP32
-// products with c (read through L1), block sum.
+// products with c (read through L1), block sum.  The inverse is read with
+// an evict-last L2 policy (the SpMV's matrix stream is evict-first), so it
+// stays in L2 from one flexible-CG iteration to the next.
 constexpr int kMvThreads = 128;
 template <class VT>
 __global__ void __launch_bounds__(kMvThreads) k_coarse_mv(int nc, int ld, const __half* __restrict__ inv, float rscale,
@@ -95,16 +97,17 @@ __global__ void __launch_bounds__(kMvThreads) k_coarse_mv(int nc, int ld, const 
   const int row = blockIdx.x;
   const int nv8 = nc >> 3, tail = nc & 7;  // whole 8-entry groups inside the row, then a tail
   const uint4* ir = reinterpret_cast<const uint4*>(inv + (size_t)row * ld);
+  const unsigned long long keep = l2_evict_last();
   float s[4] = {0.f, 0.f, 0.f, 0.f};
   int k = threadIdx.x;
   for (; k + 3 * kMvThreads < nv8; k += 4 * kMvThreads) {
     uint4 q[4];
 #pragma unroll
-    for (int u = 0; u < 4; u++) q[u] = __ldcs(ir + k + u * kMvThreads);
+    for (int u = 0; u < 4; u++) q[u] = ldg_hint(ir + k + u * kMvThreads, keep);
 #pragma unroll
     for (int u = 0; u < 4; u++) s[u] += dot8(q[u], c + 8 * (k + u * kMvThreads));
   }
-  for (; k < nv8; k += kMvThreads) s[0] += dot8(__ldcs(ir + k), c + 8 * k);
+  for (; k < nv8; k += kMvThreads) s[0] += dot8(ldg_hint(ir + k, keep), c + 8 * k);
   if (threadIdx.x < tail) s[1] += __half2float(inv[(size_t)row * ld + 8 * nv8 + threadIdx.x]) * c[8 * nv8 + threadIdx.x];
   float t = warp_sum((s[0] + s[1]) + (s[2] + s[3]));
   __shared__ float sw[kMvThreads / 32];

@@ -11,7 +11,8 @@
 // with grad(uprev^d)(k) = J_k^{-1} (sum_j dSv_j(k) uprev_j^d), J_k rebuilt
 // from the 8 corner coordinates.  One thread per (element, Gauss point);
 // elements and their gathered nodal values sit in shared memory; results are
-// scattered with FP64 atomics (no element colouring).  Work per element is
+// scattered with FP64 atomics (no element colouring), or, in deterministic
+// mode, one colour per launch with plain adds in a fixed order.  Work per element is
 // about 30x fewer flops than the Ae form, so the kernel is bound by the
 // gathers of Un / UnpHalf_prev and the atomic scatter, not by arithmetic.
 #include "kernels.h"
@@ -52,11 +53,16 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
   }
   for (int i = t; i < ngp; i += blockDim.x) sw[i] = (T)B->w[i];
   const int el = t / TPE, tk = t % TPE;
-  for (int e0 = blockIdx.x * EPB; e0 < a.NE; e0 += gridDim.x * EPB) {
+  // element of local slot l in this pass (-1 past the range)
+  auto elem_of = [&](int p0, int l) -> int {
+    const int pos = p0 + l;
+    return pos < a.e_end ? (a.elist ? __ldg(a.elist + pos) : pos) : -1;
+  };
+  for (int p0 = a.e_begin + blockIdx.x * EPB; p0 < a.e_end; p0 += gridDim.x * EPB) {
     __syncthreads();
     for (int idx = t; idx < EPB * 27; idx += blockDim.x) {
-      int l = idx / 27, i = idx % 27, e = e0 + l;
-      if (e < a.NE) {
+      int l = idx / 27, i = idx % 27, e = elem_of(p0, l);
+      if (e >= 0) {
         int node = __ldg(a.ltog + (size_t)e * 27 + i);
         lt[l][i] = node;
         double4 u = ldg4(a.un + node);
@@ -67,12 +73,12 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
     }
     __syncthreads();
     for (int idx = t; idx < EPB * 24; idx += blockDim.x) {
-      int l = idx / 24, r = idx % 24, e = e0 + l;
-      if (e < a.NE) X[l][r / 3][r % 3] = (T)__ldg(a.coord + 3 * (size_t)lt[l][r / 3] + r % 3);
+      int l = idx / 24, r = idx % 24, e = elem_of(p0, l);
+      if (e >= 0) X[l][r / 3][r % 3] = (T)__ldg(a.coord + 3 * (size_t)lt[l][r / 3] + r % 3);
     }
     __syncthreads();
-    const int e = e0 + el;
-    if (e < a.NE && tk < ngp) {
+    const int e = elem_of(p0, el);
+    if (e >= 0 && tk < ngp) {
       const int k = tk;
       // Jacobian of the trilinear corner map at Gauss point k
       T J[3][3];
@@ -122,7 +128,7 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
       }
     }
     __syncthreads();
-    if (e < a.NE) {
+    if (e >= 0) {
       for (int i = tk; i < 27; i += TPE) {
         T s0 = 0, s1 = 0, s2 = 0;
         for (int k = 0; k < ngp; k++) {
@@ -132,9 +138,15 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
           s2 += sv * cc[el][k][2];
         }
         double4* dst = a.r1 + lt[el][i];
-        atomicAdd(&dst->x, -(double)s0);
-        atomicAdd(&dst->y, -(double)s1);
-        atomicAdd(&dst->z, -(double)s2);
+        if (a.plain) {  // one colour per launch: no other element of it touches this node
+          dst->x -= (double)s0;
+          dst->y -= (double)s1;
+          dst->z -= (double)s2;
+        } else {
+          atomicAdd(&dst->x, -(double)s0);
+          atomicAdd(&dst->y, -(double)s1);
+          atomicAdd(&dst->z, -(double)s2);
+        }
       }
     }
   }
@@ -144,14 +156,16 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
 
 template <class T>
 cudaError_t launch_convect(const ConvArgs<T>& a, int num_sms, cudaStream_t s) {
+  const int ne = a.e_end - a.e_begin;
+  if (ne <= 0) return cudaSuccess;
   if (a.ngp <= 8) {
     constexpr int EPB = kConvThreads / 8;
-    int grid = (a.NE + EPB - 1) / EPB;
+    int grid = (ne + EPB - 1) / EPB;
     if (grid > num_sms * 12) grid = num_sms * 12;
     k_convect<T, 8><<<grid, kConvThreads, 0, s>>>(a);
   } else {
     constexpr int EPB = kConvThreads / 32;
-    int grid = (a.NE + EPB - 1) / EPB;
+    int grid = (ne + EPB - 1) / EPB;
     if (grid > num_sms * 12) grid = num_sms * 12;
     k_convect<T, 32><<<grid, kConvThreads, 0, s>>>(a);
   }

@@ -30,7 +30,13 @@ namespace cfd {
 namespace {
 
 constexpr int kFcgThreads = 256;
-constexpr int kFcgParts = 2 + 2 * kFcgMaxM;  // partial sums per block
+// partial sums per block of an SpMV kernel instantiated for at most MD
+// stored directions: (z,w), (z,r), (z,q_j), (p_j,r)
+template <int MD>
+__host__ __device__ constexpr int fcg_parts() {
+  return 2 + 2 * MD;
+}
+constexpr int kFcgParts = fcg_parts<kFcgMaxM>();
 
 template <class VT>
 __device__ __forceinline__ VT sell_row(const int* __restrict__ off, const int* __restrict__ col,
@@ -77,29 +83,32 @@ __device__ __forceinline__ void gather_partials(const double* part, int nblk, do
 
 // Per-row part of the SpMV kernels: w[i] and the dot products of the
 // iteration (z,w) (z,r) (z,q_j) (p_j,r), accumulated into v.
-template <class VT>
-__device__ __forceinline__ void fcg_row_dots(const FcgArgs<VT>& a, int i, VT wi, int nd, double (&v)[kFcgParts]) {
+template <int MD, class VT>
+__device__ __forceinline__ void fcg_row_dots(const FcgArgs<VT>& a, int i, VT wi, int nd,
+                                             double (&v)[fcg_parts<MD>()]) {
   const size_t n = (size_t)a.n;
   a.w[i] = wi;
   const double zi = a.z[i], ri = a.r[i];
   v[0] += zi * (double)wi;
   v[1] += zi * ri;
 #pragma unroll
-  for (int j = 0; j < kFcgMaxM; j++) {
+  for (int j = 0; j < MD; j++) {
     if (j < nd) {
       v[2 + j] += zi * (double)a.q[j * n + i];
-      v[2 + kFcgMaxM + j] += (double)a.p[j * n + i] * ri;
+      v[2 + MD + j] += (double)a.p[j * n + i] * ri;
     }
   }
 }
 
 // Block sums of the SpMV's partials; the last block to finish forms the
 // coefficients beta_j, (p,q) and alpha of the iteration.
-template <class VT>
-__device__ __forceinline__ void fcg_spmv_finish(const FcgArgs<VT>& a, double (&v)[kFcgParts], int nd, int m, int it) {
-  block_sum<kFcgParts>(v);
-  if (!post_partials<kFcgParts>(v, a.st.part, a.st.cnt)) return;
-  gather_partials<kFcgParts>(a.st.part, gridDim.x, v);
+template <int MD, class VT>
+__device__ __forceinline__ void fcg_spmv_finish(const FcgArgs<VT>& a, double (&v)[fcg_parts<MD>()], int nd, int m,
+                                                int it) {
+  constexpr int NV = fcg_parts<MD>();
+  block_sum<NV>(v);
+  if (!post_partials<NV>(v, a.st.part, a.st.cnt)) return;
+  gather_partials<NV>(a.st.part, gridDim.x, v);
   if (threadIdx.x == 0) {
     double* s = a.st.sc;
     if (ld_volatile_i32(a.st.err)) {
@@ -112,10 +121,10 @@ __device__ __forceinline__ void fcg_spmv_finish(const FcgArgs<VT>& a, double (&v
 #pragma unroll
     for (int j = 0; j < kFcgMaxM; j++) {
       beta[j] = 0.0;
-      if (j < nd) {
+      if (j < MD && j < nd) {
         beta[j] = v[2 + j] / s[kFcgPQ0 + j];
         pq -= beta[j] * v[2 + j];
-        pr -= beta[j] * v[2 + kFcgMaxM + j];
+        pr -= beta[j] * v[2 + MD + j];
       }
     }
     const double alpha = pr / pq;
@@ -184,7 +193,7 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_start(FcgArgs<VT> a, int wa
 // w = Z z with the matrix streamed through shared memory (ChunkStream, as in
 // the persistent PCG): 16 warps per block, each owning a contiguous range of
 // 32-row slices, lane = row.
-template <class VT>
+template <class VT, int MD>
 __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
   if (*a.st.done) return;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -215,9 +224,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
   mbar_init_fence();
   __syncwarp();
   st.start(lane);
-  double v[kFcgParts];
+  double v[fcg_parts<MD>()];
 #pragma unroll
-  for (int k = 0; k < kFcgParts; k++) v[k] = 0.0;
+  for (int k = 0; k < fcg_parts<MD>(); k++) v[k] = 0.0;
   for (int sl = st.s_begin; sl < st.s_end; sl++) {
     VT acc = 0;
     const int wd = (__ldg(a.off + sl + 1) - __ldg(a.off + sl)) >> 5;
@@ -226,10 +235,10 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
       st.release(lane);
     }
     const int i = sl * 32 + lane;
-    if (i < a.n) fcg_row_dots(a, i, acc, nd, v);
+    if (i < a.n) fcg_row_dots<MD>(a, i, acc, nd, v);
   }
   if (!st.failed) st.drain(a.st.timeout_ns);
-  fcg_spmv_finish(a, v, nd, m, it);
+  fcg_spmv_finish<MD>(a, v, nd, m, it);
 }
 
 // w = Z z on a structured grid of pressure nodes (identity numbering, node
@@ -240,7 +249,10 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
 // contiguous across the warp.  Each warp owns a contiguous range of slices
 // and streams it through shared memory in chunks of 25 taps (one dz plane,
 // 3.2 KB), two chunks in flight per warp on bulk asynchronous copies.  Taps
-// that leave the grid have zero coefficients; their index is clamped.
+// that leave the grid have zero coefficients.  Slices whose every tap stays
+// inside [0, n) read z at i + dx + fx dy + fxy dz directly (five row
+// pointers per plane, dx folded into the load offsets); the few slices
+// within two planes of either end clamp the index.
 constexpr int kStTaps = 25;
 constexpr int kStBuf = 2;
 template <class VT>
@@ -248,7 +260,30 @@ constexpr size_t stencil_smem_bytes() {
   return (size_t)kPcgWarps * kStBuf * (kStTaps * 32 * sizeof(VT) + sizeof(unsigned long long));
 }
 
-template <class VT>
+// One dz plane of a row (25 taps, coefficients q[t * 32] in shared memory)
+// into the five per-dy accumulators.
+template <bool CLAMP, class VT>
+__device__ __forceinline__ void stencil_plane(const VT* q, const VT* __restrict__ z, int base, int fx, int n,
+                                              VT (&acc)[5]) {
+#pragma unroll
+  for (int dy = -2; dy <= 2; dy++) {
+    const int rb = base + fx * dy;
+#pragma unroll
+    for (int dx = -2; dx <= 2; dx++) {
+      VT zv;
+      if constexpr (CLAMP) {
+        int j = rb + dx;
+        j = j < 0 ? 0 : (j >= n ? n - 1 : j);
+        zv = __ldg(z + j);
+      } else {
+        zv = __ldg(z + rb + dx);
+      }
+      acc[dy + 2] += q[((dy + 2) * 5 + dx + 2) * 32] * zv;
+    }
+  }
+}
+
+template <class VT, int MD>
 __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT> a) {
   if (*a.st.done) return;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -269,26 +304,31 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT>
     for (int b = 0; b < kStBuf; b++) mbar_init(mbar + b, 1);
   mbar_init_fence();
   __syncwarp();
+  // the coefficients are read once per iteration: evict-first in L2, so the
+  // vectors and the coarse inverse stay
+  const unsigned long long once = l2_evict_first();
   auto issue = [&](int k) {  // chunk k of the warp's range into buffer k % kStBuf
     if (lane == 0 && k < total) {
       const int b = k % kStBuf;
       const VT* src = a.stencil + ((size_t)(s0 + k / 5) * 125 + (k % 5) * kStTaps) * 32;
       fence_proxy_async_smem();
       mbar_expect_tx(mbar + b, kChunkBytes);
-      bulk_g2s(buf + (size_t)b * kStTaps * 32, src, kChunkBytes, mbar + b);
+      bulk_g2s_hint(buf + (size_t)b * kStTaps * 32, src, kChunkBytes, mbar + b, once);
     }
   };
   for (int k = 0; k < kStBuf; k++) issue(k);
   bool ok = true;
   int kfail = 0;
   const VT* __restrict__ z = a.z;
-  double v[kFcgParts];
+  const int reach = 2 + 2 * fx + 2 * fxy;  // largest |j - i| of a tap
+  double v[fcg_parts<MD>()];
 #pragma unroll
-  for (int k = 0; k < kFcgParts; k++) v[k] = 0.0;
+  for (int k = 0; k < fcg_parts<MD>(); k++) v[k] = 0.0;
   int k = 0;
   for (int sl = s0; sl < s1; sl++) {
     const int i = sl * 32 + lane;
-    VT acc = 0;
+    const bool inside = sl * 32 >= reach && sl * 32 + 31 + reach < n;  // warp-uniform
+    VT acc[5] = {0, 0, 0, 0, 0};
     for (int dz = -2; dz <= 2; dz++, k++) {
       const int b = k % kStBuf;
       if (ok && !mbar_wait_bounded(mbar + b, (unsigned)((k / kStBuf) & 1), a.st.timeout_ns)) {
@@ -298,18 +338,15 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT>
       }
       if (ok) {
         const VT* q = buf + (size_t)b * kStTaps * 32 + lane;
-#pragma unroll
-        for (int t = 0; t < kStTaps; t++) {
-          const int dy = t / 5 - 2, dx = t % 5 - 2;
-          int j = i + dx + fx * dy + fxy * dz;
-          j = j < 0 ? 0 : (j >= n ? n - 1 : j);
-          acc += q[t * 32] * __ldg(z + j);
-        }
+        if (inside)
+          stencil_plane<false>(q, z, i + fxy * dz, fx, n, acc);
+        else
+          stencil_plane<true>(q, z, i + fxy * dz, fx, n, acc);
       }
       __syncwarp();
       if (ok) issue(k + kStBuf);
     }
-    if (i < n) fcg_row_dots(a, i, acc, nd, v);
+    if (i < n) fcg_row_dots<MD>(a, i, ((acc[0] + acc[1]) + (acc[2] + acc[3])) + acc[4], nd, v);
   }
   if (!ok && lane == 0) {
     // a bounded wait gave up: give the copies still in flight one more
@@ -317,7 +354,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT>
     for (int kk = kfail; kk < kfail + kStBuf && kk < total; kk++)
       mbar_wait_bounded(mbar + kk % kStBuf, (unsigned)((kk / kStBuf) & 1), a.st.timeout_ns);
   }
-  fcg_spmv_finish(a, v, nd, m, it);
+  fcg_spmv_finish<MD>(a, v, nd, m, it);
 }
 
 template <class VT>
@@ -412,22 +449,32 @@ cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <class VT>
-cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s) {
-  if (a.spmv_grid < 1 || a.spmv_grid > kFcgMaxBlocks) return cudaErrorInvalidValue;
+template <class VT, int MD>
+cudaError_t launch_fcg_spmv_md(const FcgArgs<VT>& a, cudaStream_t s) {
   if (a.stencil) {  // one wave of two blocks of 16 warps per SM
     const size_t smem = stencil_smem_bytes<VT>();
-    cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv_stencil<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv_stencil<VT, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    k_fcg_spmv_stencil<VT><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
+    k_fcg_spmv_stencil<VT, MD><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
     return cudaGetLastError();
   }
   const size_t smem = pcg_smem_bytes<VT>();
-  cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv<VT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv<VT, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_fcg_spmv<VT><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
+  k_fcg_spmv<VT, MD><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
   return cudaGetLastError();
+}
+
+// the SpMV's dot partials are sized for the solve's window m: 1 (CG with a
+// fixed preconditioner), up to 4, up to kFcgMaxM
+template <class VT>
+cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s) {
+  if (a.spmv_grid < 1 || a.spmv_grid > kFcgMaxBlocks) return cudaErrorInvalidValue;
+  if (a.st.m < 1 || a.st.m > kFcgMaxM) return cudaErrorInvalidValue;
+  if (a.st.m == 1) return launch_fcg_spmv_md<VT, 1>(a, s);
+  if (a.st.m <= 4) return launch_fcg_spmv_md<VT, 4>(a, s);
+  return launch_fcg_spmv_md<VT, kFcgMaxM>(a, s);
 }
 
 template <class VT>

@@ -31,6 +31,11 @@ struct AsmArgs {
   const int *g_rp, *g_col;
   double *g1, *g2, *g3;
   double* msum;  // NN: row sums of M
+  // element range [e_begin, e_end) of the list elist (null: ids themselves);
+  // plain = 1: the range is one colour (no two elements share a node), so
+  // the scatter adds without atomics and the sums are bitwise reproducible
+  const int* elist;
+  int e_begin, e_end, plain;
 };
 cudaError_t launch_assemble(const AsmArgs& a, int num_sms, cudaStream_t s);
 
@@ -65,6 +70,8 @@ struct ConvArgs {
   const double4* un;     // convecting velocity (time level n)
   const double4* uprev;  // UnpHalf_prev
   double4* r1;           // accumulates -A(un) uprev (zeroed by the caller)
+  const int* elist;      // element range and plain scatter as in AsmArgs
+  int e_begin, e_end, plain;
 };
 template <class T>
 cudaError_t launch_convect(const ConvArgs<T>& a, int num_sms, cudaStream_t s);

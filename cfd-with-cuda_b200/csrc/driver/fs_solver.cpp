@@ -7,7 +7,7 @@
 //
 // Solver options (not part of the deck, so the deck stays unchanged):
 //   CFD_PRECISION=fp64|mixed  CFD_CG_RTOL=<x>  CFD_CG_WARM=0|1
-//   CFD_NGP=8|27  CFD_DEVICE=<n>  CFD_MAXSTEPS=<n>
+//   CFD_NGP=8|27  CFD_DEVICE=<n>  CFD_MAXSTEPS=<n>  CFD_DETERMINISTIC=0|1
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -57,6 +57,7 @@ int main(int argc, char** argv) {
   if (const char* p = std::getenv("CFD_CG_WARM")) o.cg_warm = std::atoi(p);
   if (const char* p = std::getenv("CFD_NGP")) o.ngp_override = std::atoi(p);
   if (const char* p = std::getenv("CFD_PRECOND")) o.precond = std::strcmp(p, "twolevel") == 0 ? CFD_PC_TWOLEVEL : CFD_PC_JACOBI;
+  if (const char* p = std::getenv("CFD_DETERMINISTIC")) o.deterministic = std::atoi(p) != 0;
   long maxsteps = -1;
   if (const char* p = std::getenv("CFD_MAXSTEPS")) maxsteps = std::atol(p);
   check(c, cfd_set_options(c, &o), "cfd_set_options");

@@ -80,6 +80,15 @@ int cfdh_get_pattern(const cfd_host* h, int which, int* rowptr, int* col) {
   return CFD_OK;
 }
 
+int cfdh_element_colors(const cfd_host* h, int* order, int* off) {
+  if (!h) return CFD_E_BADARG;
+  std::vector<int> o, f;
+  if (cfd::color_elements(h->P, o, f)) return -1;
+  if (order) std::copy(o.begin(), o.end(), order);
+  if (off) std::copy(f.begin(), f.end(), off);
+  return (int)f.size() - 1;
+}
+
 int cfdh_write_tecplot(const cfd_host* h, const double* U, const double* Pv, const char* path, const char* title) {
   if (!h || !U || !Pv || !path) return CFD_E_BADARG;
   return cfd::write_tecplot(h->P, U, Pv, path, title ? title : "");

@@ -541,4 +541,28 @@ int preprocess(HostProblem& P, std::string& err) {
   return CFD_OK;
 }
 
+int color_elements(const HostProblem& P, std::vector<int>& order, std::vector<int>& off) {
+  const int NE = P.NE;
+  std::vector<uint64_t> used((size_t)P.NCN, 0);  // colours of the elements touching each corner node
+  std::vector<int> color(NE);
+  int ncol = 0;
+  for (int e = 0; e < NE; e++) {
+    uint64_t m = 0;
+    for (int c = 0; c < 8; c++) m |= used[P.ltog[(size_t)e * 27 + c]];
+    if (~m == 0) return -1;
+    int k = 0;
+    while (m & (1ull << k)) k++;
+    color[e] = k;
+    ncol = std::max(ncol, k + 1);
+    for (int c = 0; c < 8; c++) used[P.ltog[(size_t)e * 27 + c]] |= 1ull << k;
+  }
+  off.assign(ncol + 1, 0);
+  for (int e = 0; e < NE; e++) off[color[e] + 1]++;
+  for (int c = 0; c < ncol; c++) off[c + 1] += off[c];
+  order.assign(NE, 0);
+  std::vector<int> pos(off.begin(), off.end() - 1);
+  for (int e = 0; e < NE; e++) order[pos[color[e]]++] = e;
+  return 0;
+}
+
 }  // namespace cfd

@@ -54,6 +54,14 @@ int read_inp(const std::string& path, HostProblem& P, std::string& err);
 // Fills NN, coord, ltog (mid nodes), bcnode/bcid, monPoint and all patterns.
 int preprocess(HostProblem& P, std::string& err);
 
+// Conflict-free greedy colouring of the elements over their corner nodes
+// (elements that share a node get different colours): order lists the
+// elements colour by colour (ascending element id inside a colour), colour c
+// owns order[off[c] .. off[c+1]).  The reference colours elements for the
+// same purpose, serialising its scatters (setupMeshColoring,
+// blascoCodinaHuerta.cpp:853-947).  Returns 0, or -1 beyond 64 colours.
+int color_elements(const HostProblem& P, std::vector<int>& order, std::vector<int>& off);
+
 // Edge corner pairs, face corner quads and face mid-node lists of a hex27
 // element (blascoCodinaHuerta.cpp:1005-1054, 1143-1180, 1485-1528).
 extern const int kEdge[12][2];

@@ -74,6 +74,12 @@ typedef struct {
                         the first fcg_net_iters iterations of each pressure
                         solve (of its first inner solve in CFD_MIXED), the
                         two-level part alone after them (0 = every iteration) */
+  int deterministic; /* 1: element assembly and convection run one element
+                        colour per launch (no two elements of a colour share
+                        a node) with plain adds instead of FP64 atomics, so
+                        repeated runs are bitwise identical, as the
+                        reference's coloured assembly (CUDAcodes.cu:915-936);
+                        0 (default): one launch over all elements, atomics */
 } cfd_options;
 
 typedef struct {
@@ -346,6 +352,12 @@ int cfdh_get_bcnodes(const cfd_host* h, int* out);  /* nBCnodes x 2 (node, bc) *
  * (at most 6000).  Host only; no counterpart in the reference. */
 int cfdh_coarse_inverse(const int dims[3], const int* rowptr, const int* col, const double* val, int* cd,
                         double* inv);
+/* Element colouring of the deterministic mode (setupMeshColoring,
+ * blascoCodinaHuerta.cpp:853-947): returns the number of colours C (or -1
+ * beyond 64); order (NE, may be NULL) lists the elements colour by colour,
+ * colour c owning order[off[c] .. off[c+1]) (off: C + 1 ints, may be NULL;
+ * call once with NULLs to learn C). */
+int cfdh_element_colors(const cfd_host* h, int* order, int* off);
 /* which: 0 K (NN x NN), 1 G (NN x NNp), 2 G^T (NNp x NN), 3 Z (NNp x NNp) */
 int cfdh_get_pattern(const cfd_host* h, int which, int* rowptr, int* col);
 /* createTecplot layout (blascoCodinaHuerta.cpp:4249-4482) for given state. */

@@ -205,3 +205,48 @@ def test_failures_are_reported_not_hung(decks):
         s.step2GPU(1)
     assert ei.value.code == cfdfs.CFD_E_NONFINITE
     s.close()
+
+
+def _det_run(path, steps, **kw):
+    import cfdfs
+    s = cfdfs.Solver(device=0, deterministic=1, **kw)
+    s.load(path)
+    s.step0()
+    ops = [s.matrix(w)[2].copy() for w in ("K", "G", "Z")]
+    st = s.run(steps)
+    U, P = s.state()
+    s.close()
+    return ops, st, U, P
+
+
+@pytest.mark.parametrize("key", ["c1", "c1_27", "perturbed"])
+def test_deterministic_mode(decks, oracle_mod, key):
+    """Coloured assembly and convection without atomics: the oracle's
+    operators and run to the usual tolerances, and two runs in separate
+    contexts bitwise identical (operators, velocity and pressure)."""
+    o = oracle_mod.Oracle(decks[key])
+    o.step0()
+    info_o = o.run(-1)
+    steps = info_o["steps"]
+    ops1, st1, U1, P1 = _det_run(decks[key], steps)
+    ops2, st2, U2, P2 = _det_run(decks[key], steps)
+    assert rel_l2(ops1[0], o.values("K")) < OP_TOL
+    assert rel_l2(ops1[2], o.values("Z")) < OP_TOL
+    assert st1.steps == steps
+    assert rel_l2(U1, o.vec("Un")) < RUN_TOL and rel_l2(P1, o.vec("Pn")) < RUN_TOL
+    for a, b in zip(ops1, ops2):
+        assert np.array_equal(a, b)
+    assert np.array_equal(U1, U2) and np.array_equal(P1, P2)
+    assert st1.cg_iters == st2.cg_iters
+    o.close()
+
+
+def test_deterministic_mixed_twolevel(decks):
+    """The mixed two-level path is bitwise reproducible in deterministic mode
+    (its Krylov reductions are fixed-order block sums already)."""
+    import cfdfs
+    kw = dict(precision=cfdfs.MIXED, precond=cfdfs.PC_TWOLEVEL)
+    _, st1, U1, P1 = _det_run(decks["c1"], 6, **kw)
+    _, st2, U2, P2 = _det_run(decks["c1"], 6, **kw)
+    assert np.array_equal(U1, U2) and np.array_equal(P1, P2)
+    assert st1.cg_iters == st2.cg_iters

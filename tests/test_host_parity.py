@@ -62,3 +62,25 @@ def test_bad_decks_rejected(tmp_path, decks):
             HostMesh(str(p))
     with pytest.raises(CfdError):
         HostMesh(str(tmp_path / "missing.inp"))
+
+
+@pytest.mark.parametrize("key", ["c1", "graded", "perturbed", "duct_small"])
+def test_element_colouring_conflict_free(decks, key):
+    """The deterministic mode's colouring (one colour per launch, plain adds):
+    every element exactly once, and no two elements of a colour share any of
+    their 27 nodes (corners, edge and face mid-nodes, centre)."""
+    from cfdfs import HostMesh
+    h = HostMesh(decks[key])
+    order, off = h.element_colors()
+    assert np.array_equal(np.sort(order), np.arange(h.NE))
+    assert off[0] == 0 and off[-1] == h.NE and np.all(np.diff(off) > 0)
+    ltog = h.ltog()
+    for c in range(len(off) - 1):
+        els = order[off[c]:off[c + 1]]
+        assert np.all(np.diff(els) > 0)  # ascending inside a colour: a fixed order
+        nodes = ltog[els].ravel()
+        assert len(np.unique(nodes)) == len(nodes), f"colour {c} shares a node"
+    # a structured hex mesh needs the 8 colours of the parity classes
+    if key in ("c1", "graded", "perturbed"):
+        assert len(off) - 1 == 8
+    h.close()
