@@ -19,10 +19,14 @@
 // reads phase (d != 0) at coarse index X + (d == -1 ? -1 : 0), again a
 // constant row shift inside that phase's planes (low-side halo only).
 //
-// One thread issues tcgen05.mma (M = 128 rows, N = output channels of the
-// slice, K = 16 input channels) into a 128-column TMEM accumulator; the four
-// warps read it back with tcgen05.ld (warp w owns rows 32w..32w+31), add the
-// bias, apply the activation and store BF16 (or FP32) channels-last.
+// Lane 0 of every warp issues tcgen05.mma (M = 128 rows, N = output
+// channels of the slice, K = 16 input channels) for its share of the CTA's
+// tiles -- or, when a group has fewer tiles than warps, for its share of a
+// tile's taps into its own TMEM accumulator (split K) -- and commits to its
+// own mbarrier, so the per-instruction issue cost is spread over four
+// issuers.  The warps read the accumulators back with tcgen05.ld (warp w
+// owns rows 32w..32w+31), sum the split-K partials, add the bias, apply the
+// activation and store BF16 (or FP32) channels-last.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
