@@ -32,7 +32,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "cfd-with-cuda_b200"))
 
 METRIC = "steps/s at 64³ cavity: mixed+learned-precond vs plain FP64 CG, rel err≤1e-6"
-WORKLOAD = "lid-driven cavity 64x64x64 hex27/hex8 (129^3 velocity, 65^3 pressure nodes), Re=1000, dt=0.002"
+def workload(n):
+    return (f"lid-driven cavity {n}x{n}x{n} hex27/hex8 ({2 * n + 1}^3 velocity, {n + 1}^3 pressure nodes), "
+            "Re=1000, dt=0.002")
 N_ELEM, RE, DT, T_STEPS = 64, 1000.0, 0.002, 100
 WEIGHTS = os.path.join(ROOT, "cfd-with-cuda_b200", "weights", "unet_cavity.bin")
 
@@ -352,7 +354,7 @@ def run_ours(args, rank, world, local_rank):
             "vs_baseline": None,
             "dtype": ("f32+f64" if precision == cfdfs.MIXED else "f64") + ("+bf16" if learned else ""),
             "data": "synthetic: generated structured cavity deck (no dataset); fluid starts at rest",
-            "config": {"workload": WORKLOAD, "elements": args.n ** 3, "precision": args.precision,
+            "config": {"workload": workload(args.n), "elements": args.n ** 3, "precision": args.precision,
                        "precond": {"learned": "Jacobi + coarse space + learned U-Net correction in flexible CG "
                                    f"(network in the first {args.net_iters or 'every'} iteration(s) of each solve; "
                                    "Jacobi-PCG fallback)",
@@ -430,7 +432,7 @@ def run_reference(args, rank, world):
     return {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": "steps/s", "n_gpus": world,
             "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": round(1000 * el / steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: generated structured cavity deck", "config": {"workload": WORKLOAD,
+            "data": "synthetic: generated structured cavity deck", "config": {"workload": workload(args.n),
                                                                             "precision": "fp64", "ngp": 8},
             "cpu_baseline": {"value": round(v, 5), "unit": "steps/s", "cores": cores, "kind": "port",
                              "sample": f"{steps} time steps (capped by a {args.cpu_budget:.0f} s budget) of the "

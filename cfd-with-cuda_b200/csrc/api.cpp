@@ -131,6 +131,11 @@ struct cfd_ctx {
   DevBuf<float> ks_val32, gs1_32, gs2_32, gs3_32, gts1_32, gts2_32, gts3_32, zs_val32, zdinv32;
   // velocity-sized state, double4 per node
   DevBuf<double4> vbuf[12];
+  // CFD_MIXED: float4 copies of the gathered velocity vectors (Un,
+  // UnpHalf_prev, UnpHalf, Acc_prev, Acc, d)
+  DevBuf<float4> fbuf[6];
+  float4 *un32 = nullptr, *uphp32 = nullptr, *uph32 = nullptr, *accp32 = nullptr, *acc32 = nullptr,
+         *d32 = nullptr;
   double4 *un = nullptr, *unp1 = nullptr, *unp1_prev = nullptr, *unphalf = nullptr, *unphalf_prev = nullptr,
           *acc = nullptr, *acc_prev = nullptr, *kacc = nullptr, *r1conv = nullptr, *dvec = nullptr, *r1dbg = nullptr,
           *r3dbg = nullptr;
@@ -378,6 +383,14 @@ int upload_problem(cfd_ctx* c) {
   c->un = c->vbuf[0].p; c->unp1 = c->vbuf[1].p; c->unp1_prev = c->vbuf[2].p; c->unphalf = c->vbuf[3].p;
   c->unphalf_prev = c->vbuf[4].p; c->acc = c->vbuf[5].p; c->acc_prev = c->vbuf[6].p; c->kacc = c->vbuf[7].p;
   c->r1conv = c->vbuf[8].p; c->dvec = c->vbuf[9].p; c->r1dbg = c->vbuf[10].p; c->r3dbg = c->vbuf[11].p;
+  if (mixed(c)) {
+    for (auto& b : c->fbuf) {
+      CU(b.alloc(NN));
+      CU(cudaMemsetAsync(b.p, 0, b.bytes(), s));
+    }
+    c->un32 = c->fbuf[0].p; c->uphp32 = c->fbuf[1].p; c->uph32 = c->fbuf[2].p;
+    c->accp32 = c->fbuf[3].p; c->acc32 = c->fbuf[4].p; c->d32 = c->fbuf[5].p;
+  }
   for (auto& b : c->pbuf) {
     CU(b.alloc(NNp));
     CU(cudaMemsetAsync(b.p, 0, b.bytes(), s));
@@ -1183,6 +1196,10 @@ int cfd_begin_step(cfd_ctx* c) {
   CU(cudaMemcpyAsync(c->unphalf_prev, c->un, NN * sizeof(double4), cudaMemcpyDeviceToDevice, s));
   CU(cudaMemcpyAsync(c->pnp1_prev, c->pn, NNp * sizeof(double), cudaMemcpyDeviceToDevice, s));
   CU(cudaMemsetAsync(c->acc_prev, 0, NN * sizeof(double4), s));
+  if (mixed(c)) {  // the gathered FP32 copies of the same vectors
+    KL(CFD_K_OTHER, launch_vec4_to_f32((int)NN, c->un, c->un32, c->uphp32, s));
+    CU(cudaMemsetAsync(c->accp32, 0, NN * sizeof(float4), s));
+  }
   return CFD_OK;
 }
 
@@ -1210,7 +1227,7 @@ int cfd_convect(cfd_ctx* c) {
     return CFD_OK;
   };
   if (mixed(c)) {
-    ConvArgs<float> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
+    ConvArgs<float> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un32, c->uphp32, c->r1conv};
     return run(a, [&](const ConvArgs<float>& x) { return launch_convect<float>(x, c->num_sms, s); });
   }
   ConvArgs<double> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
@@ -1224,18 +1241,20 @@ int cfd_step1(cfd_ctx* c, int iter) {
   auto fill = [&](auto& a) {
     a.NN = c->P.NN; a.iter = iter; a.dt = c->P.dt;
     a.k_off = c->ks_off.p; a.k_col = c->ks_col.p; a.g_off = c->gs_off.p; a.g_col = c->gs_col.p;
-    a.uprev = c->unphalf_prev; a.un = c->un; a.r1conv = c->r1conv; a.kacc = c->kacc;
+    a.un = c->un; a.r1conv = c->r1conv; a.kacc = c->kacc;
     a.pn = c->pn; a.minv_free = c->minv_free.p; a.minv_orig = c->minv_orig.p;
     a.unphalf = c->unphalf; a.d = c->dvec; a.r1out = c->r_debug ? c->r1dbg : nullptr;
   };
   if (mixed(c)) {
     Step1Args<float> a{};
     fill(a);
+    a.uprev = c->uphp32; a.unphalf_g = c->uph32; a.d_g = c->d32;
     a.kval = c->ks_val32.p; a.g1 = c->gs1_32.p; a.g2 = c->gs2_32.p; a.g3 = c->gs3_32.p;
     KL(CFD_K_STEP1, launch_step1<float>(a, c->num_sms, s));
   } else {
     Step1Args<double> a{};
     fill(a);
+    a.uprev = c->unphalf_prev;
     a.kval = c->ks_val.p; a.g1 = c->gs1.p; a.g2 = c->gs2.p; a.g3 = c->gs3.p;
     KL(CFD_K_STEP1, launch_step1<double>(a, c->num_sms, s));
   }
@@ -1248,7 +1267,7 @@ int cfd_step2(cfd_ctx* c, int iter, cfd_solve_stats* st) {
   cudaStream_t s = c->stream;
   const int pin = c->P.zeroP;
   if (mixed(c)) {
-    GtArgs<float> a{c->P.NNp, pin, c->gts_off.p, c->gts_col.p, c->gts1_32.p, c->gts2_32.p, c->gts3_32.p, c->dvec, c->r2};
+    GtArgs<float> a{c->P.NNp, pin, c->gts_off.p, c->gts_col.p, c->gts1_32.p, c->gts2_32.p, c->gts3_32.p, c->d32, c->r2};
     KL(CFD_K_GT, launch_gt<float>(a, c->num_sms, s));
   } else {
     GtArgs<double> a{c->P.NNp, pin, c->gts_off.p, c->gts_col.p, c->gts1.p, c->gts2.p, c->gts3.p, c->dvec, c->r2};
@@ -1273,6 +1292,7 @@ int cfd_step3(cfd_ctx* c, int iter) {
   if (mixed(c)) {
     Step3Args<float> a{};
     fill(a);
+    a.acc_g = c->acc32;
     a.g1 = c->gs1_32.p; a.g2 = c->gs2_32.p; a.g3 = c->gs3_32.p;
     KL(CFD_K_STEP3, launch_step3<float>(a, s));
   } else {
@@ -1305,6 +1325,8 @@ int cfd_rotate(cfd_ctx* c) {
   std::swap(c->unp1_prev, c->unp1);
   std::swap(c->acc_prev, c->acc);
   std::swap(c->pnp1_prev, c->pnp1);
+  std::swap(c->uphp32, c->uph32);
+  std::swap(c->accp32, c->acc32);
   return CFD_OK;
 }
 
@@ -1313,7 +1335,7 @@ int cfd_k_times_acc(cfd_ctx* c) {
   NEED(c->assembled, "cfd_k_times_acc before cfd_step0");
   cudaStream_t s = c->stream;
   if (mixed(c)) {
-    SpmvK3Args<float> a{c->P.NN, c->ks_off.p, c->ks_col.p, c->ks_val32.p, c->acc_prev, c->kacc};
+    SpmvK3Args<float> a{c->P.NN, c->ks_off.p, c->ks_col.p, c->ks_val32.p, c->accp32, c->kacc};
     KL(CFD_K_SPMV_K3, launch_spmv_k3<float>(a, c->num_sms, s));
   } else {
     SpmvK3Args<double> a{c->P.NN, c->ks_off.p, c->ks_col.p, c->ks_val.p, c->acc_prev, c->kacc};

@@ -126,6 +126,14 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
+// Read-only load of a gathered velocity value: the float4 copy or the double4
+// state.
+__device__ __forceinline__ float4 ldgv(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ double4 ldgv(const double4* p) { return ldg4(p); }
+__device__ __forceinline__ float4 to_f4(const double4& v) {
+  return make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+}
+
 // ---- bulk asynchronous copies (global -> shared) completed on an mbarrier ----
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));

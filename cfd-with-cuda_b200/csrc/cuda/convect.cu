@@ -65,8 +65,8 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
       if (e >= 0) {
         int node = __ldg(a.ltog + (size_t)e * 27 + i);
         lt[l][i] = node;
-        double4 u = ldg4(a.un + node);
-        double4 p = ldg4(a.uprev + node);
+        const auto u = ldgv(a.un + node);
+        const auto p = ldgv(a.uprev + node);
         u0[l][i][0] = (T)u.x; u0[l][i][1] = (T)u.y; u0[l][i][2] = (T)u.z;
         up[l][i][0] = (T)p.x; up[l][i][1] = (T)p.y; up[l][i][2] = (T)p.z;
       }

@@ -12,6 +12,12 @@
 //                           one thread owns one row and a warp-wide load of
 //                           entry j is one contiguous 128/256-byte segment.
 //                           Padding entries hold value 0 and a valid column.
+//   gathered copies         CFD_MIXED keeps float4 copies (x, y, z, 0) of the
+//                           velocity vectors that SpMVs and the convection
+//                           gather (Un, UnpHalf_prev, Acc_prev, d): those
+//                           kernels round every gathered value to FP32, so
+//                           the copies give identical results at half the
+//                           L1/L2 traffic of the 32-byte double4 gathers
 #pragma once
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -19,6 +25,19 @@
 #include "common.cuh"
 
 namespace cfd {
+
+// Type of a gathered velocity vector: the float4 copy for FP32 operator
+// values, the FP64 state itself otherwise.
+template <class VT>
+struct GatherVec {
+  using type = double4;
+};
+template <>
+struct GatherVec<float> {
+  using type = float4;
+};
+template <class VT>
+using GVec = typename GatherVec<VT>::type;
 
 struct AsmArgs {
   int NE, ngp;
@@ -67,8 +86,8 @@ struct ConvArgs {
   const int* ltog;
   const double* coord;
   const Basis* basis;
-  const double4* un;     // convecting velocity (time level n)
-  const double4* uprev;  // UnpHalf_prev
+  const GVec<T>* un;     // convecting velocity (time level n)
+  const GVec<T>* uprev;  // UnpHalf_prev
   double4* r1;           // accumulates -A(un) uprev (zeroed by the caller)
   const int* elist;      // element range and plain scatter as in AsmArgs
   int e_begin, e_end, plain;
@@ -84,9 +103,12 @@ struct Step1Args {
   const VT* kval;
   const int *g_off, *g_col;  // SELL-32
   const VT *g1, *g2, *g3;
-  const double4 *uprev, *un, *r1conv, *kacc;
+  const GVec<VT>* uprev;  // UnpHalf_prev, gathered by K
+  const double4 *un, *r1conv, *kacc;
   const double *pn, *minv_free, *minv_orig;
   double4 *unphalf, *d, *r1out;  // r1out may be null
+  GVec<VT>* unphalf_g;           // float4 copies of UnpHalf and d (VT = float)
+  GVec<VT>* d_g;
 };
 template <class VT>
 cudaError_t launch_step1(const Step1Args<VT>& a, int num_sms, cudaStream_t s);
@@ -96,7 +118,7 @@ struct GtArgs {
   int NNp, pin;  // pin: row forced to 0 (< 1 disables, as the reference's node > 0 test)
   const int *gt_off, *gt_col;  // SELL-32
   const VT *gt1, *gt2, *gt3;
-  const double4* d;
+  const GVec<VT>* d;
   double* out;
 };
 template <class VT>
@@ -114,6 +136,7 @@ struct Step3Args {
   double4 *acc, *unp1, *r3out;  // r3out may be null
   double* part;                 // 3 x nblocks partials: sum U^2, sum dU^2, max |dU|/dt
   int nblocks;
+  GVec<VT>* acc_g;  // float4 copy of Acc (VT = float)
 };
 template <class VT>
 cudaError_t launch_step3(const Step3Args<VT>& a, cudaStream_t s);
@@ -124,7 +147,7 @@ struct SpmvK3Args {
   int NN;
   const int *off, *col;  // SELL-32
   const VT* val;
-  const double4* x;
+  const GVec<VT>* x;
   double4* y;
 };
 template <class VT>
@@ -260,6 +283,8 @@ cudaError_t launch_wait_selftest(const int* flag, int* err, unsigned long long t
 
 // layout conversion between the reference's [u|v|w] blocks and double4 nodes
 cudaError_t launch_blocks_to_vec4(int NN, const double* blocks, double4* v, cudaStream_t s);
+// a = b = (float4) v
+cudaError_t launch_vec4_to_f32(int NN, const double4* v, float4* a, float4* b, cudaStream_t s);
 cudaError_t launch_vec4_to_blocks(int NN, const double4* v, double* blocks, cudaStream_t s);
 cudaError_t launch_apply_bc(int n, const int* nodes, const double* uvw, double4* u, cudaStream_t s);
 

@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kRowThreads) k_step1(Step1Args<VT> a) {
 #pragma unroll 4
     for (int j = 0; j < w; j++) {
       const VT v = __ldcs(val + 32 * j);
-      const double4 x = ldg4(a.uprev + __ldcs(col + 32 * j));
+      const auto x = ldgv(a.uprev + __ldcs(col + 32 * j));
       kx += v * (VT)x.x;
       ky += v * (VT)x.y;
       kz += v * (VT)x.z;
@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(kRowThreads) k_step1(Step1Args<VT> a) {
   h.z = u.z + a.dt * rz * mf;
   h.w = 0.0;
   a.unphalf[row] = h;
+  if constexpr (sizeof(VT) == 4) a.unphalf_g[row] = to_f4(h);
   double4 d;
   d.x = inv_dt2 * h.x;
   d.y = inv_dt2 * h.y;
@@ -86,6 +87,7 @@ __global__ void __launch_bounds__(kRowThreads) k_step1(Step1Args<VT> a) {
     d.z = d.z - mo * ka.z;
   }
   a.d[row] = d;
+  if constexpr (sizeof(VT) == 4) a.d_g[row] = to_f4(d);
   if (a.r1out) a.r1out[row] = make_double4(rx, ry, rz, 0.0);
 }
 
@@ -101,7 +103,7 @@ __global__ void __launch_bounds__(kRowThreads) k_gt(GtArgs<VT> a) {
 #pragma unroll 4
   for (int j = 0; j < w; j++) {
     const int e = b + 32 * j;
-    const double4 d = ldg4(a.d + __ldcs(a.gt_col + e));
+    const auto d = ldgv(a.d + __ldcs(a.gt_col + e));
     acc += __ldcs(a.gt1 + e) * (VT)d.x + __ldcs(a.gt2 + e) * (VT)d.y + __ldcs(a.gt3 + e) * (VT)d.z;
   }
   a.out[row] = (a.pin > 0 && row == a.pin) ? 0.0 : (double)acc;
@@ -141,6 +143,7 @@ __global__ void __launch_bounds__(kRowThreads) k_step3(Step3Args<VT> a) {
     const double4 h = a.unphalf[row];
     const double4 u1 = make_double4(h.x + a.dt * acc.x, h.y + a.dt * acc.y, h.z + a.dt * acc.z, 0.0);
     a.acc[row] = acc;
+    if constexpr (sizeof(VT) == 4) a.acc_g[row] = to_f4(acc);
     a.unp1[row] = u1;
     if (a.r3out) a.r3out[row] = make_double4(rx, ry, rz, 0.0);
     const double4 pv = a.unp1_prev[row];
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(kRowThreads) k_spmv_k3(SpmvK3Args<VT> a) {
   for (int j = 0; j < w; j++) {
     const int e = b + 32 * j;
     const VT v = __ldcs(a.val + e);
-    const double4 x = ldg4(a.x + __ldcs(a.col + e));
+    const auto x = ldgv(a.x + __ldcs(a.col + e));
     sx += v * (VT)x.x;
     sy += v * (VT)x.y;
     sz += v * (VT)x.z;
@@ -303,6 +306,19 @@ cudaError_t launch_csr_to_sell(int nrows, const int* rp, const double* csr, cons
   k_csr_to_sell<T><<<rows_grid((long long)nslices * 32), kRowThreads, 0, s>>>(nrows, rp, csr, off, sell);
   return cudaGetLastError();
 }
+__global__ void k_vec4_to_f32(int NN, const double4* __restrict__ v, float4* a, float4* b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x) {
+    const float4 f = to_f4(v[i]);
+    a[i] = f;
+    b[i] = f;
+  }
+}
+
+cudaError_t launch_vec4_to_f32(int NN, const double4* v, float4* a, float4* b, cudaStream_t s) {
+  k_vec4_to_f32<<<rows_grid(NN), kRowThreads, 0, s>>>(NN, v, a, b);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_blocks_to_vec4(int NN, const double* blocks, double4* v, cudaStream_t s) {
   k_blocks_to_vec4<<<ew_grid(NN), 256, 0, s>>>(NN, blocks, v);
   return cudaGetLastError();
