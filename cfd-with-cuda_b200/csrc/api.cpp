@@ -161,10 +161,19 @@ struct cfd_ctx {
   DevBuf<int> upmap;  // voxel -> pressure node (empty: identity)
   DevBuf<double> fcg_sc, fcg_part, fcg_work64;
   DevBuf<float> fcg_work32;
+  DevBuf<float> fcg_z1;  // D^-1 r of the split FP32 iteration
+  // Z P per 32-row slice, 27 taps per row, and each row's coarse box origin
+  // (split FP32 iteration; cs_zp_ok when every box fits 3 x 3 x 3)
+  DevBuf<float> cs_zp;
+  DevBuf<int> cs_wlo;
+  bool cs_zp_ok = false;
+  cudaStream_t stream2 = nullptr;  // the coarse solve beside the SpMV
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   DevBuf<unsigned> fcg_cnt;
   DevBuf<int> fcg_done, fcg_err;
   int fcg_window = 25;
   bool fcg_use_graph = true;
+  bool fcg_split = true;  // CFD_FCG_SPLIT=0: the sequential FP32 iteration
   FcgGraph fcg_graph[2][2];  // [FP32 inner solves, FP64 solves][two-level only, with the network]
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
@@ -548,7 +557,9 @@ int ensure_coarse(cfd_ctx* c) {
   }
   CoarseSpace cs;
   std::string err;
-  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err))
+  // Z P for the split FP32 iteration (structured form, identity numbering)
+  const bool want_zp = mixed(c) && c->h_pmap.empty();
+  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err, want_zp))
     return fail(c, CFD_E_NONFINITE, "%s", err.c_str());
   const int nc = cs.nc;
   for (int a = 0; a < 3; a++) {
@@ -604,7 +615,27 @@ int ensure_coarse(cfd_ctx* c) {
   CU(c->cs_c32.alloc(ld));
   CU(cudaMemset(c->cs_c32.p, 0, ld * sizeof(float)));
   CU(c->cs_e64.alloc(nc));
-  if (mixed(c)) CU(c->cs_e32.alloc(nc));
+  if (mixed(c)) {
+    // zeros past nc: the 27-tap boxes of Z P read up to two coarse steps
+    // past a row's box origin
+    const size_t pad = 2 + 2 * (size_t)cs.cd[0] + 2 * (size_t)cs.cd[0] * cs.cd[1];
+    CU(c->cs_e32.alloc(nc + pad));
+    CU(cudaMemset(c->cs_e32.p, 0, (nc + pad) * sizeof(float)));
+  }
+  c->cs_zp_ok = false;
+  c->cs_zp.reset();
+  c->cs_wlo.reset();
+  if (want_zp && cs.w_ok) {
+    const int np = P.NNp;
+    std::vector<float> zp(zp_elems(np), 0.f);
+    for (int p = 0; p < np; p++)
+      for (int t = 0; t < 27; t++) zp[((size_t)(p >> 5) * 27 + t) * 32 + (p & 31)] = (float)cs.w27[27 * (size_t)p + t];
+    CU(c->cs_zp.alloc(zp.size()));
+    CU(cudaMemcpy(c->cs_zp.p, zp.data(), zp.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CU(c->cs_wlo.alloc(np));
+    CU(cudaMemcpy(c->cs_wlo.p, cs.wlo.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+    c->cs_zp_ok = true;
+  }
   // FP32 inner solves on an identity-numbered grid stream Z without column
   // indices (125 coefficients per row) when every coupling stays within two
   // grid steps
@@ -720,8 +751,6 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   // a nonlinear (network) preconditioner needs the deeper orthogonalisation;
   // the linear two-level one is symmetric, for which FCG(1) is CG
   a.st.m = use_net ? c->opt.fcg_m : 1;
-  KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
-  c->launches++;
   const int* pmap = c->upmap.p;
   const VT* dinv;
   float* cc = c->cs_c32.p;
@@ -733,6 +762,19 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
     dinv = c->zdinv.p;
     ce = c->cs_e64.p;
   }
+  // FP32 solves on the structured form with Z P available split the
+  // iteration so that the coarse solve runs beside the SpMV: w = Z (D^-1 r)
+  // on the solver stream, c = P^T r and e = Zc^-1 c on the second stream,
+  // then z = D^-1 r + P e and w += (Z P) e with the dots (the update and
+  // start kernels leave D^-1 r in z1).  Iterations with the network keep
+  // the sequential form: its correction would need a second SpMV.
+  const bool split = sizeof(VT) == 4 && a.stencil && c->cs_zp_ok && !pmap && c->fcg_split;
+  if (split) {
+    if (!c->fcg_z1.p) CU(c->fcg_z1.alloc(n));
+    a.z1 = reinterpret_cast<VT*>(c->fcg_z1.p);
+    a.dinv = dinv;
+  }
+  KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
   const CoarseArgs<VT> ca = coarse_args<VT>(c, true);
   // one flexible-CG iteration: preconditioner (U-Net, coarse restriction
   // and solve, combination), SpMV + dots + coefficients, update + tests
@@ -745,25 +787,57 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       if (e == cudaSuccess) e = netp->forward(s, nullptr, a.st.done);
       return e;
     };
-    auto coarse = [&]() -> cudaError_t {
-      cudaError_t e = launch_coarse_restrict<VT>(ca, a.r, cc, a.st.done, s);
-      if (e == cudaSuccess) e = launch_coarse_solve<VT>(ca, cc, ce, a.st.done, s);
+    auto coarse = [&](cudaStream_t cs) -> cudaError_t {
+      cudaError_t e = launch_coarse_restrict<VT>(ca, a.r, cc, a.st.done, cs);
+      if (e == cudaSuccess) e = launch_coarse_solve<VT>(ca, cc, ce, a.st.done, cs);
       return e;
     };
     auto combine = [&]() -> cudaError_t {
       return launch_precond<VT>(ca, n, a.r, dinv, ce, netp ? netp->out : nullptr, a.st.sc + kFcgRR,
                                 c->unet_dscale, a.z, a.st.done, s);
     };
+    if constexpr (sizeof(VT) == 4) {
+      if (split && !netp) {
+        // per-launch profiling times every launch on the solver stream
+        const bool fork = !c->prof_on;
+        cudaStream_t sb = fork ? c->stream2 : s;
+        if (fork) {
+          CU(cudaEventRecord(c->ev_fork, s));
+          CU(cudaStreamWaitEvent(sb, c->ev_fork, 0));
+        }
+        if (counted) {
+          KL(CFD_K_COARSE, coarse(sb));
+          KL(CFD_K_SPMV_Z, launch_fcg_spmv_jacobi<VT>(a, s));
+        } else {
+          CU(coarse(sb));
+          CU(launch_fcg_spmv_jacobi<VT>(a, s));
+        }
+        if (fork) {
+          CU(cudaEventRecord(c->ev_join, sb));
+          CU(cudaStreamWaitEvent(s, c->ev_join, 0));
+        }
+        if (counted) {
+          KL(CFD_K_FCG, launch_fcg_combine<VT>(a, ca, c->cs_zp.p, c->cs_wlo.p, ce, s));
+          KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
+          c->launches += 1;  // the coarse pair counts as one klaunch
+        } else {
+          CU(launch_fcg_combine<VT>(a, ca, c->cs_zp.p, c->cs_wlo.p, ce, s));
+          CU(launch_fcg_update<VT>(a, s));
+        }
+        return CFD_OK;
+      }
+    }
     if (counted) {
       if (netp) KL(CFD_K_UNET, unet());
-      KL(CFD_K_COARSE, coarse());
+      KL(CFD_K_COARSE, coarse(s));
       KL(CFD_K_FCG, combine());
       KL(CFD_K_SPMV_Z, launch_fcg_spmv<VT>(a, s));
       KL(CFD_K_FCG, launch_fcg_update<VT>(a, s));
-      c->launches += (netp ? netp->launches - l0 + 1 : 0) + 2 + 3;
+      // klaunch counted one launch for the network and one for the coarse pair
+      c->launches += (netp ? netp->launches - l0 : 0) + 1;
     } else {
       if (netp) CU(unet());
-      CU(coarse());
+      CU(coarse(s));
       CU(combine());
       CU(launch_fcg_spmv<VT>(a, s));
       CU(launch_fcg_update<VT>(a, s));
@@ -1022,8 +1096,13 @@ int cfd_create(cfd_ctx** out, int device) {
   if (cudaSetDevice(device) != cudaSuccess) return CFD_E_CUDA;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return CFD_E_CUDA;
+  if (cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess) return CFD_E_CUDA;
+  if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return CFD_E_CUDA;
   if (cudaMallocHost((void**)&c->h_small, 64 * sizeof(double)) != cudaSuccess) return CFD_E_CUDA;
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
   *out = c.release();
   return CFD_OK;
 }
@@ -1032,9 +1111,14 @@ void cfd_destroy(cfd_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream2) cudaStreamSynchronize(c->stream2);
   if (c->h_small) cudaFreeHost(c->h_small);
-  cudaStream_t s = c->stream;
+  cudaStream_t s = c->stream, s2 = c->stream2;
+  cudaEvent_t e1 = c->ev_fork, e2 = c->ev_join;
   delete c;
+  if (e1) cudaEventDestroy(e1);
+  if (e2) cudaEventDestroy(e2);
+  if (s2) cudaStreamDestroy(s2);
   if (s) cudaStreamDestroy(s);
 }
 

@@ -84,11 +84,11 @@ __device__ __forceinline__ void gather_partials(const double* part, int nblk, do
 // Per-row part of the SpMV kernels: w[i] and the dot products of the
 // iteration (z,w) (z,r) (z,q_j) (p_j,r), accumulated into v.
 template <int MD, class VT>
-__device__ __forceinline__ void fcg_row_dots(const FcgArgs<VT>& a, int i, VT wi, int nd,
+__device__ __forceinline__ void fcg_row_dots(const FcgArgs<VT>& a, int i, VT zv, VT wi, int nd,
                                              double (&v)[fcg_parts<MD>()]) {
   const size_t n = (size_t)a.n;
   a.w[i] = wi;
-  const double zi = a.z[i], ri = a.r[i];
+  const double zi = zv, ri = a.r[i];
   v[0] += zi * (double)wi;
   v[1] += zi * ri;
 #pragma unroll
@@ -157,6 +157,7 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_start(FcgArgs<VT> a, int wa
     else
       a.x[i] = 0;
     a.r[i] = ri;
+    if (a.z1) a.z1[i] = a.dinv[i] * ri;
     v[0] += (double)bi * bi;
     v[1] += (double)ri * ri;
   }
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
       st.release(lane);
     }
     const int i = sl * 32 + lane;
-    if (i < a.n) fcg_row_dots<MD>(a, i, acc, nd, v);
+    if (i < a.n) fcg_row_dots<MD>(a, i, a.z[i], acc, nd, v);
   }
   if (!st.failed) st.drain(a.st.timeout_ns);
   fcg_spmv_finish<MD>(a, v, nd, m, it);
@@ -283,7 +284,8 @@ __device__ __forceinline__ void stencil_plane(const VT* q, const VT* __restrict_
   }
 }
 
-template <class VT, int MD>
+// DOTS = false: w = Z z only (the Jacobi part of the split iteration).
+template <class VT, int MD, bool DOTS>
 __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT> a) {
   if (*a.st.done) return;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -346,13 +348,67 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT>
       __syncwarp();
       if (ok) issue(k + kStBuf);
     }
-    if (i < n) fcg_row_dots<MD>(a, i, ((acc[0] + acc[1]) + (acc[2] + acc[3])) + acc[4], nd, v);
+    if (i < n) {
+      const VT wi = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + acc[4];
+      if constexpr (DOTS)
+        fcg_row_dots<MD>(a, i, z[i], wi, nd, v);
+      else
+        a.w[i] = wi;
+    }
   }
   if (!ok && lane == 0) {
     // a bounded wait gave up: give the copies still in flight one more
     // bounded wait before the block (and its shared memory) ends
     for (int kk = kfail; kk < kfail + kStBuf && kk < total; kk++)
       mbar_wait_bounded(mbar + kk % kStBuf, (unsigned)((kk / kStBuf) & 1), a.st.timeout_ns);
+  }
+  if constexpr (DOTS) fcg_spmv_finish<MD>(a, v, nd, m, it);
+}
+
+// The second half of the split iteration: z = z1 + P e (trilinear
+// prolongation of the coarse solution), w = w + (Z P) e with the 27 taps of
+// the row's coarse box, the dot products of the iteration, and in the last
+// block the coefficients (as the SpMV kernels do).  Identity numbering.
+constexpr int kCombineThreads = 256;
+template <class VT, int MD>
+__global__ void __launch_bounds__(kCombineThreads) k_fcg_combine(FcgArgs<VT> a, CoarseArgs<VT> ca,
+                                                                 const float* __restrict__ wst,
+                                                                 const int* __restrict__ wlo,
+                                                                 const VT* __restrict__ e) {
+  if (*a.st.done) return;
+  const double* sc = a.st.sc;
+  const int m = (int)sc[kFcgM], it = (int)sc[kFcgIt];
+  const int nd = it < m ? it : m;
+  const int fx = ca.fd[0], fy = ca.fd[1];
+  const int cx = ca.cd[0], cxy = ca.cd[0] * ca.cd[1];
+  const int bx = ca.cd[0] > 1, by = ca.cd[1] > 1, bz = ca.cd[2] > 1;
+  double v[fcg_parts<MD>()];
+#pragma unroll
+  for (int k = 0; k < fcg_parts<MD>(); k++) v[k] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const int x = i % fx, y = (i / fx) % fy, zz = i / (fx * fy);
+    const int ix = ca.i0x[x], iy = ca.i0y[y], iz = ca.i0z[zz];
+    const VT wx = (VT)ca.fx[x], wy = (VT)ca.fy[y], wz = (VT)ca.fz[zz];
+    const VT* e0 = e + ix + cx * iy + cxy * iz;
+    VT pe = 0;
+#pragma unroll
+    for (int cnr = 0; cnr < 8; cnr++) {
+      const int dx = cnr & 1, dy = (cnr >> 1) & 1, dz = cnr >> 2;
+      if ((dx && !bx) || (dy && !by) || (dz && !bz)) continue;
+      const VT wt = (dx ? wx : 1 - wx) * (dy ? wy : 1 - wy) * (dz ? wz : 1 - wz);
+      pe += wt * e0[dx + cx * dy + cxy * dz];
+    }
+    const VT zi = a.z1[i] + pe;
+    a.z[i] = zi;
+    const float* wr = wst + (size_t)(i >> 5) * 27 * 32 + (i & 31);
+    const VT* eb = e + wlo[i];
+    VT we = 0;
+#pragma unroll
+    for (int t = 0; t < 27; t++) {
+      const int dx = t % 3, dy = (t / 3) % 3, dz = t / 9;
+      we += (VT)__ldcs(wr + t * 32) * eb[dx + cx * dy + cxy * dz];
+    }
+    fcg_row_dots<MD>(a, i, zi, a.w[i] + we, nd, v);
   }
   fcg_spmv_finish<MD>(a, v, nd, m, it);
 }
@@ -383,6 +439,7 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_update(FcgArgs<VT> a) {
     a.x[i] += alpha * pi;
     const VT ri = a.r[i] - alpha * qi;
     a.r[i] = ri;
+    if (a.z1) a.z1[i] = a.dinv[i] * ri;
     v[0] += (double)ri * ri;
   }
   block_sum<1>(v);
@@ -440,6 +497,7 @@ int nblocks(int n) {
 
 int fcg_blocks(int n) { return nblocks(n); }
 size_t stencil_elems(int n) { return (size_t)((n + 31) >> 5) * 125 * 32; }
+size_t zp_elems(int n) { return (size_t)((n + 31) >> 5) * 27 * 32; }
 int fcg_part_words(int n) { return kFcgParts * (nblocks(n) > kFcgMaxBlocks ? nblocks(n) : kFcgMaxBlocks); }
 
 template <class VT>
@@ -449,16 +507,20 @@ cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <class VT, int MD, bool DOTS>
+cudaError_t launch_stencil_kernel(const FcgArgs<VT>& a, cudaStream_t s) {
+  // one wave of two blocks of 16 warps per SM
+  const size_t smem = stencil_smem_bytes<VT>();
+  cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv_stencil<VT, MD, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  k_fcg_spmv_stencil<VT, MD, DOTS><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <class VT, int MD>
 cudaError_t launch_fcg_spmv_md(const FcgArgs<VT>& a, cudaStream_t s) {
-  if (a.stencil) {  // one wave of two blocks of 16 warps per SM
-    const size_t smem = stencil_smem_bytes<VT>();
-    cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv_stencil<VT, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    k_fcg_spmv_stencil<VT, MD><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
-    return cudaGetLastError();
-  }
+  if (a.stencil) return launch_stencil_kernel<VT, MD, true>(a, s);
   const size_t smem = pcg_smem_bytes<VT>();
   cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv<VT, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -475,6 +537,31 @@ cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s) {
   if (a.st.m == 1) return launch_fcg_spmv_md<VT, 1>(a, s);
   if (a.st.m <= 4) return launch_fcg_spmv_md<VT, 4>(a, s);
   return launch_fcg_spmv_md<VT, kFcgMaxM>(a, s);
+}
+
+template <class VT>
+cudaError_t launch_fcg_spmv_jacobi(const FcgArgs<VT>& a, cudaStream_t s) {
+  if (!a.stencil || !a.z1 || a.spmv_grid < 1 || a.spmv_grid > kFcgMaxBlocks) return cudaErrorInvalidValue;
+  FcgArgs<VT> b = a;
+  b.z = a.z1;  // w = Z z1
+  return launch_stencil_kernel<VT, 1, false>(b, s);
+}
+
+template <class VT, int MD>
+cudaError_t launch_combine_md(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, const float* wst, const int* wlo,
+                              const VT* e, cudaStream_t s) {
+  k_fcg_combine<VT, MD><<<nblocks(a.n), kCombineThreads, 0, s>>>(a, ca, wst, wlo, e);
+  return cudaGetLastError();
+}
+
+template <class VT>
+cudaError_t launch_fcg_combine(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, const float* wst, const int* wlo,
+                               const VT* e, cudaStream_t s) {
+  if (!a.z1 || ca.pmap || a.st.m < 1 || a.st.m > kFcgMaxM) return cudaErrorInvalidValue;
+  if ((long long)ca.fd[0] * ca.fd[1] * ca.fd[2] != a.n) return cudaErrorInvalidValue;
+  if (a.st.m == 1) return launch_combine_md<VT, 1>(a, ca, wst, wlo, e, s);
+  if (a.st.m <= 4) return launch_combine_md<VT, 4>(a, ca, wst, wlo, e, s);
+  return launch_combine_md<VT, kFcgMaxM>(a, ca, wst, wlo, e, s);
 }
 
 template <class VT>
@@ -502,5 +589,8 @@ template cudaError_t launch_fcg_spmv<float>(const FcgArgs<float>&, cudaStream_t)
 template cudaError_t launch_fcg_spmv<double>(const FcgArgs<double>&, cudaStream_t);
 template cudaError_t launch_fcg_update<float>(const FcgArgs<float>&, cudaStream_t);
 template cudaError_t launch_fcg_update<double>(const FcgArgs<double>&, cudaStream_t);
+template cudaError_t launch_fcg_spmv_jacobi<float>(const FcgArgs<float>&, cudaStream_t);
+template cudaError_t launch_fcg_combine<float>(const FcgArgs<float>&, const CoarseArgs<float>&, const float*,
+                                               const int*, const float*, cudaStream_t);
 
 }  // namespace cfd

@@ -209,7 +209,9 @@ struct FcgState {
 // p and q point at m ring slots of n entries each; spmv_grid: blocks of the
 // SpMV kernel (two per SM, at most kFcgMaxBlocks).  stencil (may be null):
 // the matrix in structured form (launch_stencil_build) on the grid fd, used
-// by the SpMV instead of the SELL arrays.
+// by the SpMV instead of the SELL arrays.  z1 (may be null): the start and
+// update kernels also write z1 = dinv r, the Jacobi part of the next
+// preconditioned residual.
 template <class VT> struct FcgArgs {
   int n; const int *off, *col; const VT* val; const VT* b;
   VT *x, *r, *z, *w, *p, *q;
@@ -217,6 +219,8 @@ template <class VT> struct FcgArgs {
   const VT* stencil;
   int fd[3];
   FcgState st;
+  VT* z1;
+  const VT* dinv;
 };
 struct Int3 {
   int v[3];
@@ -259,6 +263,21 @@ cudaError_t launch_precond(const CoarseArgs<VT>& a, int nv, const VT* r, const V
 template <class VT> cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s);
 template <class VT> cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s);
 template <class VT> cudaError_t launch_fcg_update(const FcgArgs<VT>& a, cudaStream_t s);
+// The two-level iteration split so that the coarse solve overlaps the SpMV
+// (identity numbering, structured Z):
+//   w = Z z1                               launch_fcg_spmv_jacobi (z1 from
+//                                          the update), beside
+//   c = P^T r, e = Zc^-1 c                 launch_coarse_restrict / _solve
+//   z = z1 + P e, w += (Z P) e, dots,      launch_fcg_combine
+//   coefficients
+// wst: Z P per 32-row slice, 27 taps per row (wst[slice][tap][lane], tap
+// dx + 3 dy + 9 dz over the row's coarse box with origin wlo[row]); e must
+// hold 2 + 2 cd[0] + 2 cd[0] cd[1] zeros past its nc entries.
+size_t zp_elems(int n);
+template <class VT> cudaError_t launch_fcg_spmv_jacobi(const FcgArgs<VT>& a, cudaStream_t s);
+template <class VT>
+cudaError_t launch_fcg_combine(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, const float* wst, const int* wlo,
+                               const VT* e, cudaStream_t s);
 
 void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi);
 template <class VT>

@@ -147,7 +147,8 @@ void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]) {
 }
 
 int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_p, const std::vector<int>& rp,
-                 const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err) {
+                 const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err,
+                 bool with_w) {
   for (int a = 0; a < 3; a++) cs.fd[a] = fd[a];
   coarse_lattice(fd, max_nodes, cs.cd, cs.h);
   const int nc = cs.cd[0] * cs.cd[1] * cs.cd[2];
@@ -204,6 +205,29 @@ int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_
         if (wt == 0.0) continue;
         const int jx = ix + dx - l[0], jy = iy + dy - l[1], jz = iz + dz - l[2];
         w[jx + b[0] * (jy + b[1] * jz)] += val[k] * wt;
+      }
+    }
+  }
+  cs.w_ok = false;
+  cs.wlo.clear();
+  cs.w27.clear();
+  if (with_w) {
+    int widest = 0;
+    for (size_t k = 0; k < bx.size(); k++) widest = std::max(widest, bx[k]);
+    if (widest <= 3) {
+      cs.w_ok = true;
+      cs.wlo.resize(np);
+      cs.w27.assign(27 * (size_t)np, 0.0);
+#pragma omp parallel for schedule(static)
+      for (int p = 0; p < np; p++) {
+        const int* l = &lo[3 * (size_t)p];
+        const int* b = &bx[3 * (size_t)p];
+        const double* w = &W[(size_t)p * wmax];
+        cs.wlo[p] = l[0] + cs.cd[0] * (l[1] + cs.cd[1] * l[2]);
+        for (int jz = 0; jz < b[2]; jz++)
+          for (int jy = 0; jy < b[1]; jy++)
+            for (int jx = 0; jx < b[0]; jx++)
+              cs.w27[27 * (size_t)p + jx + 3 * jy + 9 * jz] = w[jx + b[0] * (jy + b[1] * jz)];
       }
     }
   }

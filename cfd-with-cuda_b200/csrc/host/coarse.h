@@ -16,6 +16,13 @@ struct CoarseSpace {
   double h[3] = {1, 1, 1};    // coarse spacing in voxels: (fd - 1) / (cd - 1)
   int nc = 0;                 // cd[0] cd[1] cd[2]
   std::vector<double> inv;    // nc x nc inverse of Zc (symmetric, row-major)
+  // W = Z P row by row (with_w): row p couples to the coarse nodes of a box
+  // of at most 3 per axis with origin wlo[p] (a coarse node index); w27
+  // holds its 27 coefficients, tap dx + 3 dy + 9 dz (zero outside the box).
+  // w_ok is false when some row's box is wider.
+  bool w_ok = false;
+  std::vector<int> wlo;
+  std::vector<double> w27;
 };
 
 // Coarse lattice for a voxel grid: spacing 4 voxels where the axis allows,
@@ -23,9 +30,11 @@ struct CoarseSpace {
 void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]);
 
 // Builds Zc = P^T Z P from Z in CSR (pressure-node numbering) and inverts it
-// (Cholesky, FP64).  vox_of_p maps a pressure node to its voxel (empty:
-// identity).  Returns 0, or -1 with err set when Zc is not positive definite.
+// (Cholesky, FP64); with_w also keeps W = Z P in 27-tap boxes.  vox_of_p
+// maps a pressure node to its voxel (empty: identity).  Returns 0, or -1 with
+// err set when Zc is not positive definite.
 int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_p, const std::vector<int>& rp,
-                 const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err);
+                 const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err,
+                 bool with_w = false);
 
 }  // namespace cfd

@@ -146,3 +146,34 @@ def test_twolevel_run_matches_oracle(decks, oracle_mod, precision):
     assert rel_l2(Ug, o.vec("Un")) < tol and rel_l2(Pg, o.vec("Pn")) < tol
     s.close()
     o.close()
+
+
+def test_split_iteration_matches_sequential(cavity16, monkeypatch):
+    """The FP32 two-level iteration with the coarse solve beside the SpMV
+    (w = Z D^-1 r + (Z P) e) against the sequential form (w = Z z): the same
+    tolerance in about the same iterations and the same solution and run to
+    FP32 rounding; the bits differ, which shows the split form ran (every
+    kernel of both forms is deterministic)."""
+    import cfdfs
+    kw = dict(precision=cfdfs.MIXED, precond=cfdfs.PC_TWOLEVEL, cg_rtol=1e-10)
+    monkeypatch.setenv("CFD_FCG_SPLIT", "0")
+    s_seq = _solver(cavity16, **kw)
+    monkeypatch.setenv("CFD_FCG_SPLIT", "1")
+    s_spl = _solver(cavity16, **kw)
+    b = np.random.default_rng(5).standard_normal(s_spl.refresh().NNp)
+    b[s_spl.info.zeroPressureNode] = 0.0
+    x1, st1 = s_seq.pressure_solve(b)
+    x2, st2 = s_spl.pressure_solve(b)
+    assert st1.status == 0 and st2.status == 0 and st2.fallback == 0
+    assert abs(st1.iterations - st2.iterations) <= 2, (st1.iterations, st2.iterations)
+    _, nr = s_spl.pressure_residual(b, x2)
+    assert nr <= 1.01e-10 * np.linalg.norm(b)
+    assert rel_l2(x2, x1) < 1e-7
+    assert not np.array_equal(x1, x2)
+    s_seq.run(4)
+    s_spl.run(4)
+    U1, P1 = s_seq.state()
+    U2, P2 = s_spl.state()
+    assert rel_l2(U2, U1) < 1e-7 and rel_l2(P2, P1) < 1e-6
+    s_seq.close()
+    s_spl.close()
