@@ -23,27 +23,31 @@ namespace {
 
 constexpr int kConvThreads = 128;
 
+// Four values of T read from shared memory by one vector load.
+template <class T>
+struct alignas(4 * sizeof(T)) Quad {
+  T x, y, z, w;
+};
+
 template <class T, int TPE>
 __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
   constexpr int EPB = kConvThreads / TPE;
   constexpr int NG = TPE < kMaxNGP ? TPE : kMaxNGP;
-  __shared__ T sSv[NG][27];
-  __shared__ T sdSv[3][NG][27];
+  // operands of the Gauss-point loops packed four to a vector load: the
+  // loops are bound by shared-memory instructions, not by their FMAs
+  __shared__ Quad<T> sB[NG][27];  // {Sv, dSv/dxi, dSv/deta, dSv/dzeta}
   __shared__ T sdSp[3][NG][8];
   __shared__ T sw[NG];
-  __shared__ T u0[EPB][27][3];
-  __shared__ T up[EPB][27][3];
+  __shared__ Quad<T> u0[EPB][27];
+  __shared__ Quad<T> up[EPB][27];
   __shared__ T X[EPB][8][3];
-  __shared__ T cc[EPB][NG][3];
+  __shared__ Quad<T> cc[EPB][NG];
   __shared__ int lt[EPB][27];
   const int t = threadIdx.x, ngp = a.ngp;
   const Basis* B = a.basis;
   for (int i = t; i < ngp * 27; i += blockDim.x) {
     int k = i / 27, j = i % 27;
-    sSv[k][j] = (T)B->Sv[k][j];
-    sdSv[0][k][j] = (T)B->dSv[0][k][j];
-    sdSv[1][k][j] = (T)B->dSv[1][k][j];
-    sdSv[2][k][j] = (T)B->dSv[2][k][j];
+    sB[k][j] = Quad<T>{(T)B->Sv[k][j], (T)B->dSv[0][k][j], (T)B->dSv[1][k][j], (T)B->dSv[2][k][j]};
   }
   for (int i = t; i < ngp * 8; i += blockDim.x) {
     int k = i / 8, m = i % 8;
@@ -67,8 +71,8 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
         lt[l][i] = node;
         const auto u = ldgv(a.un + node);
         const auto p = ldgv(a.uprev + node);
-        u0[l][i][0] = (T)u.x; u0[l][i][1] = (T)u.y; u0[l][i][2] = (T)u.z;
-        up[l][i][0] = (T)p.x; up[l][i][1] = (T)p.y; up[l][i][2] = (T)p.z;
+        u0[l][i] = Quad<T>{(T)u.x, (T)u.y, (T)u.z, T(0)};
+        up[l][i] = Quad<T>{(T)p.x, (T)p.y, (T)p.z, T(0)};
       }
     }
     __syncthreads();
@@ -109,33 +113,37 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
       T g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // g[a][d] = d uprev^d / d xi_a
 #pragma unroll 3
       for (int j = 0; j < 27; j++) {
-        T sv = sSv[k][j], d0 = sdSv[0][k][j], d1 = sdSv[1][k][j], d2 = sdSv[2][k][j];
-        T a0 = u0[el][j][0], a1 = u0[el][j][1], a2 = u0[el][j][2];
-        T b0 = up[el][j][0], b1 = up[el][j][1], b2 = up[el][j][2];
+        const Quad<T> bs = sB[k][j], ua = u0[el][j], ub = up[el][j];
+        const T sv = bs.x, d0 = bs.y, d1 = bs.z, d2 = bs.w;
+        const T a0 = ua.x, a1 = ua.y, a2 = ua.z;
+        const T b0 = ub.x, b1 = ub.y, b2 = ub.z;
         uk[0] += sv * a0; uk[1] += sv * a1; uk[2] += sv * a2;
         g[0][0] += d0 * b0; g[0][1] += d0 * b1; g[0][2] += d0 * b2;
         g[1][0] += d1 * b0; g[1][1] += d1 * b1; g[1][2] += d1 * b2;
         g[2][0] += d2 * b0; g[2][1] += d2 * b1; g[2][2] += d2 * b2;
       }
       const T f = det * sw[k];
+      T ck[3];
 #pragma unroll
       for (int d = 0; d < 3; d++) {
         // physical gradient of uprev^d: grad_i = sum_a iJ[i][a] g[a][d]
         T gx = iJ[0][0] * g[0][d] + iJ[0][1] * g[1][d] + iJ[0][2] * g[2][d];
         T gy = iJ[1][0] * g[0][d] + iJ[1][1] * g[1][d] + iJ[1][2] * g[2][d];
         T gz = iJ[2][0] * g[0][d] + iJ[2][1] * g[1][d] + iJ[2][2] * g[2][d];
-        cc[el][k][d] = (uk[0] * gx + uk[1] * gy + uk[2] * gz) * f;
+        ck[d] = (uk[0] * gx + uk[1] * gy + uk[2] * gz) * f;
       }
+      cc[el][k] = Quad<T>{ck[0], ck[1], ck[2], T(0)};
     }
     __syncthreads();
     if (e >= 0) {
       for (int i = tk; i < 27; i += TPE) {
         T s0 = 0, s1 = 0, s2 = 0;
         for (int k = 0; k < ngp; k++) {
-          T sv = sSv[k][i];
-          s0 += sv * cc[el][k][0];
-          s1 += sv * cc[el][k][1];
-          s2 += sv * cc[el][k][2];
+          const T sv = sB[k][i].x;
+          const Quad<T> ck = cc[el][k];
+          s0 += sv * ck.x;
+          s1 += sv * ck.y;
+          s2 += sv * ck.z;
         }
         double4* dst = a.r1 + lt[el][i];
         if (a.plain) {  // one colour per launch: no other element of it touches this node
