@@ -174,6 +174,9 @@ struct cfd_ctx {
   int fcg_window = 25;
   bool fcg_use_graph = true;
   bool fcg_split = true;  // CFD_FCG_SPLIT=0: the sequential FP32 iteration
+  // blocks per SM of the split iteration's SpMV (CFD_SPLIT_SPMV_PER_SM, 1 or
+  // 2): one leaves half of every SM to the coarse kernels beside it
+  int split_spmv_per_sm = 2;
   FcgGraph fcg_graph[2][2];  // [FP32 inner solves, FP64 solves][two-level only, with the network]
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
@@ -805,12 +808,14 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
           CU(cudaEventRecord(c->ev_fork, s));
           CU(cudaStreamWaitEvent(sb, c->ev_fork, 0));
         }
+        FcgArgs<VT> aj = a;
+        aj.spmv_grid = std::min(c->split_spmv_per_sm * c->num_sms, kFcgMaxBlocks);
         if (counted) {
           KL(CFD_K_COARSE, coarse(sb));
-          KL(CFD_K_SPMV_Z, launch_fcg_spmv_jacobi<VT>(a, s));
+          KL(CFD_K_SPMV_Z, launch_fcg_spmv_jacobi<VT>(aj, s));
         } else {
           CU(coarse(sb));
-          CU(launch_fcg_spmv_jacobi<VT>(a, s));
+          CU(launch_fcg_spmv_jacobi<VT>(aj, s));
         }
         if (fork) {
           CU(cudaEventRecord(c->ev_join, sb));
@@ -1103,6 +1108,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (cudaMallocHost((void**)&c->h_small, 64 * sizeof(double)) != cudaSuccess) return CFD_E_CUDA;
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_SPLIT_SPMV_PER_SM")) c->split_spmv_per_sm = std::atoi(e) == 1 ? 1 : 2;
   *out = c.release();
   return CFD_OK;
 }
