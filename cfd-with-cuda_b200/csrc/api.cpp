@@ -173,11 +173,26 @@ struct cfd_ctx {
   DevBuf<int> fcg_done, fcg_err;
   int fcg_window = 25;
   bool fcg_use_graph = true;
-  bool fcg_split = true;  // CFD_FCG_SPLIT=0: the sequential FP32 iteration
+  // CFD_FCG_SPLIT=1: the split FP32 iteration (coarse solve on a second
+  // stream beside the SpMV); measured slower than the sequential form on the
+  // 64^3 cavity (8.97 against 8.13 ms per step), so off by default
+  bool fcg_split = false;
+  // CFD_FCG_ANCHOR=0: with the network in the head iterations only, keep the
+  // ring of the last fcg_m directions instead of anchoring the head's
+  bool fcg_anchor = true;
   // blocks per SM of the split iteration's SpMV (CFD_SPLIT_SPMV_PER_SM, 1 or
   // 2): one leaves half of every SM to the coarse kernels beside it
   int split_spmv_per_sm = 2;
-  FcgGraph fcg_graph[2][2];  // [FP32 inner solves, FP64 solves][two-level only, with the network]
+  // [FP32 inner solves, FP64 solves][two-level only, with the network]
+  // [window m = 1, m > 1]: the first inner solve of a mixed pressure solve
+  // keeps the network's directions and the refinement solves do not, so
+  // each window has its own graph instead of a re-capture per solve
+  FcgGraph fcg_graph[2][2][2];
+  void reset_fcg_graphs() {
+    for (auto& gp : fcg_graph)
+      for (auto& gq : gp)
+        for (auto& g : gq) g.reset();
+  }
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
 
@@ -516,8 +531,7 @@ int set_grid(cfd_ctx* c, const int dims[3], const int* p_of_vox) {
   for (int a = 0; a < 3; a++) c->udims[a] = dims[a];
   c->grid_set = true;
   c->coarse_ready = false;
-  for (auto& gp : c->fcg_graph)
-    for (auto& g : gp) g.reset();
+  c->reset_fcg_graphs();
   return CFD_OK;
 }
 
@@ -658,8 +672,7 @@ int ensure_coarse(cfd_ctx* c) {
   }
   c->coarse_ready = true;
   c->coarse_gen++;
-  for (auto& gp : c->fcg_graph)
-    for (auto& g : gp) g.reset();
+  c->reset_fcg_graphs();
   c->coarse_setup_s = wall_seconds() - t0;
   return CFD_OK;
 }
@@ -752,8 +765,17 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   a.st.maxit = maxit;
   a.st.window = c->fcg_window;
   // a nonlinear (network) preconditioner needs the deeper orthogonalisation;
-  // the linear two-level one is symmetric, for which FCG(1) is CG
-  a.st.m = use_net ? c->opt.fcg_m : 1;
+  // the linear two-level one is symmetric, for which FCG(1) is CG.  When
+  // the network serves only the first h iterations, their directions stay
+  // in slots 0..h-1 and each later one is orthogonalised against them and
+  // its predecessor (m = h + 1): after the head the residual is Z-orthogonal
+  // to the head's directions, and CG deflated by that space (Saad, Yeung,
+  // Erhel, Guyomarc'h 2000) keeps every direction Z-orthogonal to all
+  // earlier ones with this short recurrence.
+  const int head_iters = c->opt.fcg_net_iters;
+  const bool anchored = use_net && c->fcg_anchor && head_iters > 0 && head_iters + 1 <= kFcgMaxM;
+  a.st.m = !use_net ? 1 : (anchored ? head_iters + 1 : c->opt.fcg_m);
+  a.st.anchor = anchored ? head_iters : 0;
   const int* pmap = c->upmap.p;
   const VT* dinv;
   float* cc = c->cs_c32.p;
@@ -858,7 +880,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
     out = nullptr;
     if (!c->fcg_use_graph || c->prof_on) return CFD_OK;
     if (with_net) CU(netp->prepare_tc(s));  // packs and plans outside the capture
-    FcgGraph& g = c->fcg_graph[sizeof(VT) == 4 ? 0 : 1][with_net ? 1 : 0];
+    FcgGraph& g = c->fcg_graph[sizeof(VT) == 4 ? 0 : 1][with_net ? 1 : 0][a.st.m > 1 ? 1 : 0];
     FcgGraph::Key key{a.b, a.x, a.r, with_net ? c->unet : nullptr, with_net ? netp->gen : 0,
                       with_net ? netp->plan_gen : 0, with_net ? netp->tc_enabled : false, pmap, dinv,
                       c->unet_dscale, n, c->coarse_gen, iters, a.st.m};
@@ -1108,6 +1130,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (cudaMallocHost((void**)&c->h_small, 64 * sizeof(double)) != cudaSuccess) return CFD_E_CUDA;
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_FCG_ANCHOR")) c->fcg_anchor = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_SPLIT_SPMV_PER_SM")) c->split_spmv_per_sm = std::atoi(e) == 1 ? 1 : 2;
   *out = c.release();
   return CFD_OK;
@@ -1947,8 +1970,7 @@ int cfd_unet_train_batch(cfd_unet* u, const int dims[3], int nb, const float* x,
 int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_vox) {
   if (!c) return CFD_E_BADARG;
   if (!u) {
-    for (auto& gp : c->fcg_graph)
-      for (auto& g : gp) g.reset();
+    c->reset_fcg_graphs();
     c->unet = nullptr;
     c->unet_owned.reset();
     return CFD_OK;
@@ -1967,8 +1989,7 @@ int cfd_unet_attach(cfd_ctx* c, cfd_unet* u, const int dims[3], const int* p_of_
     int rc = set_grid(c, dims, p_of_vox);
     if (rc) return rc;
   }
-  for (auto& gp : c->fcg_graph)
-    for (auto& g : gp) g.reset();
+  c->reset_fcg_graphs();
   {
     std::vector<double> dg(nv);
     CU(cudaStreamSynchronize(c->stream));

@@ -140,7 +140,8 @@ __device__ __forceinline__ void fcg_spmv_finish(const FcgArgs<VT>& a, double (&v
 #pragma unroll
     for (int j = 0; j < kFcgMaxM; j++) s[kFcgBeta0 + j] = beta[j];
     s[kFcgAlpha] = alpha;
-    s[kFcgPQ0 + it % m] = pq;  // the new direction takes the oldest slot
+    // the new direction takes the oldest (or, anchored, the last) slot
+    s[kFcgPQ0 + fcg_slot(it, m, (int)s[kFcgAnchor])] = pq;
   }
 }
 
@@ -177,6 +178,7 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_start(FcgArgs<VT> a, int wa
     sc[kFcgMaxit] = st.maxit;
     sc[kFcgWindow] = st.window;
     sc[kFcgM] = st.m;
+    sc[kFcgAnchor] = st.anchor;
     int done = 0;
     double status = -1;
     if (!isfinite(v[0]) || !isfinite(v[1])) {
@@ -418,7 +420,7 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_update(FcgArgs<VT> a) {
   if (*a.st.done) return;
   const double* sc = a.st.sc;
   const int m = (int)sc[kFcgM], it = (int)sc[kFcgIt];
-  const int nd = it < m ? it : m, slot = it % m;
+  const int nd = it < m ? it : m, slot = fcg_slot(it, m, (int)sc[kFcgAnchor]);
   const VT alpha = (VT)sc[kFcgAlpha];
   VT beta[kFcgMaxM];
 #pragma unroll
@@ -503,6 +505,7 @@ int fcg_part_words(int n) { return kFcgParts * (nblocks(n) > kFcgMaxBlocks ? nbl
 template <class VT>
 cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s) {
   if (a.st.m < 1 || a.st.m > kFcgMaxM) return cudaErrorInvalidValue;
+  if (a.st.anchor < 0 || (a.st.anchor > 0 && a.st.m != a.st.anchor + 1)) return cudaErrorInvalidValue;
   k_fcg_start<VT><<<nblocks(a.n), kFcgThreads, 0, s>>>(a, warm);
   return cudaGetLastError();
 }
@@ -529,12 +532,14 @@ cudaError_t launch_fcg_spmv_md(const FcgArgs<VT>& a, cudaStream_t s) {
 }
 
 // the SpMV's dot partials are sized for the solve's window m: 1 (CG with a
-// fixed preconditioner), up to 4, up to kFcgMaxM
+// fixed preconditioner), 2 (one anchored direction and the last), up to 4,
+// up to kFcgMaxM
 template <class VT>
 cudaError_t launch_fcg_spmv(const FcgArgs<VT>& a, cudaStream_t s) {
   if (a.spmv_grid < 1 || a.spmv_grid > kFcgMaxBlocks) return cudaErrorInvalidValue;
   if (a.st.m < 1 || a.st.m > kFcgMaxM) return cudaErrorInvalidValue;
   if (a.st.m == 1) return launch_fcg_spmv_md<VT, 1>(a, s);
+  if (a.st.m == 2) return launch_fcg_spmv_md<VT, 2>(a, s);
   if (a.st.m <= 4) return launch_fcg_spmv_md<VT, 4>(a, s);
   return launch_fcg_spmv_md<VT, kFcgMaxM>(a, s);
 }

@@ -188,11 +188,14 @@ struct PcgArgs {
 // iteration limit, 2 non-finite, 4 stalled (the residual fell by less than
 // sqrt(stall2) over the last window iterations, or the direction broke
 // down).  PQ0.. and Beta0.. hold (p_j, q_j) and beta_j per ring slot.
+// Anchor a > 0 (with m = a + 1): directions 0..a-1 keep slots 0..a-1 for the
+// whole solve and every later direction overwrites slot a, so each new
+// direction is orthogonalised against the first a and the previous one.
 constexpr int kFcgMaxM = 8;        // directions kept at most
 constexpr int kFcgMaxBlocks = 444;  // grid of the iteration kernels (3 per SM)
 enum {
   kFcgRR = 0, kFcgBB, kFcgAlpha, kFcgIt, kFcgStatus, kFcgRRMark, kFcgRtol, kFcgStall2, kFcgMaxit, kFcgWindow,
-  kFcgM, kFcgPQ0 = 12, kFcgBeta0 = kFcgPQ0 + kFcgMaxM, kFcgScalars = kFcgBeta0 + kFcgMaxM
+  kFcgM, kFcgAnchor, kFcgPQ0 = 12, kFcgBeta0 = kFcgPQ0 + kFcgMaxM, kFcgScalars = kFcgBeta0 + kFcgMaxM
 };
 // The iteration kernels read the solve's settings from sc[] (written by the
 // start kernel), so a captured sequence of iterations serves every solve.
@@ -205,7 +208,12 @@ struct FcgState {
   unsigned long long timeout_ns;
   double rtol, stall2;  // read by the start kernel only
   int maxit, window, m;
+  int anchor;  // 0: ring of the last m directions; a > 0: first a kept (m = a + 1)
 };
+// Slot of direction it (0-based) for window m and anchor a.
+__host__ __device__ inline int fcg_slot(int it, int m, int a) {
+  return a > 0 ? (it < a ? it : a) : it % m;
+}
 // p and q point at m ring slots of n entries each; spmv_grid: blocks of the
 // SpMV kernel (two per SM, at most kFcgMaxBlocks).  stencil (may be null):
 // the matrix in structured form (launch_stencil_build) on the grid fd, used

@@ -169,6 +169,38 @@ def test_flexible_cg_solves_to_tolerance(decks, precision):
     net.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_anchored_head_matches_ring(decks, monkeypatch, precision):
+    """With the network in the first iteration of a solve only, flexible CG
+    keeps the network's direction and orthogonalises each later direction
+    against it and its predecessor (CG deflated by the network's direction,
+    two stored directions).  It reaches the requested residual with the
+    solution of the ring of the last 4 directions (CFD_FCG_ANCHOR=0) and,
+    when neither solve fell back to Jacobi-PCG, in at most two more
+    iterations."""
+    import cfdfs
+    kw = dict(precision=precision, cg_rtol=1e-10, precond=cfdfs.PC_LEARNED, fcg_net_iters=1)
+    net = cfdfs.UNet(device=0, seed=5)
+    out = {}
+    for anchor in ("1", "0"):
+        monkeypatch.setenv("CFD_FCG_ANCHOR", anchor)
+        s = _solver(decks["c1"], **kw)
+        s.attach_unet(net, (9, 9, 9))
+        b = np.random.default_rng(3).standard_normal(s.refresh().NNp)
+        b[s.info.zeroPressureNode] = 0.0
+        x, st = s.pressure_solve(b)
+        _, nr = s.pressure_residual(b, x)
+        out[anchor] = (x, st, nr / np.linalg.norm(b))
+        s.close()
+    net.close()
+    (xa, sa, ra), (xr, sr, rr) = out["1"], out["0"]
+    assert sa.status == 0 and sr.status == 0
+    assert ra <= 1.01e-10 and rr <= 1.01e-10
+    assert rel_l2(xa, xr) < 1e-6
+    if sa.fallback == 0 and sr.fallback == 0:
+        assert sa.iterations <= sr.iterations + 2, (sa.iterations, sr.iterations)
+
+
 def test_zero_network_is_twolevel_cg(decks):
     """The preconditioner is a Jacobi step plus the coarse-space correction
     plus the network's correction, so a network that outputs zero turns
