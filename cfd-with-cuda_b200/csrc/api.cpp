@@ -215,6 +215,9 @@ struct cfd_ctx {
 
   int timeN = 0;
   double timeT = 0, maxAcc = 0;
+  // set by cfd_rotate, cleared by cfd_step3 and cfd_begin_step: the latest
+  // Unp1 / Pnp1 then sit in the _prev buffers
+  bool rotated = false;
   double last_norms[5] = {0, 0, 0, 0, 0};
   bool r_debug = true;
 
@@ -1309,6 +1312,7 @@ int cfd_begin_step(cfd_ctx* c) {
   CU(cudaMemcpyAsync(c->unphalf_prev, c->un, NN * sizeof(double4), cudaMemcpyDeviceToDevice, s));
   CU(cudaMemcpyAsync(c->pnp1_prev, c->pn, NNp * sizeof(double), cudaMemcpyDeviceToDevice, s));
   CU(cudaMemsetAsync(c->acc_prev, 0, NN * sizeof(double4), s));
+  c->rotated = false;
   if (mixed(c)) {  // the gathered FP32 copies of the same vectors
     KL(CFD_K_OTHER, launch_vec4_to_f32((int)NN, c->un, c->un32, c->uphp32, s));
     CU(cudaMemsetAsync(c->accp32, 0, NN * sizeof(float4), s));
@@ -1414,6 +1418,7 @@ int cfd_step3(cfd_ctx* c, int iter) {
     a.g1 = c->gs1.p; a.g2 = c->gs2.p; a.g3 = c->gs3.p;
     KL(CFD_K_STEP3, launch_step3<double>(a, s));
   }
+  c->rotated = false;
   return CFD_OK;
 }
 
@@ -1432,8 +1437,12 @@ int cfd_check_iter(cfd_ctx* c, double tol, int* converged, double* norms) {
   return CFD_OK;
 }
 
+// The reference copies (UnpHalf_prev = UnpHalf, Unp1_prev = Unp1, ...,
+// BCH.cpp:2964-2984), so the current vectors keep their values; here the
+// buffers swap, and the current ones are rewritten by the next stages.
 int cfd_rotate(cfd_ctx* c) {
   if (!c) return CFD_E_BADARG;
+  c->rotated = true;
   std::swap(c->unphalf_prev, c->unphalf);
   std::swap(c->unp1_prev, c->unp1);
   std::swap(c->acc_prev, c->acc);
@@ -1467,10 +1476,21 @@ int cfd_check_steady(cfd_ctx* c, double crit, double* maxAcc, int* steady) {
   return CFD_OK;
 }
 
+// Un <- Unp1, Pn <- Pnp1 (BCH.cpp:3080-3081).  When the sub-iteration loop
+// ran out (maxIter iterations without convergence), the last iteration was
+// rotated: its Unp1 and Pnp1 are in the _prev buffers.  Unp1_prev must keep
+// that Unp1 too (the next step's first convergence test compares against
+// it, BCH.cpp:2874 being commented out), so the velocity is copied.
 int cfd_end_step(cfd_ctx* c) {
   if (!c) return CFD_E_BADARG;
-  std::swap(c->un, c->unp1);
-  std::swap(c->pn, c->pnp1);
+  if (c->rotated) {
+    CU(cudaMemcpyAsync(c->un, c->unp1_prev, c->P.NN * sizeof(double4), cudaMemcpyDeviceToDevice, c->stream));
+    std::swap(c->pn, c->pnp1_prev);
+  } else {
+    std::swap(c->un, c->unp1);
+    std::swap(c->pn, c->pnp1);
+  }
+  c->rotated = false;
   return CFD_OK;
 }
 

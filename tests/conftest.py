@@ -66,6 +66,9 @@ def decks(tmp_path_factory):
     out["c1"] = meshgen.write_cavity(str(d / "c1.inp"), meshgen.CavitySpec(8, re=100, dt=0.01, steps=20, ngp=8))
     out["c1_27"] = meshgen.write_cavity(str(d / "c1_27.inp"),
                                         meshgen.CavitySpec(8, re=100, dt=0.01, steps=20, ngp=27))
+    # sub-iteration limit 2: every step ends with the loop run out
+    out["c1_runout"] = meshgen.write_cavity(str(d / "c1_runout.inp"),
+                                            meshgen.CavitySpec(8, re=100, dt=0.01, steps=5, ngp=8, max_iter=2))
     out["graded"] = meshgen.write_cavity(str(d / "graded.inp"),
                                          meshgen.CavitySpec(6, re=400, dt=0.005, steps=5, ngp=8, grading=1.5))
     xyz, conn, faces = perturbed_box(5, 4, 3, 0.2, seed=7)

@@ -128,6 +128,22 @@ def test_full_run_fp64(decks, oracle_mod, key, steps):
     o.close()
 
 
+def test_exhausted_subiterations_match_oracle(decks, oracle_mod):
+    """With a sub-iteration limit of 2, every step runs out of sub-iterations
+    and ends with a rotation; the reference copies the vectors there, so the
+    new state is the last iterate (the pointer-swapping rotation must hand
+    over the same vectors)."""
+    o, s = _pair(decks, oracle_mod, "c1_runout")
+    info_o = o.run(-1)
+    st = s.run(-1)
+    assert st.steps == info_o["steps"] == 5
+    assert st.subiters == info_o["subits"] == 10 and st.last_iter == 3
+    Ug, Pg = s.state()
+    assert rel_l2(Ug, o.vec("Un")) < RUN_TOL and rel_l2(Pg, o.vec("Pn")) < RUN_TOL
+    s.close()
+    o.close()
+
+
 def test_stage_driver_equals_fused_run(decks, oracle_mod):
     """cfd_run and the stage-by-stage entry points give the same result."""
     import cfdfs
