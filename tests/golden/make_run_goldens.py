@@ -10,6 +10,8 @@ runs with these files.
 Cases:
 - ``c2_cavity32``: lid-driven cavity, 32^3 hex27/hex8 elements, Re 400,
   dt 0.005, 200 steps, NGP 8 (the FP64 drop-in configuration).
+- ``c3_cavity64``: lid-driven cavity, 64^3 elements, Re 1000, dt 0.002,
+  100 steps, NGP 8 (the configuration of the headline benchmark).
 - ``duct_24x160``: bent square duct (inlet leg 3, 90-degree bend of
   centreline radius 2, outlet leg 3), 24 x 24 elements across by 160 along,
   Re 200, dt 0.005, 300 steps, NGP 8, parabolic inlet of peak 1.0 set on the
@@ -35,6 +37,8 @@ CASES = {
     "c2_cavity32": dict(kind="cavity", n=32, re=400.0, dt=0.005, steps=200, ngp=8, u_stride=163, p_stride=13),
     "duct_24x160": dict(kind="duct", n_cross=24, n_axial=160, re=200.0, dt=0.005, steps=300, ngp=8,
                         u_stride=499, p_stride=37),
+    "c3_cavity64": dict(kind="cavity", n=64, re=1000.0, dt=0.002, steps=100, ngp=8, u_stride=1499,
+                        p_stride=101),
 }
 
 

@@ -4,6 +4,8 @@ oracle for minutes; too long to repeat on every test run):
 
 - the 32^3 cavity at Re 400, 200 steps (the FP64 drop-in configuration), by
   the FP64 Jacobi-PCG path and by the mixed-precision learned path;
+- the 64^3 cavity at Re 1000, dt 0.002, 100 steps (the configuration of the
+  headline benchmark), by the same two paths;
 - the bent square duct, 24 x 24 x 160 elements, Re 200, 300 steps, parabolic
   inlet, by the same two paths.
 
@@ -83,13 +85,13 @@ def _check(case, st, U, P, tol, counters):
         assert abs(st.cg_iters - int(gd["cg_its"])) <= 2 * st.subiters
 
 
-@pytest.mark.parametrize("case", ["c2_cavity32", "duct_24x160"])
+@pytest.mark.parametrize("case", ["c2_cavity32", "c3_cavity64", "duct_24x160"])
 def test_full_size_fp64_run_matches_oracle(case, tmp_path):
     st, U, P = _run(case, tmp_path, 0, learned=False)
     _check(case, st, U, P, FP64_TOL, counters=True)
 
 
-@pytest.mark.parametrize("case", ["c2_cavity32", "duct_24x160"])
+@pytest.mark.parametrize("case", ["c2_cavity32", "c3_cavity64", "duct_24x160"])
 def test_full_size_mixed_learned_run_matches_oracle(case, tmp_path):
     import cfdfs
     st, U, P = _run(case, tmp_path, cfdfs.MIXED, learned=True)

@@ -21,7 +21,7 @@ def _gen():
     return m
 
 
-@pytest.mark.parametrize("case", ["c2_cavity32", "duct_24x160"])
+@pytest.mark.parametrize("case", ["c2_cavity32", "c3_cavity64", "duct_24x160"])
 def test_golden_file_fits_its_deck(case, tmp_path):
     from cfdfs import HostMesh
     g = _gen()
@@ -34,11 +34,12 @@ def test_golden_file_fits_its_deck(case, tmp_path):
     h.close()
 
 
-def test_cavity_golden_keeps_mirror_symmetry():
+@pytest.mark.parametrize("case", ["c2_cavity32", "c3_cavity64"])
+def test_cavity_golden_keeps_mirror_symmetry(case):
     """The lid moves along x, so the flow is symmetric about the plane
     y = 1/2, where v vanishes: v at the monitor node (the cube centre) is
     zero to rounding while u and w are not."""
-    gd = np.load(os.path.join(HERE, "golden", "c2_cavity32.npz"))
+    gd = np.load(os.path.join(HERE, "golden", f"{case}.npz"))
     u, v, w, _ = gd["mon"]
     assert abs(v) < 1e-12 * max(abs(u), abs(w))
     assert abs(u) > 1e-3
