@@ -170,6 +170,30 @@ def unet_flops(dims):
     return sum(2 * 27 * ci * co * vox[l] for (l, ci, co) in convs)
 
 
+def rank_barrier(dist) -> None:
+    """Barrier over the replicas; nothing to do for one process."""
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, x: float, device: str = "cuda") -> float:
+    """The largest x over the replicas (every rank times its own GPU; the
+    job is as fast as its slowest rank).  device: where the all-reduce
+    buffer lives, "cuda" for NCCL, "cpu" for gloo."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world: int, units_per_rank: float, ms_max: float) -> float:
+    """Whole-job rate of independent replicas (weak scaling): the units all
+    ranks processed over the slowest rank's time in milliseconds."""
+    return world * units_per_rank / (ms_max / 1000.0)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -187,15 +211,10 @@ def run_ours(args, rank, world, local_rank):
     pc_of = {"learned": cfdfs.PC_LEARNED, "twolevel": cfdfs.PC_TWOLEVEL, "jacobi": cfdfs.PC_JACOBI}
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        rank_barrier(dist)
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def ranks_max(x: float) -> float:
+        return max_over_ranks(dist, x)
 
     def timed_solver(precision, precond, steps, warmup):
         s = cfdfs.Solver(device=local_rank, precision=precision, cg_rtol=1e-8, cg_maxit=args.cg_maxit,
@@ -228,16 +247,16 @@ def run_ours(args, rank, world, local_rank):
     precision = cfdfs.MIXED if args.precision == "mixed" else cfdfs.FP64
     s, r = timed_solver(precision, args.precond, args.steps, args.warmup)
     info = s.refresh()
-    ms_max = max_over_ranks(r["ms"])
-    value = world * args.steps / (ms_max / 1000.0)
+    ms_max = ranks_max(r["ms"])
+    value = replica_rate(world, args.steps, ms_max)
 
     # the same precision with the two-level preconditioner alone (the learned
     # preconditioner without its network): what the network adds
     twolevel = None
     if learned and args.fp64_steps:
         s2, r2 = timed_solver(precision, "twolevel", args.steps, args.warmup)
-        ms2 = max_over_ranks(r2["ms"])
-        twolevel = dict(steps_per_s=round(world * args.steps / (ms2 / 1000.0), 4), ms_per_step=round(ms2 / args.steps, 3),
+        ms2 = ranks_max(r2["ms"])
+        twolevel = dict(steps_per_s=round(replica_rate(world, args.steps, ms2), 4), ms_per_step=round(ms2 / args.steps, 3),
                         cg_iters_per_step=round(r2["st"].cg_iters / max(1, r2["st"].steps), 1))
         s2.close()
 
@@ -246,8 +265,8 @@ def run_ours(args, rank, world, local_rank):
     fp64, acc = None, None
     if args.fp64_steps and not (precision == cfdfs.FP64 and args.precond == "jacobi"):
         s64, r64 = timed_solver(cfdfs.FP64, "jacobi", args.steps, args.warmup)
-        ms64 = max_over_ranks(r64["ms"])
-        fp64 = dict(steps=args.steps, steps_per_s=round(world * args.steps / (ms64 / 1000.0), 4),
+        ms64 = ranks_max(r64["ms"])
+        fp64 = dict(steps=args.steps, steps_per_s=round(replica_rate(world, args.steps, ms64), 4),
                     ms_per_step=round(ms64 / args.steps, 3),
                     cg_iters_per_step=round(r64["st"].cg_iters / max(1, r64["st"].steps), 1))
         U1, P1 = s.state()
@@ -285,9 +304,9 @@ def run_ours(args, rank, world, local_rank):
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    e2e_value = world * n_e2e / (e2e_ms / 1000.0)
-    e2e_dev_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs))
+    e2e_ms = ranks_max(ev0.elapsed_time(ev1))
+    e2e_value = replica_rate(world, n_e2e, e2e_ms)
+    e2e_dev_ms = ranks_max(sum(a.elapsed_time(b) for a, b in evs))
     state_bytes = (3 * info.NN + info.NNp) * 8
 
     # per-kernel-class event timing on a separate short pass (events around
@@ -376,7 +395,7 @@ def run_ours(args, rank, world, local_rank):
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 4), "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": n_e2e,
-                    "device_steps_per_s_same_steps": round(world * n_e2e / (e2e_dev_ms / 1000.0), 4),
+                    "device_steps_per_s_same_steps": round(replica_rate(world, n_e2e, e2e_dev_ms), 4),
                     "path": "C ABI: cfd_upload_state + cfd_run(1) + cfd_download_state, pinned host buffers"},
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],
