@@ -8,6 +8,15 @@
 // Solver options (not part of the deck, so the deck stays unchanged):
 //   CFD_PRECISION=fp64|mixed  CFD_CG_RTOL=<x>  CFD_CG_WARM=0|1
 //   CFD_NGP=8|27  CFD_DEVICE=<n>  CFD_MAXSTEPS=<n>  CFD_DETERMINISTIC=0|1
+//   CFD_PRECOND=jacobi|twolevel|learned
+//   CFD_UNET=<weight file> (learned; default weights/unet_cavity.bin beside
+//     the bin/ folder of this program)
+//   CFD_FCG_NET_ITERS=<n> (learned; network in the first n iterations of a
+//     pressure solve, 0 = every iteration; default 1)
+//   CFD_PGRID=nx,ny,nz (twolevel / learned: the structured grid of the
+//     pressure nodes, identity numbering, when they do not form a cube)
+#include <unistd.h>
+
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -20,6 +29,16 @@
 
 static double now() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// weights/unet_cavity.bin next to the bin/ folder that holds this program
+static std::string default_weights() {
+  char buf[4096];
+  const ssize_t n = readlink("/proc/self/exe", buf, sizeof(buf) - 1);
+  if (n <= 0) return "unet_cavity.bin";
+  buf[n] = 0;
+  std::string exe(buf);
+  return exe.substr(0, exe.rfind('/')) + "/../weights/unet_cavity.bin";
 }
 
 static int check(cfd_ctx* c, int rc, const char* what) {
@@ -56,7 +75,16 @@ int main(int argc, char** argv) {
   if (const char* p = std::getenv("CFD_CG_RTOL")) o.cg_rtol = std::atof(p);
   if (const char* p = std::getenv("CFD_CG_WARM")) o.cg_warm = std::atoi(p);
   if (const char* p = std::getenv("CFD_NGP")) o.ngp_override = std::atoi(p);
-  if (const char* p = std::getenv("CFD_PRECOND")) o.precond = std::strcmp(p, "twolevel") == 0 ? CFD_PC_TWOLEVEL : CFD_PC_JACOBI;
+  if (const char* p = std::getenv("CFD_PRECOND"))
+    o.precond = std::strcmp(p, "twolevel") == 0  ? CFD_PC_TWOLEVEL
+                : std::strcmp(p, "learned") == 0 ? CFD_PC_LEARNED
+                                                 : CFD_PC_JACOBI;
+  if (o.precond == CFD_PC_LEARNED) o.fcg_net_iters = 1;
+  if (const char* p = std::getenv("CFD_FCG_NET_ITERS")) o.fcg_net_iters = std::atoi(p);
+  int pgrid[3] = {0, 0, 0};
+  bool have_pgrid = false;
+  if (const char* p = std::getenv("CFD_PGRID"))
+    have_pgrid = std::sscanf(p, "%d,%d,%d", &pgrid[0], &pgrid[1], &pgrid[2]) == 3;
   if (const char* p = std::getenv("CFD_DETERMINISTIC")) o.deterministic = std::atoi(p) != 0;
   long maxsteps = -1;
   if (const char* p = std::getenv("CFD_MAXSTEPS")) maxsteps = std::atol(p);
@@ -83,6 +111,12 @@ int main(int argc, char** argv) {
   check(c, cfd_write_tecplot(c, (name + ".dat").c_str(), name.c_str()), "cfd_write_tecplot");
   t = now();
   check(c, cfd_step0(c), "cfd_step0");
+  if (have_pgrid) check(c, cfd_set_pressure_grid(c, pgrid, nullptr), "cfd_set_pressure_grid");
+  if (o.precond == CFD_PC_LEARNED) {
+    const char* w = std::getenv("CFD_UNET");
+    const std::string wpath = w ? std::string(w) : default_weights();
+    check(c, cfd_unet_load(c, wpath.c_str(), have_pgrid ? pgrid : nullptr), "cfd_unet_load");
+  }
   std::printf("step0()                took  %8.3f seconds.\n", now() - t);
   std::printf("\n NN = %d\n NNp = %d\n sparseM_NNZ = %lld\n sparseG_NNZ = %lld\n NNZ of Z = %lld\n", info.NN,
               info.NNp, 3 * info.nnzK, 3 * info.nnzG, info.nnzZ);
