@@ -169,7 +169,9 @@ int cfd_k_times_acc(cfd_ctx* ctx);
 /* checkConvergenceInTimeGPU, CUDAcodes.cu:1151-1178, with the CPU
  * semantics maxAcc = max |Unp1 - Un| / dt (blascoCodinaHuerta.cpp:3052-3060). */
 int cfd_check_steady(cfd_ctx* ctx, double crit, double* maxAcc, int* steady);
-/* Un <- Unp1, Pn <- Pnp1, blascoCodinaHuerta.cpp:3068-3081. */
+/* Un <- Unp1, Pn <- Pnp1, blascoCodinaHuerta.cpp:3068-3081.  Called right
+ * after cfd_rotate (a sub-iteration loop that ran out of iterations), it
+ * still takes the last iterate, as the reference's copying rotation does. */
 int cfd_end_step(cfd_ctx* ctx);
 
 /* Whole time loop on the device with one small readback per sub-iteration:
