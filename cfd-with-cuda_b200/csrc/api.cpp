@@ -1124,7 +1124,9 @@ int cfd_create(cfd_ctx** out, int device) {
   c->device = device;
   cfd_default_options(&c->opt);
   if (cudaSetDevice(device) != cudaSuccess) return CFD_E_CUDA;
-  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+      c->num_sms < 1)
+    return CFD_E_CUDA;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return CFD_E_CUDA;
   if (cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess) return CFD_E_CUDA;
   if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||

@@ -84,7 +84,10 @@ UnetNet::~UnetNet() {
 int UnetNet::init(unsigned long long seed) {
   nparam = unet_param_count();
   if (cudaGetDevice(&device) != cudaSuccess) return -1;
-  cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || num_sms < 1) {
+    err = "cannot read the SM count of the device";
+    return -1;
+  }
   if (const char* e = std::getenv("CFD_UNET_TC")) tc_enabled = std::atoi(e) != 0;
   if (!own_stream && cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
   const size_t b = (size_t)nparam * sizeof(float);
