@@ -59,6 +59,52 @@ def test_operator_identities(decks, oracle_mod):
     o.close()
 
 
+@pytest.mark.parametrize("key", ["c1", "c1_27"])
+def test_convection_identities(decks, oracle_mod, key):
+    """R1 = -A(Un) UnpHalf_prev with A_ij = sum_k Sv_i (u . grad Sv_j) detJ w
+    (calculateMatrixA, blascoCodinaHuerta.cpp:3520-3685), per component:
+    - a constant field has no convective derivative (A 1 = 0, because the
+      gradients of the 27 shape functions sum to zero);
+    - R1 is linear in UnpHalf_prev;
+    - with u constant and x zero on the boundary, x . A x = 1/2 sum of
+      u . grad(x^2) over the Gauss points vanishes: along each axis the
+      tensor Gauss rule integrates the derivative of the polynomial x^2
+      exactly, and the two elements of a shared face evaluate it at the same
+      face points, so the element sums telescope to the boundary, where x
+      is zero.  This holds for NGP 8 and 27 alike."""
+    o = oracle_mod.Oracle(decks[key])
+    o.step0()
+    NN = o.NN
+    X = o.coord()
+    x, y, z = X[:, 0], X[:, 1], X[:, 2]
+    o.set_vec("Un", np.concatenate([np.sin(np.pi * x) * y, np.cos(np.pi * y) * z, x * y * z]))
+    rng = np.random.default_rng(7)
+
+    def conv(v):
+        o.set_vec("UnpHalf_prev", v)
+        return o.convect()
+
+    v1, v2 = rng.standard_normal(3 * NN), rng.standard_normal(3 * NN)
+    r1, r2 = conv(v1), conv(v2)
+    scale = np.abs(r1).max()
+    assert scale > 0
+    assert np.abs(conv(np.ones(3 * NN))).max() < 1e-13 * scale
+    r12 = conv(2.0 * v1 - 3.0 * v2)
+    assert np.abs(r12 - (2.0 * r1 - 3.0 * r2)).max() < 1e-12 * np.abs(r12).max()
+
+    u = np.array([0.3, -0.5, 0.7])
+    o.set_vec("Un", np.repeat(u, NN))
+    bc = o.bcnodes()[:, 0]
+    xv = rng.standard_normal(3 * NN)
+    for d in range(3):
+        xv[d * NN + bc] = 0.0
+    r = conv(xv)
+    for d in range(3):
+        xd, rd = xv[d * NN:(d + 1) * NN], r[d * NN:(d + 1) * NN]
+        assert abs(xd @ rd) < 1e-12 * np.linalg.norm(xd) * np.linalg.norm(rd)
+    o.close()
+
+
 def test_sizes_against_formulas(decks, oracle_mod):
     golden = json.load(open(GOLDEN))
     o = oracle_mod.Oracle(decks["c1"])
