@@ -105,6 +105,38 @@ def test_convection_identities(decks, oracle_mod, key):
     o.close()
 
 
+def test_linear_fields_are_integrated_exactly(decks, oracle_mod):
+    """A velocity or pressure field that is linear in the coordinates is
+    represented exactly by the hex27 / hex8 spaces of straight-sided
+    elements (mid-nodes at the corner averages), and the Gauss rule integrates
+    the products below exactly, even on the non-affine perturbed mesh:
+    - x.K x = nu |a|^2 |Omega| for x = a.X (K = nu int grad Sv . grad Sv);
+    - sum_i X_d,i (G_d p)_i = -(1/rho) int p for p = b.X
+      (G_d = -(1/rho) int Sp_j d_d Sv_i, and sum_i X_d,i Sv_i = X_d)."""
+    a = np.array([0.3, 0.2, -0.5])
+    b = np.array([0.7, -0.4, 0.25])
+    for key in ("perturbed", "graded"):
+        o = oracle_mod.Oracle(decks[key])
+        o.step0()
+        X = o.coord()
+        gw = o.basis()["gqw"]
+        vol = float((o.detj() * gw[None, :]).sum())
+        x = X @ a
+        K = o.csr("K")
+        assert abs(x @ (K @ x) - o.viscosity * (a @ a) * vol) < 1e-12 * o.viscosity * vol
+        # int p over the domain from the hex8 interpolation at the Gauss points
+        bas = o.basis()
+        conn = o.ltog()[:, :8]
+        p = X[: o.NNp] @ b
+        p_gp = p[conn] @ bas["Sp"].T                   # NE x NGP
+        int_p = float((p_gp * o.detj() * gw[None, :]).sum())
+        for d, name in enumerate(("G1", "G2", "G3")):
+            G = o.csr(name)
+            lhs = X[:, d] @ (G @ p)
+            assert abs(lhs + int_p / o.density) < 1e-12 * max(1.0, abs(int_p)), (key, name, lhs, int_p)
+        o.close()
+
+
 def test_sizes_against_formulas(decks, oracle_mod):
     golden = json.load(open(GOLDEN))
     o = oracle_mod.Oracle(decks["c1"])
