@@ -64,6 +64,46 @@ def test_bad_decks_rejected(tmp_path, decks):
         HostMesh(str(tmp_path / "missing.inp"))
 
 
+def _edit_after(text, header, fn):
+    """The deck with fn applied to the first data line after the line that
+    starts with header (skipping the ==== separator lines)."""
+    lines = text.split("\n")
+    i = next(k for k, l in enumerate(lines) if l.startswith(header)) + 1
+    while lines[i].startswith("===="):
+        i += 1
+    lines[i] = fn(lines[i])
+    return "\n".join(lines)
+
+
+def test_out_of_range_values_rejected(tmp_path, decks):
+    """Values that would index outside the mesh or break the time loop are
+    rejected on the host with a message, before anything reaches the device:
+    a velocity BC face outside 1..6, a BC number beyond nBC, a zero-pressure
+    node beyond the corner nodes, dt <= 0, and an NGP other than 1, 8, 27."""
+    from cfdfs import HostMesh, CfdError
+    good = open(decks["c1"]).read()
+    HostMesh(decks["c1"]).close()
+    hdr = "Velocity BC (Elem# Face# BC#)"
+    cases = {
+        "face": (_edit_after(good, hdr, lambda l: " ".join(l.split()[:1] + ["9"] + l.split()[2:])),
+                 "velocity BC face out of range"),
+        "bc_id": (_edit_after(good, hdr, lambda l: " ".join(l.split()[:2] + ["5"])),
+                  "velocity BC face out of range"),
+        "zero_p": (_edit_after(good, "Node number where pressure", lambda l: "100000"),
+                   "zero-pressure node out of range"),
+        "dt": ("\n".join(("dt       : 0.0" if l.startswith("dt ") else l) for l in good.split("\n")),
+               "dt must be > 0"),
+        "ngp": ("\n".join(("NGP      : 4" if l.startswith("NGP") else l) for l in good.split("\n")),
+                "NGP must be 1, 8 or 27"),
+    }
+    for name, (text, msg) in cases.items():
+        assert text != good, name
+        p = tmp_path / f"{name}.inp"
+        p.write_text(text)
+        with pytest.raises(CfdError, match=msg):
+            HostMesh(str(p))
+
+
 @pytest.mark.parametrize("key", ["c1", "graded", "perturbed", "duct_small"])
 def test_element_colouring_conflict_free(decks, key):
     """The deterministic mode's colouring (one colour per launch, plain adds):
