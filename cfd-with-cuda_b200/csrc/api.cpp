@@ -1204,6 +1204,9 @@ int cfd_load_mesh(cfd_ctx* c, const cfd_problem_info* info, const double* coords
   P.zeroP = info->zeroPressureNode;
   NEED(P.NE > 0 && P.NCN > 0 && P.dt > 0 && P.maxIter > 0, "bad problem sizes");
   NEED(P.NGP == 1 || P.NGP == 8 || P.NGP == 27, "NGP must be 1, 8 or 27");
+  // negative: no pin (the reference pins only p > 0); beyond the corner
+  // nodes the pin would silently not apply and leave Z singular
+  NEED(P.zeroP < P.NCN, "zero-pressure node out of range");
   P.NNp = P.NCN;
   P.coord.assign(coords, coords + 3 * (size_t)P.NCN);
   P.ltog.assign((size_t)P.NE * 27, -1);
