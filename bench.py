@@ -386,6 +386,7 @@ def run_ours(args, rank, world, local_rank):
                        "setup_s": round(r["setup_s"], 2)},
             "cg_iters_per_step": round(r["st"].cg_iters / max(1, r["st"].steps), 1),
             "subiters_per_step": round(r["st"].subiters / max(1, r["st"].steps), 2),
+            "pressure_fallbacks": int(r["st"].fallbacks),  # solves that fell back to Jacobi-PCG
             "fp64_path": fp64,
             "twolevel_path": twolevel,
             "speedup_vs_fp64": round(value / fp64["steps_per_s"], 3) if fp64 else None,
