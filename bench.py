@@ -158,6 +158,28 @@ def algorithmic_bytes(info, klass, iters_per_launch, mixed):
     return 0
 
 
+def cg_iteration_bytes(info, mixed):
+    """Algorithmic bytes of one CG iteration: one pass over Z (values and
+    int32 columns) with its vectors, plus p, r, x, Ap and the diagonal."""
+    s = 4 if mixed else 8
+    return info.nnzZ * (s + 4) + 4 * (info.NNp + 1) + 2 * info.NNp * s + 9 * info.NNp * s
+
+
+def step_bytes(info, steps, subiters, cg_iters, mixed):
+    """Algorithmic HBM bytes of one time step, averaged over a run: per
+    sub-iteration the convection, step1 (K u, G p, update), G^T, step3 and
+    about 12 element-wise passes over the FP64 state; per CG iteration
+    cg_iteration_bytes; one K Acc pass per sub-iteration that did not end
+    its step (subiters - steps, exact when no step ran out)."""
+    per_sub = (algorithmic_bytes(info, "convect", 0, mixed) + algorithmic_bytes(info, "step1", 0, mixed)
+               + algorithmic_bytes(info, "gt", 0, mixed) + algorithmic_bytes(info, "step3", 0, mixed)
+               + 12 * 3 * info.NN * 8)
+    kacc = max(0, subiters - steps)
+    total = (subiters * per_sub + cg_iters * cg_iteration_bytes(info, mixed)
+             + kacc * algorithmic_bytes(info, "spmv_k3", 0, mixed))
+    return total / max(1, steps)
+
+
 def unet_flops(dims):
     """FLOPs of one U-Net application on a pressure grid (multiply-adds of the
     11 convolutions, counted as 2 flops each)."""
@@ -349,6 +371,13 @@ def run_ours(args, rank, world, local_rank):
                 # dram__bytes_read.sum + dram__bytes_write.sum of one launch
                 # (one ncu --set full capture of this kernel on the 64^3 cavity)
                 roof["traffic"] = int(139.889152e6 + 4.155648e6)
+    # the whole step on the same algorithmic byte counts, with the timed
+    # run's own sub-iteration and CG iteration counts
+    st_t = r["st"]
+    b_step = step_bytes(info, st_t.steps, st_t.subiters, st_t.cg_iters, precision == cfdfs.MIXED)
+    step_ach = b_step / (ms_max / args.steps / 1000.0) / 1e9
+    step_roof = {"bound": "hbm", "bytes_per_step": int(b_step), "achieved": round(step_ach, 1), "peak": peak,
+                 "unit": "GB/s", "frac": round(step_ach / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs"}
     total_ms = sum(v["ms"] for v in prof.values())
     kernels = {k: dict(launches=v["launches"], ms=round(v["ms"], 3),
                        share=round(v["ms"] / total_ms, 4) if total_ms else 0.0,
@@ -392,6 +421,7 @@ def run_ours(args, rank, world, local_rank):
             "speedup_vs_fp64": round(value / fp64["steps_per_s"], 3) if fp64 else None,
             "accuracy": acc,
             "roofline": roof,
+            "step_roofline": step_roof,
             "kernels": kernels,
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_value, 4), "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
