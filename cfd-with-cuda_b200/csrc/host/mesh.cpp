@@ -23,7 +23,9 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
+#include <parallel/algorithm>
 #include <sstream>
+#include <utility>
 
 #include "../../../include/cfdfs.h"
 #include "problem.h"
@@ -268,60 +270,72 @@ struct Key2 {
 };
 
 // Numbers the distinct keys in order of first appearance (appearance index =
-// position in keys[]) starting at base; out[i] = number of keys[i].
+// position in keys[]) starting at base; out[i] = number of keys[i].  The
+// (key, index) pairs are sorted in parallel; since the indices differ, the
+// order is total and each group of equal keys starts at its first
+// appearance.
 template <class K>
 int number_by_first_appearance(const std::vector<K>& keys, int base, std::vector<int>& out) {
-  size_t n = keys.size();
-  std::vector<uint32_t> idx(n);
-  std::iota(idx.begin(), idx.end(), 0u);
-  std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) {
-    if (keys[x] == keys[y]) return x < y;
-    return keys[x] < keys[y];
+  const size_t n = keys.size();
+  std::vector<std::pair<K, uint32_t>> kv(n);
+#pragma omp parallel for schedule(static)
+  for (size_t i = 0; i < n; i++) kv[i] = {keys[i], (uint32_t)i};
+  __gnu_parallel::sort(kv.begin(), kv.end(), [](const std::pair<K, uint32_t>& x, const std::pair<K, uint32_t>& y) {
+    return x.first < y.first || (x.first == y.first && x.second < y.second);
   });
-  // group leader = first appearance (smallest index, first in group)
+  // group leader = first appearance (smallest index, first in its group)
   std::vector<uint32_t> leader(n);
-  std::vector<uint32_t> leaders;
+  std::vector<char> first(n, 0);
   for (size_t s = 0; s < n;) {
     size_t t = s;
-    while (t < n && keys[idx[t]] == keys[idx[s]]) t++;
-    for (size_t u = s; u < t; u++) leader[idx[u]] = idx[s];
-    leaders.push_back(idx[s]);
+    while (t < n && kv[t].first == kv[s].first) t++;
+    for (size_t u = s; u < t; u++) leader[kv[u].second] = kv[s].second;
+    first[kv[s].second] = 1;
     s = t;
   }
-  std::sort(leaders.begin(), leaders.end());
+  // leaders numbered in index order
   std::vector<int> number(n, -1);
-  for (size_t r = 0; r < leaders.size(); r++) number[leaders[r]] = base + (int)r;
+  int count = 0;
+  for (size_t i = 0; i < n; i++)
+    if (first[i]) number[i] = base + count++;
   out.resize(n);
+#pragma omp parallel for schedule(static)
   for (size_t i = 0; i < n; i++) out[i] = number[leader[i]];
-  return (int)leaders.size();
+  return count;
 }
 
-// CSR of the union, per row, of the node sets of the elements around it.
+// Row r: the distinct nodes j in [first, first + count) of the elements
+// around r (in incidence order), written to out when it is not null;
+// returns how many.  stamp (ncols entries) must not hold r on entry.
+inline int gather_row(int r, const std::vector<int>& inc_rp, const std::vector<int>& inc_el, const std::vector<int>& ltog,
+                      int first, int count, std::vector<int>& stamp, int* out) {
+  int k = 0;
+  for (int t = inc_rp[r]; t < inc_rp[r + 1]; t++) {
+    const int* L = &ltog[(size_t)inc_el[t] * 27];
+    for (int j = first; j < first + count; j++) {
+      const int v = L[j];
+      if (stamp[v] != r) {
+        stamp[v] = r;
+        if (out) out[k] = v;
+        k++;
+      }
+    }
+  }
+  return k;
+}
+
+// CSR of the union, per row, of the node sets of the elements around it:
+// one pass counts the row lengths, a second fills the rows in place and
+// sorts them.
 void build_pattern(int nrows, const std::vector<int>& inc_rp, const std::vector<int>& inc_el,
                    const std::vector<int>& ltog, int first, int count, int ncols, std::vector<int>& rp,
                    std::vector<int>& col, int& maxrow) {
   std::vector<int> len(nrows, 0);
-  std::vector<std::vector<int>> rows(nrows);
 #pragma omp parallel
   {
     std::vector<int> stamp(ncols, -1);
 #pragma omp for schedule(dynamic, 1024)
-    for (int r = 0; r < nrows; r++) {
-      std::vector<int>& c = rows[r];
-      c.reserve(128);
-      for (int t = inc_rp[r]; t < inc_rp[r + 1]; t++) {
-        const int* L = &ltog[(size_t)inc_el[t] * 27];
-        for (int j = first; j < first + count; j++) {
-          int v = L[j];
-          if (stamp[v] != r) {
-            stamp[v] = r;
-            c.push_back(v);
-          }
-        }
-      }
-      std::sort(c.begin(), c.end());
-      len[r] = (int)c.size();
-    }
+    for (int r = 0; r < nrows; r++) len[r] = gather_row(r, inc_rp, inc_el, ltog, first, count, stamp, nullptr);
   }
   rp.assign(nrows + 1, 0);
   maxrow = 0;
@@ -330,10 +344,15 @@ void build_pattern(int nrows, const std::vector<int>& inc_rp, const std::vector<
     maxrow = std::max(maxrow, len[r]);
   }
   col.resize(rp[nrows]);
-#pragma omp parallel for schedule(static)
-  for (int r = 0; r < nrows; r++) {
-    std::copy(rows[r].begin(), rows[r].end(), col.begin() + rp[r]);
-    std::vector<int>().swap(rows[r]);
+#pragma omp parallel
+  {
+    std::vector<int> stamp(ncols, -1);
+#pragma omp for schedule(dynamic, 1024)
+    for (int r = 0; r < nrows; r++) {
+      int* c = col.data() + rp[r];
+      gather_row(r, inc_rp, inc_el, ltog, first, count, stamp, c);
+      std::sort(c, c + len[r]);
+    }
   }
 }
 
@@ -475,48 +494,48 @@ int preprocess(HostProblem& P, std::string& err) {
   // ---- patterns ----
   build_pattern(P.NN, inc_rp, inc_el, P.ltog, 0, 27, P.NN, P.k_rp, P.k_col, P.maxKrow);
   build_pattern(P.NN, inc_rp, inc_el, P.ltog, 0, 8, P.NNp, P.g_rp, P.g_col, P.maxGrow);
-  // G^T by counting sort (rows p, columns v ascending)
-  {
-    size_t nnz = P.g_col.size();
-    P.gt_rp.assign(P.NNp + 1, 0);
-    for (size_t i = 0; i < nnz; i++) P.gt_rp[P.g_col[i] + 1]++;
-    for (int p = 0; p < P.NNp; p++) P.gt_rp[p + 1] += P.gt_rp[p];
-    P.gt_col.resize(nnz);
-    P.gt_pos.resize(nnz);
-    std::vector<int> fill(P.gt_rp.begin(), P.gt_rp.end() - 1);
-    for (int v = 0; v < P.NN; v++)
-      for (int i = P.g_rp[v]; i < P.g_rp[v + 1]; i++) {
-        int p = P.g_col[i];
-        P.gt_col[fill[p]] = v;
-        P.gt_pos[fill[p]] = i;
-        fill[p]++;
-      }
-    P.maxGtrow = 0;
-    for (int p = 0; p < P.NNp; p++) P.maxGtrow = std::max(P.maxGtrow, P.gt_rp[p + 1] - P.gt_rp[p]);
+  // G^T (rows p, columns v ascending): (v, p) is in G exactly when v and the
+  // corner node p share an element, so row p is the union of the 27 nodes
+  // of the elements around p (pressure nodes are the corner nodes 0..NCN-1);
+  // gt_pos = index of (v, p) in the sorted G row v
+  build_pattern(P.NNp, inc_rp, inc_el, P.ltog, 0, 27, P.NN, P.gt_rp, P.gt_col, P.maxGtrow);
+  if (P.gt_col.size() != P.g_col.size()) {
+    err = "inconsistent G and G^T patterns";
+    return CFD_E_BADINPUT;
   }
-  // Z pattern: row p = union of G-row columns over the velocity nodes in G^T row p
+  P.gt_pos.resize(P.gt_col.size());
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int p = 0; p < P.NNp; p++)
+    for (int t = P.gt_rp[p]; t < P.gt_rp[p + 1]; t++) {
+      const int v = P.gt_col[t];
+      const int* b = P.g_col.data() + P.g_rp[v];
+      const int* e = P.g_col.data() + P.g_rp[v + 1];
+      P.gt_pos[t] = (int)(std::lower_bound(b, e, p) - P.g_col.data());
+    }
+  // Z pattern: row p = union of G-row columns over the velocity nodes in
+  // G^T row p (counted, then filled in place and sorted)
   {
+    auto zrow = [&](int p, std::vector<int>& stamp, int* out) {
+      int k = 0;
+      for (int t = P.gt_rp[p]; t < P.gt_rp[p + 1]; t++) {
+        const int v = P.gt_col[t];
+        for (int i = P.g_rp[v]; i < P.g_rp[v + 1]; i++) {
+          const int q = P.g_col[i];
+          if (stamp[q] != p) {
+            stamp[q] = p;
+            if (out) out[k] = q;
+            k++;
+          }
+        }
+      }
+      return k;
+    };
     std::vector<int> len(P.NNp, 0);
-    std::vector<std::vector<int>> rows(P.NNp);
 #pragma omp parallel
     {
       std::vector<int> stamp(P.NNp, -1);
 #pragma omp for schedule(dynamic, 256)
-      for (int p = 0; p < P.NNp; p++) {
-        auto& c = rows[p];
-        for (int t = P.gt_rp[p]; t < P.gt_rp[p + 1]; t++) {
-          int v = P.gt_col[t];
-          for (int i = P.g_rp[v]; i < P.g_rp[v + 1]; i++) {
-            int q = P.g_col[i];
-            if (stamp[q] != p) {
-              stamp[q] = p;
-              c.push_back(q);
-            }
-          }
-        }
-        std::sort(c.begin(), c.end());
-        len[p] = (int)c.size();
-      }
+      for (int p = 0; p < P.NNp; p++) len[p] = zrow(p, stamp, nullptr);
     }
     P.z_rp.assign(P.NNp + 1, 0);
     P.maxZrow = 0;
@@ -525,8 +544,16 @@ int preprocess(HostProblem& P, std::string& err) {
       P.maxZrow = std::max(P.maxZrow, len[p]);
     }
     P.z_col.resize(P.z_rp[P.NNp]);
-#pragma omp parallel for schedule(static)
-    for (int p = 0; p < P.NNp; p++) std::copy(rows[p].begin(), rows[p].end(), P.z_col.begin() + P.z_rp[p]);
+#pragma omp parallel
+    {
+      std::vector<int> stamp(P.NNp, -1);
+#pragma omp for schedule(dynamic, 256)
+      for (int p = 0; p < P.NNp; p++) {
+        int* c = P.z_col.data() + P.z_rp[p];
+        zrow(p, stamp, c);
+        std::sort(c, c + len[p]);
+      }
+    }
   }
   if ((long long)P.k_rp[P.NN] >= (1LL << 31) - 1) {
     err = "K has more than 2^31 non-zeros";
