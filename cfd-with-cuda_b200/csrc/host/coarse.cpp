@@ -72,16 +72,48 @@ bool cholesky(std::vector<double>& A, int n) {
         ri[j] = s / rj[j];
       }
     }
-#pragma omp parallel for schedule(dynamic, 8)
-    for (int i = k1; i < n; i++) {
-      double* ri = a + (size_t)i * n;
-      const double* pi = ri + k0;
-      for (int j = k1; j <= i; j++) {
-        const double* pj = a + (size_t)j * n + k0;
-        double s = 0.0;
-#pragma omp simd reduction(+ : s)
-        for (int k = 0; k < k1 - k0; k++) s += pi[k] * pj[k];
-        ri[j] -= s;
+    // trailing update A[i][j] -= sum_k A[i][k] A[j][k] (k in the panel,
+    // k1 <= j <= i) in 4 x 4 tiles: 16 dot products share the loads of 8
+    // panel rows
+    const int nbk = k1 - k0;
+    const int ntile = (n - k1 + 3) / 4;
+#pragma omp parallel for schedule(dynamic, 2)
+    for (int ti = 0; ti < ntile; ti++) {
+      const int i0 = k1 + 4 * ti;
+      const int ni = std::min(4, n - i0);
+      for (int j0 = k1; j0 < i0 + ni; j0 += 4) {
+        const int nj = std::min(4, n - j0);
+        double s[4][4] = {};
+        if (ni == 4 && nj == 4) {
+          const double *p0 = a + (size_t)i0 * n + k0, *p1 = p0 + n, *p2 = p1 + n, *p3 = p2 + n;
+          const double *q0 = a + (size_t)j0 * n + k0, *q1 = q0 + n, *q2 = q1 + n, *q3 = q2 + n;
+          double s00 = 0, s01 = 0, s02 = 0, s03 = 0, s10 = 0, s11 = 0, s12 = 0, s13 = 0;
+          double s20 = 0, s21 = 0, s22 = 0, s23 = 0, s30 = 0, s31 = 0, s32 = 0, s33 = 0;
+#pragma omp simd reduction(+ : s00, s01, s02, s03, s10, s11, s12, s13, s20, s21, s22, s23, s30, s31, s32, s33)
+          for (int k = 0; k < nbk; k++) {
+            const double x0 = p0[k], x1 = p1[k], x2 = p2[k], x3 = p3[k];
+            const double y0 = q0[k], y1 = q1[k], y2 = q2[k], y3 = q3[k];
+            s00 += x0 * y0; s01 += x0 * y1; s02 += x0 * y2; s03 += x0 * y3;
+            s10 += x1 * y0; s11 += x1 * y1; s12 += x1 * y2; s13 += x1 * y3;
+            s20 += x2 * y0; s21 += x2 * y1; s22 += x2 * y2; s23 += x2 * y3;
+            s30 += x3 * y0; s31 += x3 * y1; s32 += x3 * y2; s33 += x3 * y3;
+          }
+          const double t[4][4] = {{s00, s01, s02, s03}, {s10, s11, s12, s13}, {s20, s21, s22, s23},
+                                  {s30, s31, s32, s33}};
+          for (int u = 0; u < 4; u++)
+            for (int v = 0; v < 4; v++) s[u][v] = t[u][v];
+        } else {
+          for (int u = 0; u < ni; u++)
+            for (int v = 0; v < nj; v++) {
+              const double* pi = a + (size_t)(i0 + u) * n + k0;
+              const double* pj = a + (size_t)(j0 + v) * n + k0;
+              double acc = 0.0;
+              for (int k = 0; k < nbk; k++) acc += pi[k] * pj[k];
+              s[u][v] = acc;
+            }
+        }
+        for (int u = 0; u < ni; u++)
+          for (int v = 0; v < nj && j0 + v <= i0 + u; v++) a[(size_t)(i0 + u) * n + j0 + v] -= s[u][v];
       }
     }
   }
@@ -91,35 +123,53 @@ bool cholesky(std::vector<double>& A, int n) {
 // From the Cholesky factor L (lower triangle of A): inv = (L L^T)^-1 =
 // L^-T L^-1.  U = L^-T is formed row by row in the upper triangle of A (the
 // diagonal of L kept aside), then inv[a][b] = sum_{i >= max(a,b)} U[a][i] U[b][i].
+//
+// Both phases are memory-bound dot products over long rows.  A task owns a
+// tile of consecutive rows (of U in the first phase, of the result in the
+// second) and walks the streamed rows once for the whole tile, so each
+// streamed row is read once per tile instead of once per row; every dot
+// product is the same loop as row by row, so the result does not depend on
+// the tiling.
 void cholesky_inverse(std::vector<double>& A, int n, std::vector<double>& inv) {
+  constexpr int kTileU = 16, kTileInv = 32;
   double* a = A.data();
   std::vector<double> ld(n), ud(n);
-  for (int i = 0; i < n; i++) ld[i] = a[(size_t)i * n + i];
+  for (int i = 0; i < n; i++) {
+    ld[i] = a[(size_t)i * n + i];
+    ud[i] = 1.0 / ld[i];
+  }
   // U[j][i] = (delta_ij - sum_{k=j}^{i-1} L[i][k] U[j][k]) / L[i][i], i >= j
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int j = 0; j < n; j++) {
-    double* uj = a + (size_t)j * n;  // U[j][i] stored at A[j][i] (i > j)
-    ud[j] = 1.0 / ld[j];
-    for (int i = j + 1; i < n; i++) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int j0 = 0; j0 < n; j0 += kTileU) {
+    const int j1 = std::min(n, j0 + kTileU);
+    for (int i = j0 + 1; i < n; i++) {
       const double* li = a + (size_t)i * n;
-      double s = li[j] * ud[j];
+      const int je = std::min(j1, i);
+      for (int j = j0; j < je; j++) {
+        double* uj = a + (size_t)j * n;  // U[j][i] stored at A[j][i] (i > j)
+        double s = li[j] * ud[j];
 #pragma omp simd reduction(+ : s)
-      for (int k = j + 1; k < i; k++) s += li[k] * uj[k];
-      uj[i] = -s / ld[i];
+        for (int k = j + 1; k < i; k++) s += li[k] * uj[k];
+        uj[i] = -s / ld[i];
+      }
     }
   }
   inv.assign((size_t)n * n, 0.0);
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int r = 0; r < n; r++) {
-    const double* ur = a + (size_t)r * n;
-    for (int c = r; c < n; c++) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int r0 = 0; r0 < n; r0 += kTileInv) {
+    const int r1 = std::min(n, r0 + kTileInv);
+    for (int c = r0; c < n; c++) {
       const double* uc = a + (size_t)c * n;
-      // i = c contributes U[r][c] U[c][c]; i > c both off-diagonal
-      double s = (c == r ? ud[r] : ur[c]) * ud[c];
+      const int re = std::min(r1, c + 1);
+      for (int r = r0; r < re; r++) {
+        const double* ur = a + (size_t)r * n;
+        // i = c contributes U[r][c] U[c][c]; i > c both off-diagonal
+        double s = (c == r ? ud[r] : ur[c]) * ud[c];
 #pragma omp simd reduction(+ : s)
-      for (int i = c + 1; i < n; i++) s += ur[i] * uc[i];
-      inv[(size_t)r * n + c] = s;
-      inv[(size_t)c * n + r] = s;
+        for (int i = c + 1; i < n; i++) s += ur[i] * uc[i];
+        inv[(size_t)r * n + c] = s;
+        inv[(size_t)c * n + r] = s;
+      }
     }
   }
 }
