@@ -134,6 +134,12 @@ struct Oracle {
   CgStats last_cg;
   long cg_total_its = 0;
   int last_iters = 0;
+  // Run logs for comparison with the reference's screen output: CG
+  // iterations of every pressure solve ("MKL_CG converged after N
+  // iterations.", BCH.cpp:4032) and one monitor row per time step
+  // (timeN, iter, timeT, u, v, w, p, maxAcc; BCH.cpp:3091-3093).
+  std::vector<int> cg_log;
+  std::vector<double> mon_log;
 
   // ------------------------------------------------------------------------
   // readInputFile, BCH.cpp:528-725.  Same token semantics: every header value
@@ -997,6 +1003,7 @@ struct Oracle {
       std::fill(x, x + n, 0.0);
       st.relres = 0;
       last_cg = st;
+      cg_log.push_back(0);
       return st;
     }
     double tol = cg_rtol * bnorm;
@@ -1028,6 +1035,7 @@ struct Oracle {
     st.relres = rn / bnorm;
     last_cg = st;
     cg_total_its += it;
+    cg_log.push_back(it);
     return st;
   }
 
@@ -1118,6 +1126,9 @@ struct Oracle {
     }
     last_iters = iter;
     bool steady = endStep();
+    const double row[8] = {(double)timeN, (double)iter, timeT, Un[monPoint], Un[NN + monPoint],
+                           Un[2 * (size_t)NN + monPoint], Pn[monPoint], maxAcc};
+    mon_log.insert(mon_log.end(), row, row + 8);
     if (print_monitor)
       printf("%6d  %6d  %10.5f  %12.5f  %12.5f  %12.5f  %12.5f %12.5f %12.5f\n", timeN, iter, timeT,
              Un[monPoint], Un[NN + monPoint], Un[2 * (size_t)NN + monPoint], Pn[monPoint], 0.0, maxAcc);
@@ -1418,6 +1429,16 @@ int orc_run(void* h, int nsteps, double* info) {
     info[3] = steady; info[4] = o->maxAcc;
   }
   return steps;
+}
+
+// Sizes of the run logs (out[0] pressure solves, out[1] time steps) and,
+// when the arrays are non-NULL, their contents; clear != 0 empties them.
+void orc_logs(void* h, long* sizes, int* cg, double* mon, int clear) {
+  Oracle* o = static_cast<Oracle*>(h);
+  if (sizes) { sizes[0] = (long)o->cg_log.size(); sizes[1] = (long)(o->mon_log.size() / 8); }
+  if (cg) std::copy(o->cg_log.begin(), o->cg_log.end(), cg);
+  if (mon) std::copy(o->mon_log.begin(), o->mon_log.end(), mon);
+  if (clear) { o->cg_log.clear(); o->mon_log.clear(); }
 }
 
 int orc_time(void* h, int* timeN, double* timeT) {

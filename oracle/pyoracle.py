@@ -70,6 +70,7 @@ def lib():
         L.orc_run.restype = C.c_int
         L.orc_run.argtypes = [vp, C.c_int, dp]
         L.orc_time.argtypes = [vp, ip, dp]
+        L.orc_logs.argtypes = [vp, lp, ip, dp, C.c_int]
         L.orc_write_tecplot.restype = C.c_int
         L.orc_write_tecplot.argtypes = [vp, C.c_char_p, C.c_char_p]
         L.orc_read_restart.restype = C.c_int
@@ -248,6 +249,16 @@ class Oracle:
         self.L.orc_run(self.h, nsteps, _p(info, C.c_double))
         return dict(steps=int(info[0]), cg_its=int(info[1]), subits=int(info[2]), steady=bool(info[3]),
                     max_acc=float(info[4]))
+
+    def logs(self, clear: bool = False):
+        """(CG iterations of every pressure solve, monitor rows per time
+        step [timeN, iter, timeT, u, v, w, p, maxAcc]) since the last clear."""
+        n = np.zeros(2, dtype=np.int64)
+        self.L.orc_logs(self.h, _p(n, C.c_long), None, None, 0)
+        cg = np.zeros(int(n[0]), dtype=np.int32)
+        mon = np.zeros((int(n[1]), 8))
+        self.L.orc_logs(self.h, None, _p(cg, C.c_int), _p(mon, C.c_double), 1 if clear else 0)
+        return cg, mon
 
     def time(self):
         n, t = C.c_int(0), C.c_double(0)

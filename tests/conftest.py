@@ -10,11 +10,16 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "cfd-with-cuda_b200")
-for p in (PKG, os.path.join(ROOT, "oracle")):
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+for p in (PKG, os.path.join(ROOT, "oracle"), GOLDEN):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE_DECK = "/root/reference/inputFiles/lidDrivenCavity/lidDrivenCavity_NE27000.inp"
+import ref_cases  # noqa: E402
+
+# The reference's shipped 30^3 deck is not part of this repository: tests
+# that read it find it under $CFD_REFERENCE_DIR and skip without it.
+REFERENCE_DECK = os.path.join(os.environ.get("CFD_REFERENCE_DIR", "/nonexistent"), ref_cases.SHIPPED_REL)
 
 
 def pytest_configure(config):
@@ -29,32 +34,7 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
-def perturbed_box(nx, ny, nz, amp, seed):
-    """Corner nodes of an nx x ny x nz box with interior nodes moved by a
-    seeded random offset (non-affine elements exercise the full Jacobian)."""
-    from cfdfs import meshgen
-    m = (nx + 1, ny + 1, nz + 1)
-    k, j, i = np.meshgrid(np.arange(m[2]), np.arange(m[1]), np.arange(m[0]), indexing="ij")
-    xyz = np.stack([i.ravel() / nx, j.ravel() / ny, k.ravel() / nz], axis=1).astype(np.float64)
-    rng = np.random.default_rng(seed)
-    interior = (i.ravel() > 0) & (i.ravel() < nx) & (j.ravel() > 0) & (j.ravel() < ny) & (k.ravel() > 0) & \
-               (k.ravel() < nz)
-    h = min(1.0 / nx, 1.0 / ny, 1.0 / nz)
-    xyz[interior] += rng.uniform(-amp * h, amp * h, size=(interior.sum(), 3))
-    xyz = np.round(xyz, 9)
-    ek, ej, ei = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
-    ei, ej, ek = ei.ravel(), ej.ravel(), ek.ravel()
-    node = lambda a, b, c: a + m[0] * b + m[0] * m[1] * c
-    conn = np.stack([node(ei, ej, ek), node(ei + 1, ej, ek), node(ei + 1, ej + 1, ek), node(ei, ej + 1, ek),
-                     node(ei, ej, ek + 1), node(ei + 1, ej, ek + 1), node(ei + 1, ej + 1, ek + 1),
-                     node(ei, ej + 1, ek + 1)], axis=1)
-    eid = np.arange(nx * ny * nz) + 1
-    faces = []
-    for face, sel, bc in ((1, ek == 0, 1), (5, ei == 0, 1), (3, ei == nx - 1, 1), (2, ej == 0, 1),
-                          (4, ej == ny - 1, 1), (6, ek == nz - 1, 2)):
-        e = eid[sel]
-        faces.append(np.stack([e, np.full_like(e, face), np.full_like(e, bc)], axis=1))
-    return xyz, conn, np.concatenate(faces)
+perturbed_box = ref_cases.perturbed_box
 
 
 @pytest.fixture(scope="session")

@@ -26,5 +26,7 @@ def test_bench_line_from_stand_in_solver():
     assert line["config"]["workload"].startswith("lid-driven cavity")
     assert line["e2e"]["h2d_bytes_per_step"] == line["e2e"]["d2h_bytes_per_step"] > 0
     sr = line["step_roofline"]
-    assert sr["bytes_per_step"] > 0 and sr["frac"] == pytest.approx(sr["achieved"] / sr["peak"], rel=1e-3)
+    # achieved is printed to 0.1 GB/s
+    assert sr["bytes_per_step"] > 0 and abs(sr["frac"] * sr["peak"] - sr["achieved"]) <= 0.05 + 1e-3 * sr["achieved"]
+    assert line["e2e"]["steps"] == line["steps"]
     assert line["roofline"]["kernel"] == "spmv_z"
