@@ -128,6 +128,7 @@ _PROTOS = {
     "cfd_launch_count": (C.c_longlong, [_vp]),
     "cfd_profile": (C.c_int, [_vp, C.c_int]),
     "cfd_profile_read": (C.c_int, [_vp, _dp]),
+    "cfd_profile_fcg2l": (C.c_int, [_vp, _dp]),
     "cfd_selftest_wait_timeout": (C.c_int, [_vp, C.c_int]),
     "cfd_pcg_solve_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_double, C.c_int, _vp, _dp,
                                         C.c_char_p, C.c_int]),
@@ -501,7 +502,7 @@ class Solver:
 
     # ---- timing / counters ----
     KCLASS = ["convect", "step1", "gt", "pcg64", "pcg32", "resid64", "step3", "spmv_k3", "pupdate", "other",
-              "unet", "fcg", "coarse", "spmv_z"]
+              "unet", "fcg", "coarse", "spmv_z", "fcg2l"]
 
     @property
     def stream_ptr(self) -> int:
@@ -519,6 +520,15 @@ class Solver:
         return {k: dict(launches=int(out[3 * i]), ms=float(out[3 * i + 1]), iters=int(out[3 * i + 2]))
                 for i, k in enumerate(self.KCLASS)}
 
+
+    FCG2L_PHASES = ["restrict", "coarse", "zphase", "nbwait", "spmv", "dotwait", "update"]
+
+    def profile_fcg2l(self) -> dict:
+        """Phase times (ms, first block, summed) of the persistent two-level
+        iteration while profiling was on."""
+        out = np.zeros(7)
+        self._check(self.L.cfd_profile_fcg2l(self.h, _p(out, C.c_double)))
+        return dict(zip(self.FCG2L_PHASES, out.tolist()))
     def selftest_wait_timeout(self, ms: int) -> int:
         return int(self.L.cfd_selftest_wait_timeout(self.h, ms))
 

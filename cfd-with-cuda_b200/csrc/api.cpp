@@ -133,7 +133,8 @@ struct cfd_ctx {
   DevBuf<double4> vbuf[12];
   // CFD_MIXED: float4 copies of the gathered velocity vectors (Un,
   // UnpHalf_prev, UnpHalf, Acc_prev, Acc, d)
-  DevBuf<float4> fbuf[6];
+  DevBuf<float4> fbuf[7];
+  float4* r1c32 = nullptr;  // CFD_MIXED: the convection term accumulated in FP32
   float4 *un32 = nullptr, *uphp32 = nullptr, *uph32 = nullptr, *accp32 = nullptr, *acc32 = nullptr,
          *d32 = nullptr;
   double4 *un = nullptr, *unp1 = nullptr, *unp1_prev = nullptr, *unphalf = nullptr, *unphalf_prev = nullptr,
@@ -193,6 +194,15 @@ struct cfd_ctx {
       for (auto& gq : gp)
         for (auto& g : gq) g.reset();
   }
+  // persistent two-level iteration (fcg_persist.cu) for the FP32 inner
+  // solves on a structured grid; CFD_FCG_PERSIST=0 replays the per-kernel
+  // iteration graphs instead
+  bool fcg_persist = true;
+  int fcg2l_g = 0;                  // co-resident blocks of the launch
+  int fcg2l_key[3] = {0, 0, 0};     // n, blocks, reach of the neighbour ranges in fcg2l_nb
+  DevBuf<unsigned> fcg2l_sync;      // arrival counter + per-block progress
+  DevBuf<int> fcg2l_nb;             // [lo (blocks), hi (blocks)]
+  DevBuf<double> fcg2l_part, fcg2l_time;
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
 
@@ -420,6 +430,7 @@ int upload_problem(cfd_ctx* c) {
     }
     c->un32 = c->fbuf[0].p; c->uphp32 = c->fbuf[1].p; c->uph32 = c->fbuf[2].p;
     c->accp32 = c->fbuf[3].p; c->acc32 = c->fbuf[4].p; c->d32 = c->fbuf[5].p;
+    c->r1c32 = c->fbuf[6].p;
   }
   for (auto& b : c->pbuf) {
     CU(b.alloc(NNp));
@@ -706,6 +717,56 @@ CoarseArgs<VT> coarse_args(const cfd_ctx* c, bool with_coarse) {
   return a;
 }
 
+// Whether the persistent two-level iteration serves an FP32 solve with these
+// arguments (identity-numbered structured grid with the structured form of
+// Z, a window of at most 4 directions, the coarse space's limits).
+bool fcg2l_fits(const cfd_ctx* c, const FcgArgs<float>& a, const CoarseArgs<float>& ca) {
+  if (!c->fcg_persist || !a.stencil || ca.pmap || a.st.m < 1 || a.st.m > 4) return false;
+  if ((long long)ca.fd[0] * ca.fd[1] * ca.fd[2] != a.n || ca.fd[0] > 512) return false;
+  if (ca.ldinv % 8 || (size_t)ca.ldinv * sizeof(float) > fcg2l_smem_bytes()) return false;
+  for (int ax = 1; ax < 3; ax++) {
+    const double h = ca.cd[ax] > 1 ? (double)(ca.fd[ax] - 1) / (ca.cd[ax] - 1) : 1.0;
+    if ((2 * h + 1) * (2 * h + 1) > 1024) return false;
+  }
+  return true;
+}
+
+// The remaining iterations of an FP32 flexible-CG solve in one persistent
+// launch (the start kernel and any network iterations ran before).
+int run_fcg2l(cfd_ctx* c, const FcgArgs<float>& a, const CoarseArgs<float>& ca) {
+  cudaStream_t s = c->stream;
+  if (!c->fcg2l_g) c->fcg2l_g = fcg2l_grid(c->device);
+  const int G = c->fcg2l_g;
+  NEED(G > 0, "no co-resident grid for the persistent two-level iteration");
+  const int reach = 2 + 2 * a.fd[0] + 2 * a.fd[0] * a.fd[1];
+  if (c->fcg2l_key[0] != a.n || c->fcg2l_key[1] != G || c->fcg2l_key[2] != reach) {
+    std::vector<int> nb(2 * (size_t)G);
+    fcg2l_neighbor_ranges(a.n, G, reach, nb.data(), nb.data() + G);
+    CU(c->fcg2l_nb.alloc(nb.size()));
+    CU(cudaMemcpy(c->fcg2l_nb.p, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CU(c->fcg2l_sync.alloc(1 + (size_t)G));
+    CU(c->fcg2l_part.alloc(fcg2l_part_words(G)));
+    if (!c->fcg2l_time.p) {
+      CU(c->fcg2l_time.alloc(8));
+      CU(cudaMemset(c->fcg2l_time.p, 0, 8 * sizeof(double)));
+    }
+    c->fcg2l_key[0] = a.n;
+    c->fcg2l_key[1] = G;
+    c->fcg2l_key[2] = reach;
+  }
+  CU(cudaMemsetAsync(c->fcg2l_sync.p, 0, (1 + (size_t)G) * sizeof(unsigned), s));
+  Fcg2lArgs pa{};
+  pa.c = c->cs_c32.p;
+  pa.e = c->cs_e32.p;
+  pa.sync = c->fcg2l_sync.p;
+  pa.nb_lo = c->fcg2l_nb.p;
+  pa.nb_hi = c->fcg2l_nb.p + G;
+  pa.part = c->fcg2l_part.p;
+  pa.timing = c->prof_on ? c->fcg2l_time.p : nullptr;
+  KL(CFD_K_FCG2L, launch_fcg2l(a, ca, pa, G, s));
+  return CFD_OK;
+}
+
 // Flexible CG with the two-level preconditioner (Jacobi step + coarse-space
 // correction) and, for CFD_PC_LEARNED, the attached U-Net's correction.
 // VT = float: b, x are f_b, f_x and the FP32 SELL values (inner solve of
@@ -797,10 +858,10 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   // start kernels leave D^-1 r in z1).  Iterations with the network keep
   // the sequential form: its correction would need a second SpMV.
   const bool split = sizeof(VT) == 4 && a.stencil && c->cs_zp_ok && !pmap && c->fcg_split;
+  a.dinv = dinv;
   if (split) {
     if (!c->fcg_z1.p) CU(c->fcg_z1.alloc(n));
     a.z1 = reinterpret_cast<VT*>(c->fcg_z1.p);
-    a.dinv = dinv;
   }
   KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
   const CoarseArgs<VT> ca = coarse_args<VT>(c, true);
@@ -911,9 +972,13 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   };
   const bool net_all = net_iters >= (1 << 30);
   const int head = net_all ? 0 : net_iters;  // iterations of the network-only head
+  // after the head, the two-level iterations run in one persistent launch
+  // where that applies
+  bool persist = false;
+  if constexpr (sizeof(VT) == 4) persist = !net_all && !split && fcg2l_fits(c, a, ca);
   FcgGraph *G = nullptr, *GH = nullptr;
   {
-    int rc = graph_for(net_all, kFcgBatch, G);
+    int rc = persist ? CFD_OK : graph_for(net_all, kFcgBatch, G);
     if (rc) return rc;
     if (head > 0) {
       rc = graph_for(true, std::min(head, kFcgBatch), GH);
@@ -938,7 +1003,16 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
       issued += hb;
     }
   }
-  for (;;) {
+  if constexpr (sizeof(VT) == 4) {
+    if (persist) {
+      int rc = run_fcg2l(c, a, ca);
+      if (rc) return rc;
+      CU(cudaMemcpyAsync(c->h_small, c->fcg_sc.p, kFcgScalars * sizeof(double), cudaMemcpyDeviceToHost, s));
+      CU(cudaStreamSynchronize(s));
+      if (c->prof_on) c->prof[CFD_K_FCG2L][2] += c->h_small[kFcgIt] - issued;
+    }
+  }
+  for (; !persist;) {
     if (G) {
       const int reps = (batch + kFcgBatch - 1) / kFcgBatch;
       for (int k = 0; k < reps; k++) {
@@ -971,7 +1045,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   res[0] = h[kFcgIt];
   res[1] = h[kFcgBB] > 0 ? std::sqrt(h[kFcgRR] / h[kFcgBB]) : 0.0;
   res[2] = h[kFcgStatus] < 0 ? 1 : h[kFcgStatus];
-  if (c->prof_on) {
+  if (c->prof_on && !persist) {
     c->prof[CFD_K_FCG][2] += res[0];
     c->prof[CFD_K_SPMV_Z][2] += res[0];
   }
@@ -1134,6 +1208,7 @@ int cfd_create(cfd_ctx** out, int device) {
     return CFD_E_CUDA;
   if (cudaMallocHost((void**)&c->h_small, 64 * sizeof(double)) != cudaSuccess) return CFD_E_CUDA;
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_FCG_PERSIST")) c->fcg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_ANCHOR")) c->fcg_anchor = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_SPLIT_SPMV_PER_SM")) c->split_spmv_per_sm = std::atoi(e) == 1 ? 1 : 2;
@@ -1329,7 +1404,10 @@ int cfd_convect(cfd_ctx* c) {
   if (!c) return CFD_E_BADARG;
   NEED(c->assembled, "cfd_convect before cfd_step0");
   cudaStream_t s = c->stream;
-  CU(cudaMemsetAsync(c->r1conv, 0, c->P.NN * sizeof(double4), s));
+  if (mixed(c))
+    CU(cudaMemsetAsync(c->r1c32, 0, c->P.NN * sizeof(float4), s));
+  else
+    CU(cudaMemsetAsync(c->r1conv, 0, c->P.NN * sizeof(double4), s));
   NEED(!c->opt.deterministic || !c->color_off.empty(),
        "deterministic mode: the mesh needs more than 64 element colours");
   auto run = [&](auto a, auto launch) -> int {
@@ -1350,6 +1428,7 @@ int cfd_convect(cfd_ctx* c) {
   };
   if (mixed(c)) {
     ConvArgs<float> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un32, c->uphp32, c->r1conv};
+    a.r1f = c->r1c32;
     return run(a, [&](const ConvArgs<float>& x) { return launch_convect<float>(x, c->num_sms, s); });
   }
   ConvArgs<double> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};
@@ -1371,6 +1450,7 @@ int cfd_step1(cfd_ctx* c, int iter) {
     Step1Args<float> a{};
     fill(a);
     a.uprev = c->uphp32; a.unphalf_g = c->uph32; a.d_g = c->d32;
+    a.r1conv32 = c->r1c32;
     a.kval = c->ks_val32.p; a.g1 = c->gs1_32.p; a.g2 = c->gs2_32.p; a.g3 = c->gs3_32.p;
     KL(CFD_K_STEP1, launch_step1<float>(a, c->num_sms, s));
   } else {
@@ -1727,8 +1807,20 @@ int cfd_profile(cfd_ctx* c, int on) {
   cudaStream_t s = c->stream;
   CU(cudaStreamSynchronize(s));
   harvest(c);
-  if (on) std::memset(c->prof, 0, sizeof(c->prof));
+  if (on) {
+    std::memset(c->prof, 0, sizeof(c->prof));
+    if (c->fcg2l_time.p) CU(cudaMemset(c->fcg2l_time.p, 0, 8 * sizeof(double)));
+  }
   c->prof_on = on != 0;
+  return CFD_OK;
+}
+
+int cfd_profile_fcg2l(cfd_ctx* c, double* out7) {
+  if (!c || !out7) return CFD_E_BADARG;
+  CU(cudaStreamSynchronize(c->stream));
+  double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (c->fcg2l_time.p) CU(cudaMemcpy(t, c->fcg2l_time.p, sizeof(t), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 7; k++) out7[k] = t[k] * 1e-6;
   return CFD_OK;
 }
 

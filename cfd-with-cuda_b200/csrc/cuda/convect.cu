@@ -11,8 +11,10 @@
 // with grad(uprev^d)(k) = J_k^{-1} (sum_j dSv_j(k) uprev_j^d), J_k rebuilt
 // from the 8 corner coordinates.  One thread per (element, Gauss point);
 // elements and their gathered nodal values sit in shared memory; results are
-// scattered with FP64 atomics (no element colouring), or, in deterministic
-// mode, one colour per launch with plain adds in a fixed order.  Work per element is
+// scattered with FP64 atomics (no element colouring; in mixed precision as
+// one FP32 16-byte vector reduction per element node into an FP32 copy of
+// the term), or, in deterministic mode, one colour per launch with plain
+// adds in a fixed order.  Work per element is
 // about 30x fewer flops than the Ae form, so the kernel is bound by the
 // gathers of Un / UnpHalf_prev and the atomic scatter, not by arithmetic.
 #include "kernels.h"
@@ -22,6 +24,13 @@ namespace cfd {
 namespace {
 
 constexpr int kConvThreads = 128;
+
+// *p += (x, y, z, w) as one 16-byte vector reduction in L2 (sm_90 and newer)
+__device__ __forceinline__ void red_add_v4_f32(float4* p, float x, float y, float z, float w) {
+  asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(x), "f"(y), "f"(z),
+               "f"(w)
+               : "memory");
+}
 
 // Four values of T read from shared memory by one vector load.
 template <class T>
@@ -144,6 +153,21 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
           s0 += sv * ck.x;
           s1 += sv * ck.y;
           s2 += sv * ck.z;
+        }
+        if constexpr (sizeof(T) == 4) {
+          if (a.r1f) {
+            float4* df = a.r1f + lt[el][i];
+            if (a.plain) {
+              float4 o = *df;
+              o.x -= (float)s0;
+              o.y -= (float)s1;
+              o.z -= (float)s2;
+              *df = o;
+            } else {
+              red_add_v4_f32(df, -(float)s0, -(float)s1, -(float)s2, 0.f);
+            }
+            continue;
+          }
         }
         double4* dst = a.r1 + lt[el][i];
         if (a.plain) {  // one colour per launch: no other element of it touches this node

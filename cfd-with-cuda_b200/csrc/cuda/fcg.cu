@@ -22,32 +22,13 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "fcg_common.cuh"
 #include "kernels.h"
 #include "sell_stream.cuh"
 
 namespace cfd {
 
 namespace {
-
-constexpr int kFcgThreads = 256;
-// partial sums per block of an SpMV kernel instantiated for at most MD
-// stored directions: (z,w), (z,r), (z,q_j), (p_j,r)
-template <int MD>
-__host__ __device__ constexpr int fcg_parts() {
-  return 2 + 2 * MD;
-}
-constexpr int kFcgParts = fcg_parts<kFcgMaxM>();
-
-template <class VT>
-__device__ __forceinline__ VT sell_row(const int* __restrict__ off, const int* __restrict__ col,
-                                       const VT* __restrict__ val, const VT* __restrict__ x, int i) {
-  const int s = i >> 5, l = i & 31;
-  const int bb = __ldg(off + s) + l, w = (__ldg(off + s + 1) - __ldg(off + s)) >> 5;
-  VT q = 0;
-#pragma unroll 4
-  for (int j = 0; j < w; j++) q += __ldcs(val + bb + 32 * j) * __ldg(x + __ldcs(col + bb + 32 * j));
-  return q;
-}
 
 // Stores this block's NV partials, and returns true in every thread of the
 // block that finished last (its thread 0 has re-armed the counter); the
@@ -79,25 +60,6 @@ __device__ __forceinline__ void gather_partials(const double* part, int nblk, do
 #pragma unroll
     for (int k = 0; k < NV; k++) v[k] += __ldcg(part + NV * b + k);
   block_sum<NV>(v);
-}
-
-// Per-row part of the SpMV kernels: w[i] and the dot products of the
-// iteration (z,w) (z,r) (z,q_j) (p_j,r), accumulated into v.
-template <int MD, class VT>
-__device__ __forceinline__ void fcg_row_dots(const FcgArgs<VT>& a, int i, VT zv, VT wi, int nd,
-                                             double (&v)[fcg_parts<MD>()]) {
-  const size_t n = (size_t)a.n;
-  a.w[i] = wi;
-  const double zi = zv, ri = a.r[i];
-  v[0] += zi * (double)wi;
-  v[1] += zi * ri;
-#pragma unroll
-  for (int j = 0; j < MD; j++) {
-    if (j < nd) {
-      v[2 + j] += zi * (double)a.q[j * n + i];
-      v[2 + MD + j] += (double)a.p[j * n + i] * ri;
-    }
-  }
 }
 
 // Block sums of the SpMV's partials; the last block to finish forms the
@@ -244,48 +206,6 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
   fcg_spmv_finish<MD>(a, v, nd, m, it);
 }
 
-// w = Z z on a structured grid of pressure nodes (identity numbering, node
-// x + fx (y + fy z)): Z couples nodes within two grid steps per axis, so a
-// row is 125 coefficients.  They are stored per 32-row slice, tap-major
-// inside the slice (coef[slice][tap][lane], zero for couplings that do not
-// exist): no column indices are streamed, and the gathers of z are
-// contiguous across the warp.  Each warp owns a contiguous range of slices
-// and streams it through shared memory in chunks of 25 taps (one dz plane,
-// 3.2 KB), two chunks in flight per warp on bulk asynchronous copies.  Taps
-// that leave the grid have zero coefficients.  Slices whose every tap stays
-// inside [0, n) read z at i + dx + fx dy + fxy dz directly (five row
-// pointers per plane, dx folded into the load offsets); the few slices
-// within two planes of either end clamp the index.
-constexpr int kStTaps = 25;
-constexpr int kStBuf = 2;
-template <class VT>
-constexpr size_t stencil_smem_bytes() {
-  return (size_t)kPcgWarps * kStBuf * (kStTaps * 32 * sizeof(VT) + sizeof(unsigned long long));
-}
-
-// One dz plane of a row (25 taps, coefficients q[t * 32] in shared memory)
-// into the five per-dy accumulators.
-template <bool CLAMP, class VT>
-__device__ __forceinline__ void stencil_plane(const VT* q, const VT* __restrict__ z, int base, int fx, int n,
-                                              VT (&acc)[5]) {
-#pragma unroll
-  for (int dy = -2; dy <= 2; dy++) {
-    const int rb = base + fx * dy;
-#pragma unroll
-    for (int dx = -2; dx <= 2; dx++) {
-      VT zv;
-      if constexpr (CLAMP) {
-        int j = rb + dx;
-        j = j < 0 ? 0 : (j >= n ? n - 1 : j);
-        zv = __ldg(z + j);
-      } else {
-        zv = __ldg(z + rb + dx);
-      }
-      acc[dy + 2] += q[((dy + 2) * 5 + dx + 2) * 32] * zv;
-    }
-  }
-}
-
 // DOTS = false: w = Z z only (the Jacobi part of the split iteration).
 template <class VT, int MD, bool DOTS>
 __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT> a) {
@@ -335,7 +255,10 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT>
     VT acc[5] = {0, 0, 0, 0, 0};
     for (int dz = -2; dz <= 2; dz++, k++) {
       const int b = k % kStBuf;
-      if (ok && !mbar_wait_bounded(mbar + b, (unsigned)((k / kStBuf) & 1), a.st.timeout_ns)) {
+      // the gathers below shuffle across the warp: every lane takes the
+      // same branch, so the outcome of the wait is made warp-uniform
+      if (ok && !__all_sync(0xffffffffu, mbar_wait_bounded(mbar + b, (unsigned)((k / kStBuf) & 1),
+                                                           a.st.timeout_ns))) {
         ok = false;
         kfail = k;
         if (lane == 0) atomicExch(a.st.err, 1);
@@ -343,9 +266,9 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT>
       if (ok) {
         const VT* q = buf + (size_t)b * kStTaps * 32 + lane;
         if (inside)
-          stencil_plane<false>(q, z, i + fxy * dz, fx, n, acc);
+          stencil_plane_shfl<false, true>(q, z, i + fxy * dz, fx, n, lane, acc);
         else
-          stencil_plane<true>(q, z, i + fxy * dz, fx, n, acc);
+          stencil_plane_shfl<true, true>(q, z, i + fxy * dz, fx, n, lane, acc);
       }
       __syncwarp();
       if (ok) issue(k + kStBuf);

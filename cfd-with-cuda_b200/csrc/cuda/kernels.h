@@ -91,6 +91,10 @@ struct ConvArgs {
   double4* r1;           // accumulates -A(un) uprev (zeroed by the caller)
   const int* elist;      // element range and plain scatter as in AsmArgs
   int e_begin, e_end, plain;
+  // T = float only, may be null: accumulate into this FP32 copy instead of
+  // r1 (zeroed by the caller; w stays 0), one 16-byte vector reduction per
+  // element node instead of three FP64 atomics
+  float4* r1f;
 };
 template <class T>
 cudaError_t launch_convect(const ConvArgs<T>& a, int num_sms, cudaStream_t s);
@@ -105,6 +109,7 @@ struct Step1Args {
   const VT *g1, *g2, *g3;
   const GVec<VT>* uprev;  // UnpHalf_prev, gathered by K
   const double4 *un, *r1conv, *kacc;
+  const float4* r1conv32;  // may be null: the FP32 convection term, read instead of r1conv
   const double *pn, *minv_free, *minv_orig;
   double4 *unphalf, *d, *r1out;  // r1out may be null
   GVec<VT>* unphalf_g;           // float4 copies of UnpHalf and d (VT = float)
@@ -286,6 +291,28 @@ template <class VT> cudaError_t launch_fcg_spmv_jacobi(const FcgArgs<VT>& a, cud
 template <class VT>
 cudaError_t launch_fcg_combine(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, const float* wst, const int* wlo,
                                const VT* e, cudaStream_t s);
+
+// Persistent two-level flexible CG (fcg_persist.cu): the remaining
+// iterations of an FP32 inner solve that the start kernel (and any network
+// iterations) began, in one cooperative launch, for an identity-numbered
+// structured grid with the structured form of Z and the coarse space; m
+// (the direction window) at most 4.  The solve's state words are read from
+// and written back to a.st.sc; a.dinv is the FP32 Jacobi diagonal.
+struct Fcg2lArgs {
+  float* c;                  // coarse restriction, nc entries
+  float* e;                  // coarse solution, nc entries
+  unsigned* sync;            // 1 + grid words, zeroed before each launch: arrival counter, block progress
+  const int *nb_lo, *nb_hi;  // per block: first and last block owning a row its SpMV gathers
+  double* part;              // 2 x fcg2l_part_words / 2 partial sums
+  double* timing;            // may be null: 7 phase times (ns) of block 0 added per launch
+};
+size_t fcg2l_smem_bytes();
+int fcg2l_grid(int device);                                    // co-resident blocks of the launch
+inline int fcg2l_part_words(int grid) { return 2 * (2 + 2 * 4) * grid; }
+// blocks each block waits for: rows within `reach` of its own
+void fcg2l_neighbor_ranges(int n, int grid, int reach, int* lo, int* hi);
+cudaError_t launch_fcg2l(const FcgArgs<float>& a, const CoarseArgs<float>& ca, const Fcg2lArgs& pa, int grid,
+                         cudaStream_t s);
 
 void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi);
 template <class VT>

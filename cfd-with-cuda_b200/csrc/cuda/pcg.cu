@@ -61,12 +61,13 @@ struct BlockSync {
         while (true) {
           if (!done) done = ld_acquire_gpu(prog + j) >= k;
           if (__all_sync(0xffffffffu, done)) break;
-          if (ld_volatile_i32(err) || global_ns() - t0 > timeout_ns) {
+          // the whole warp gives up together: every lane takes the same
+          // sequence of warp-wide votes
+          if (__any_sync(0xffffffffu, ld_volatile_i32(err) != 0 || global_ns() - t0 > timeout_ns)) {
             good = 0;
             break;
           }
         }
-        good = __all_sync(0xffffffffu, good);
         if (!good) break;
       }
       __threadfence();

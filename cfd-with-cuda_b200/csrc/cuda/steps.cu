@@ -60,7 +60,13 @@ __global__ void __launch_bounds__(kRowThreads) k_step1(Step1Args<VT> a) {
       gz += __ldcs(a.g3 + b + l + 32 * j) * p;
     }
   }
-  const double4 rc = a.r1conv[row];
+  double4 rc;
+  if (a.r1conv32) {
+    const float4 f = a.r1conv32[row];
+    rc = make_double4(f.x, f.y, f.z, 0.0);
+  } else {
+    rc = a.r1conv[row];
+  }
   const double mf = a.minv_free[row];
   double rx = (rc.x - (double)kx) - (double)gx;
   double ry = (rc.y - (double)ky) - (double)gy;

@@ -300,13 +300,22 @@ long long cfd_launch_count(const cfd_ctx* ctx);
 
 enum cfd_kernel_class {
   CFD_K_CONVECT = 0, CFD_K_STEP1, CFD_K_GT, CFD_K_PCG64, CFD_K_PCG32, CFD_K_RESID64, CFD_K_STEP3,
-  CFD_K_SPMV_K3, CFD_K_PUPDATE, CFD_K_OTHER, CFD_K_UNET, CFD_K_FCG, CFD_K_COARSE, CFD_K_SPMV_Z, CFD_K_COUNT
+  CFD_K_SPMV_K3, CFD_K_PUPDATE, CFD_K_OTHER, CFD_K_UNET, CFD_K_FCG, CFD_K_COARSE, CFD_K_SPMV_Z, CFD_K_FCG2L,
+  CFD_K_COUNT
 };
 /* Per-kernel-class CUDA-event timing on the context stream (on = 1 starts
  * and clears, 0 stops).  out receives CFD_K_COUNT triples
  * {launches, total milliseconds, Krylov iterations inside those launches}. */
 int cfd_profile(cfd_ctx* ctx, int on);
 int cfd_profile_read(cfd_ctx* ctx, double* out);
+/* While profiling is on: the device time (milliseconds, read in the first
+ * block of the launch, summed over launches) of each phase of the
+ * persistent two-level iteration (class CFD_K_FCG2L): out7 = {restriction,
+ * coarse solve, preconditioned residual, neighbour wait, structured SpMV
+ * with its dot products, reduction of the dots, update with the (r,r)
+ * reduction}; each phase's time includes the wait that ends it.  No
+ * counterpart in the reference. */
+int cfd_profile_fcg2l(cfd_ctx* ctx, double* out7);
 
 /* Runs one small kernel whose bounded wait watches a flag nothing sets, with
  * the given limit in milliseconds.  Returns CFD_E_TIMEOUT when the wait gave
@@ -325,7 +334,10 @@ int cfd_selftest_wait_timeout(cfd_ctx* ctx, int timeout_ms);
  * every GPU that loads the library until exit), so n is limited to
  * CFD_NOALLOC_MAX_N; larger n returns CFD_E_BADARG with a message in errbuf.
  * The first call on a device looks the array up (once per device); make it
- * before any stream capture.  Calls share the array: calls that overlap on
+ * before any stream capture.  With CUDA's lazy module loading (the default)
+ * that first call is also when the array is placed on the device, so it
+ * needs 16.1 MiB free: a host that reserves device memory for its own pool
+ * should make one warm-up call (any small system) before it does.  Calls share the array: calls that overlap on
  * the GPU race and must not be issued.  info (may be NULL) receives
  * {iterations, ||r||/||b||, status}; returns CFD_OK, CFD_E_NOCONV,
  * CFD_E_NONFINITE, CFD_E_TIMEOUT, CFD_E_BADARG or CFD_E_CUDA. */

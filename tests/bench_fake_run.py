@@ -44,6 +44,8 @@ class StandInSolver:
     def profile(self, on): pass
     def close(self): pass
     def vector(self, name): return np.zeros(Info.NNp)
+    def profile_fcg2l(self): return dict(restrict=0.01, coarse=0.02, zphase=0.01, nbwait=0.0, spmv=0.2, dotwait=0.02,
+                                         update=0.03)
 
     def run(self, n):
         self.n += n

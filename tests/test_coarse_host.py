@@ -60,3 +60,34 @@ def test_coarse_lattice_limits():
     L.cfdh_coarse_inverse(cfdfs._p(d, C.c_int), cfdfs._p(rp, C.c_int), cfdfs._p(rp, C.c_int),
                           cfdfs._p(np.zeros(1), C.c_double), cfdfs._p(cd, C.c_int), None)
     assert int(np.prod(cd)) <= 6000
+
+
+def _laplace7(dims, shift):
+    """Shifted 7-point Laplacian on an x-fastest grid: a synthetic SPD Z."""
+    nx, ny, nz = dims
+    n = nx * ny * nz
+    idx = np.arange(n).reshape(nz, ny, nx)
+    rows, cols, vals = [idx.ravel()], [idx.ravel()], [np.full(n, 6.0 + shift)]
+    for ax in range(3):
+        a = np.moveaxis(idx, 2 - ax, 0)
+        lo, hi = a[:-1].ravel(), a[1:].ravel()
+        rows += [lo, hi]
+        cols += [hi, lo]
+        vals += [np.full(lo.size, -1.0), np.full(lo.size, -1.0)]
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+
+
+@pytest.mark.parametrize("dims", [(25, 25, 25), (29, 21, 17)])
+def test_coarse_inverse_multi_panel(dims):
+    """Coarse sizes of 343 and 240 nodes: more than one 96-column panel of
+    the blocked Cholesky, with edge tiles of the 4 x 4 register-tiled
+    trailing update and of the row-tiled inverse."""
+    import cfdfs
+    Z = _laplace7(dims, 0.05)
+    Z.sort_indices()
+    cd, inv = cfdfs.coarse_inverse(dims, Z.indptr.astype(np.int32), Z.indices.astype(np.int32), Z.data)
+    P = sp.kron(_hats(dims[2]), sp.kron(_hats(dims[1]), _hats(dims[0]))).tocsr()
+    assert cd == tuple(_hats(n).shape[1] for n in dims)
+    assert int(np.prod(cd)) > 96 * 2
+    ref = np.linalg.inv((P.T @ Z @ P).toarray())
+    assert rel_l2(inv, ref) < 1e-10

@@ -223,11 +223,13 @@ def test_failures_are_reported_not_hung(decks):
     s.close()
 
 
-def _det_run(path, steps, **kw):
+def _det_run(path, steps, weights=None, **kw):
     import cfdfs
     s = cfdfs.Solver(device=0, deterministic=1, **kw)
     s.load(path)
     s.step0()
+    if weights:
+        s.load_unet(weights)
     ops = [s.matrix(w)[2].copy() for w in ("K", "G", "Z")]
     st = s.run(steps)
     U, P = s.state()
@@ -266,3 +268,18 @@ def test_deterministic_mixed_twolevel(decks):
     _, st2, U2, P2 = _det_run(decks["c1"], 6, **kw)
     assert np.array_equal(U1, U2) and np.array_equal(P1, P2)
     assert st1.cg_iters == st2.cg_iters
+
+
+def test_deterministic_mixed_learned(decks):
+    """The mixed learned path (the committed network in the first iteration
+    of each pressure solve, flexible CG, Jacobi-PCG fallback on a stall) is
+    bitwise reproducible in deterministic mode: the same fallback decisions,
+    iteration counts and fields in two runs."""
+    import os
+    import cfdfs
+    w = os.path.join(os.path.dirname(cfdfs.__file__), "..", "weights", "unet_cavity.bin")
+    kw = dict(precision=cfdfs.MIXED, precond=cfdfs.PC_LEARNED, fcg_net_iters=1)
+    _, st1, U1, P1 = _det_run(decks["c1"], 8, weights=w, **kw)
+    _, st2, U2, P2 = _det_run(decks["c1"], 8, weights=w, **kw)
+    assert np.array_equal(U1, U2) and np.array_equal(P1, P2)
+    assert st1.cg_iters == st2.cg_iters and st1.fallbacks == st2.fallbacks

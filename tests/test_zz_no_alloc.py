@@ -42,10 +42,19 @@ def test_noalloc_solve_matches_context_solve(decks):
         b_t = torch.from_numpy(b).to(dev)
         x_t.fill_(123.0)                                    # output is fully overwritten
         torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(0)[0]
+        reserved_before = torch.cuda.memory_reserved(0)
         rc, info, msg = cfdfs.pcg_solve_noalloc(rp_t.data_ptr(), col_t.data_ptr(), val_t.data_ptr(),
                                                 dinv_t.data_ptr(), b_t.data_ptr(), x_t.data_ptr(), n,
                                                 1e-8, 1000, stream)
         assert rc == cfdfs.CFD_OK, msg
+        torch.cuda.synchronize()
+        # the property the entry point exists for: once its static array is
+        # on the device (the first call puts it there), a call allocates no
+        # device memory, neither through CUDA nor through torch's allocator
+        if call == 1:
+            assert torch.cuda.mem_get_info(0)[0] == free_before
+            assert torch.cuda.memory_reserved(0) == reserved_before
         x_ref, st = s.pressure_solve(b)
         assert st.status == 0
         assert rel_l2(x_t.cpu().numpy(), x_ref) < SOLVE_TOL, call
