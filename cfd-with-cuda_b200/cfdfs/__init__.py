@@ -129,6 +129,7 @@ _PROTOS = {
     "cfd_profile": (C.c_int, [_vp, C.c_int]),
     "cfd_profile_read": (C.c_int, [_vp, _dp]),
     "cfd_profile_fcg2l": (C.c_int, [_vp, _dp]),
+    "cfd_spd_inverse": (C.c_int, [C.c_int, _dp, C.c_int, _dp]),
     "cfd_selftest_wait_timeout": (C.c_int, [_vp, C.c_int]),
     "cfd_pcg_solve_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_double, C.c_int, _vp, _dp,
                                         C.c_char_p, C.c_int]),
@@ -686,6 +687,16 @@ def coarse_inverse(dims, rowptr, col, val):
 
 
 NOALLOC_MAX_N = 524288
+
+
+def spd_inverse(a, device: int = 0):
+    """Inverse of a dense SPD matrix, factored and inverted on the device."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    inv = np.zeros_like(a)
+    rc = lib().cfd_spd_inverse(device, _p(a, C.c_double), a.shape[0], _p(inv, C.c_double))
+    if rc != CFD_OK:
+        raise CfdError(rc, "cfd_spd_inverse failed")
+    return inv
 
 
 def pcg_solve_noalloc(rowptr, col, val, dinv, b, x, n, rtol=1e-8, maxit=1000, stream=0):

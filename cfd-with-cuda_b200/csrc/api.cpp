@@ -198,6 +198,8 @@ struct cfd_ctx {
   // solves on a structured grid; CFD_FCG_PERSIST=0 replays the per-kernel
   // iteration graphs instead
   bool fcg_persist = true;
+  // CFD_COARSE_HOST=1: factor and invert the coarse matrix on the host
+  bool coarse_on_host = false;
   int fcg2l_g = 0;                  // co-resident blocks of the launch
   int fcg2l_key[3] = {0, 0, 0};     // n, blocks, reach of the neighbour ranges in fcg2l_nb
   DevBuf<unsigned> fcg2l_sync;      // arrival counter + per-block progress
@@ -590,7 +592,10 @@ int ensure_coarse(cfd_ctx* c) {
   std::string err;
   // Z P for the split FP32 iteration (structured form, identity numbering)
   const bool want_zp = mixed(c) && c->h_pmap.empty();
-  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err, want_zp))
+  // the dense factorisation and inverse of Zc run on the device unless
+  // CFD_COARSE_HOST=1 keeps them on the host
+  const bool on_device = !c->coarse_on_host;
+  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err, want_zp, !on_device))
     return fail(c, CFD_E_NONFINITE, "%s", err.c_str());
   const int nc = cs.nc;
   for (int a = 0; a < 3; a++) {
@@ -633,16 +638,44 @@ int ensure_coarse(cfd_ctx* c) {
   // coarse correction only has to be close, and halving the bytes of the
   // one dense operand of the iteration matters more
   const int ld = (nc + 7) & ~7;
-  double amax = 0.0;
-  for (double v : cs.inv) amax = std::max(amax, std::fabs(v));
-  const double scale = amax > 0 ? 16384.0 / amax : 1.0;
-  std::vector<__half> h16((size_t)nc * ld, __float2half(0.f));
-  for (int i = 0; i < nc; i++)
-    for (int j = 0; j < nc; j++) h16[(size_t)i * ld + j] = __float2half((float)(cs.inv[(size_t)i * nc + j] * scale));
+  if (on_device) {
+    // Zc to the device (leading dimension padded to the factorisation's
+    // tile), Cholesky and inverse in FP64, the scaled FP16 copy in place
+    const int ldd = spd_inverse_ld(nc);
+    DevBuf<double> dA, dW;
+    DevBuf<int> dinfo;
+    DevBuf<unsigned long long> dmax;
+    CU(dA.alloc((size_t)ldd * ldd));
+    CU(dW.alloc((size_t)ldd * ldd));
+    CU(dinfo.alloc(1));
+    CU(dmax.alloc(1));
+    CU(cudaMemcpy2D(dA.p, ldd * sizeof(double), cs.inv.data(), nc * sizeof(double), nc * sizeof(double), nc,
+                    cudaMemcpyHostToDevice));
+    CU(spd_inverse_device(dA.p, dW.p, nc, ldd, dinfo.p, c->stream));
+    CU(c->cs_inv16.alloc((size_t)nc * ld));
+    CU(spd_inverse_to_half(dA.p, nc, ldd, dmax.p, ld, c->cs_inv16.p, c->stream));
+    int info = 0;
+    unsigned long long bits = 0;
+    CU(cudaMemcpyAsync(&info, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaMemcpyAsync(&bits, dmax.p, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    if (info != 0) return fail(c, CFD_E_NONFINITE, "coarse matrix P^T Z P is not positive definite (row %d)", info);
+    double amax = 0.0;
+    std::memcpy(&amax, &bits, sizeof(amax));
+    c->cs_scale = amax > 0 ? 16384.0 / amax : 1.0;
+  } else {
+    double amax = 0.0;
+    for (double v : cs.inv) amax = std::max(amax, std::fabs(v));
+    const double scale = amax > 0 ? 16384.0 / amax : 1.0;
+    std::vector<__half> h16((size_t)nc * ld, __float2half(0.f));
+    for (int i = 0; i < nc; i++)
+      for (int j = 0; j < nc; j++)
+        h16[(size_t)i * ld + j] = __float2half((float)(cs.inv[(size_t)i * nc + j] * scale));
+    c->cs_scale = scale;
+    CU(c->cs_inv16.alloc(h16.size()));
+    CU(cudaMemcpy(c->cs_inv16.p, h16.data(), h16.size() * sizeof(__half), cudaMemcpyHostToDevice));
+  }
   c->cs_ld = ld;
-  c->cs_scale = scale;
-  CU(c->cs_inv16.alloc(h16.size()));
-  CU(cudaMemcpy(c->cs_inv16.p, h16.data(), h16.size() * sizeof(__half), cudaMemcpyHostToDevice));
   CU(c->cs_c32.alloc(ld));
   CU(cudaMemset(c->cs_c32.p, 0, ld * sizeof(float)));
   CU(c->cs_e64.alloc(nc));
@@ -1209,6 +1242,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (cudaMallocHost((void**)&c->h_small, 64 * sizeof(double)) != cudaSuccess) return CFD_E_CUDA;
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_PERSIST")) c->fcg_persist = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_COARSE_HOST")) c->coarse_on_host = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_ANCHOR")) c->fcg_anchor = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_SPLIT_SPMV_PER_SM")) c->split_spmv_per_sm = std::atoi(e) == 1 ? 1 : 2;
@@ -1831,6 +1865,27 @@ int cfd_profile_read(cfd_ctx* c, double* out) {
   for (int k = 0; k < CFD_K_COUNT; k++)
     for (int j = 0; j < 3; j++) out[3 * k + j] = c->prof[k][j];
   return CFD_OK;
+}
+
+int cfd_spd_inverse(int device, const double* a, int n, double* inv) {
+  if (!a || !inv || n < 1 || n > 16384) return CFD_E_BADARG;
+  if (cudaSetDevice(device) != cudaSuccess) return CFD_E_CUDA;
+  const int ld = spd_inverse_ld(n);
+  DevBuf<double> dA, dW;
+  DevBuf<int> dinfo;
+  if (dA.alloc((size_t)ld * ld) != cudaSuccess || dW.alloc((size_t)ld * ld) != cudaSuccess ||
+      dinfo.alloc(1) != cudaSuccess)
+    return CFD_E_NOMEM;
+  int info = 0;
+  cudaError_t e = cudaMemcpy2D(dA.p, ld * sizeof(double), a, n * sizeof(double), n * sizeof(double), n,
+                               cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = spd_inverse_device(dA.p, dW.p, n, ld, dinfo.p, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(&info, dinfo.p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess)
+    e = cudaMemcpy2D(inv, n * sizeof(double), dA.p, ld * sizeof(double), n * sizeof(double), n,
+                     cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return CFD_E_CUDA;
+  return info == 0 ? CFD_OK : CFD_E_NONFINITE;
 }
 
 int cfd_selftest_wait_timeout(cfd_ctx* c, int timeout_ms) {

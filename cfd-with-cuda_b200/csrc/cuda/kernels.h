@@ -314,6 +314,17 @@ void fcg2l_neighbor_ranges(int n, int grid, int reach, int* lo, int* hi);
 cudaError_t launch_fcg2l(const FcgArgs<float>& a, const CoarseArgs<float>& ca, const Fcg2lArgs& pa, int grid,
                          cudaStream_t s);
 
+// Dense SPD inverse on the device (dense_chol.cu): A (row-major, leading
+// dimension ld = spd_inverse_ld(n), the n x n matrix in its top-left corner)
+// is replaced by its inverse; work holds ld x ld doubles; *info (device) =
+// 0, or the 1-based row of the first non-positive pivot.
+int spd_inverse_ld(int n);
+cudaError_t spd_inverse_device(double* A, double* work, int n, int ld, int* info, cudaStream_t s);
+// out (n rows of ldh halves) = inv * 16384 / max|inv| (zero past column n);
+// *amax_bits receives max|inv| as the bit pattern of a double.
+cudaError_t spd_inverse_to_half(const double* inv, int n, int ld, unsigned long long* amax_bits, int ldh, __half* out,
+                                cudaStream_t s);
+
 void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi);
 template <class VT>
 cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s);

@@ -198,7 +198,7 @@ void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]) {
 
 int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_p, const std::vector<int>& rp,
                  const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err,
-                 bool with_w) {
+                 bool with_w, bool factor) {
   for (int a = 0; a < 3; a++) cs.fd[a] = fd[a];
   coarse_lattice(fd, max_nodes, cs.cd, cs.h);
   const int nc = cs.cd[0] * cs.cd[1] * cs.cd[2];
@@ -315,6 +315,10 @@ int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_
       const double s = 0.5 * (Zc[(size_t)i * nc + j] + Zc[(size_t)j * nc + i]);
       Zc[(size_t)i * nc + j] = Zc[(size_t)j * nc + i] = s;
     }
+  if (!factor) {
+    cs.inv.swap(Zc);
+    return 0;
+  }
   if (!cholesky(Zc, nc)) {
     err = "coarse matrix P^T Z P is not positive definite";
     return -1;

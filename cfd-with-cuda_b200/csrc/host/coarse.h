@@ -33,8 +33,10 @@ void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]);
 // (Cholesky, FP64); with_w also keeps W = Z P in 27-tap boxes.  vox_of_p
 // maps a pressure node to its voxel (empty: identity).  Returns 0, or -1 with
 // err set when Zc is not positive definite.
+// factor = false: cs.inv receives Zc itself (dense, symmetric, row-major),
+// to be factored and inverted elsewhere (on the device).
 int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_p, const std::vector<int>& rp,
                  const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err,
-                 bool with_w = false);
+                 bool with_w = false, bool factor = true);
 
 }  // namespace cfd

@@ -317,6 +317,13 @@ int cfd_profile_read(cfd_ctx* ctx, double* out);
  * counterpart in the reference. */
 int cfd_profile_fcg2l(cfd_ctx* ctx, double* out7);
 
+/* Inverse of a dense symmetric positive definite n x n matrix (host
+ * buffers, row-major) computed on the given device in FP64: the blocked
+ * Cholesky and inverse that build the coarse space of the two-level
+ * preconditioners on the device.  CFD_E_NONFINITE when a pivot is not
+ * positive.  No counterpart in the reference. */
+int cfd_spd_inverse(int device, const double* a, int n, double* inv);
+
 /* Runs one small kernel whose bounded wait watches a flag nothing sets, with
  * the given limit in milliseconds.  Returns CFD_E_TIMEOUT when the wait gave
  * up as designed (the context stays usable), CFD_OK otherwise. */

@@ -13,18 +13,20 @@
 //  Third-party arithmetic the reference delegates and how it is restated:
 //    * MKL mkl_dcsrmv / cuSPARSE csrmv      -> plain CSR row loops (same math).
 //    * CSparse cs_multiply (Z = G^T D G)    -> explicit accumulation in the
-//      column-scatter order of CSparse's published cs_multiply (Davis 2006);
-//      CSparse itself is absent here, so the summation order is unverified.
+//      column-scatter order of CSparse's published cs_multiply (Davis 2006).
 //    * MKL dcg / cusp::krylov::cg + Jacobi  -> own Jacobi-PCG with the stopping
 //      rule ||r||_2 <= rtol*||b||_2 and a selectable initial guess (0 = the MKL
 //      call site BCH.cpp:4002-4004, warm = the CUSP call site CU.cu:268,430).
-//      The exact stopping tests of MKL dcg and CUSP default_monitor cannot be
-//      run here: parity of CG iteration counts with them is unpinned.
-//  No reference test, golden output or fixture exists for this path; the only
-//  fixture is the shipped input deck.  Parity of this oracle with the
-//  reference binary is therefore UNPINNED; it is checked by known-answer tests
-//  derived from the mathematics (partition of unity, element volumes, K*1=0,
-//  Z symmetric positive definite, nnz formulas) and by reading.
+//      MKL dcg tests squared norms, so the reference's dpar[0] = 1e-12
+//      (BCH.cpp:4018) is rtol = 1e-6 here.
+//  Parity with the reference is PINNED: the reference's own CPU solver,
+//  compiled unmodified against the MKL/CSparse stand-ins of oracle/refshim
+//  (oracle/_ref/fs_ref), produced the fixtures tests/golden/ref_*.npz, and
+//  this oracle reproduces them (final fields to 1e-9, every pressure solve's
+//  CG iteration count and every monitor row exactly, the node numbering bit
+//  for bit; tests/test_ref_parity.py).  Known-answer tests derived from the
+//  mathematics (partition of unity, element volumes, K*1=0, Z symmetric
+//  positive definite, nnz formulas) check it as well.
 //
 //  Floating-point contraction is disabled at build time (-ffp-contract=off).
 //  Reductions use a fixed chunking so results do not depend on thread count.
