@@ -200,6 +200,8 @@ struct cfd_ctx {
   bool fcg_persist = true;
   // CFD_COARSE_HOST=1: factor and invert the coarse matrix on the host
   bool coarse_on_host = false;
+  // CFD_COARSE_SPACING=<s>: coarse-lattice spacing in voxels (default 4)
+  double coarse_spacing = 4.0;
   int fcg2l_g = 0;                  // co-resident blocks of the launch
   int fcg2l_key[3] = {0, 0, 0};     // n, blocks, reach of the neighbour ranges in fcg2l_nb
   DevBuf<unsigned> fcg2l_sync;      // arrival counter + per-block progress
@@ -595,7 +597,8 @@ int ensure_coarse(cfd_ctx* c) {
   // the dense factorisation and inverse of Zc run on the device unless
   // CFD_COARSE_HOST=1 keeps them on the host
   const bool on_device = !c->coarse_on_host;
-  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err, want_zp, !on_device))
+  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err, want_zp, !on_device,
+                   c->coarse_spacing))
     return fail(c, CFD_E_NONFINITE, "%s", err.c_str());
   const int nc = cs.nc;
   for (int a = 0; a < 3; a++) {
@@ -1243,6 +1246,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_PERSIST")) c->fcg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_HOST")) c->coarse_on_host = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_COARSE_SPACING")) c->coarse_spacing = std::atof(e);
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_ANCHOR")) c->fcg_anchor = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_SPLIT_SPMV_PER_SM")) c->split_spmv_per_sm = std::atoi(e) == 1 ? 1 : 2;

@@ -176,8 +176,8 @@ void cholesky_inverse(std::vector<double>& A, int n, std::vector<double>& inv) {
 
 }  // namespace
 
-void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]) {
-  double s = 4.0;
+void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3], double spacing) {
+  double s = spacing > 1.0 ? spacing : 4.0;
   for (;;) {
     long long total = 1;
     for (int a = 0; a < 3; a++) {
@@ -198,9 +198,9 @@ void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]) {
 
 int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_p, const std::vector<int>& rp,
                  const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err,
-                 bool with_w, bool factor) {
+                 bool with_w, bool factor, double spacing) {
   for (int a = 0; a < 3; a++) cs.fd[a] = fd[a];
-  coarse_lattice(fd, max_nodes, cs.cd, cs.h);
+  coarse_lattice(fd, max_nodes, cs.cd, cs.h, spacing);
   const int nc = cs.cd[0] * cs.cd[1] * cs.cd[2];
   cs.nc = nc;
   const Axis ax = make_axis(fd[0], cs.cd[0], cs.h[0]), ay = make_axis(fd[1], cs.cd[1], cs.h[1]),

@@ -25,9 +25,10 @@ struct CoarseSpace {
   std::vector<double> w27;
 };
 
-// Coarse lattice for a voxel grid: spacing 4 voxels where the axis allows,
-// widened until the lattice has at most max_nodes nodes.
-void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]);
+// Coarse lattice for a voxel grid: spacing `spacing` voxels (default 4)
+// where the axis allows, widened until the lattice has at most max_nodes
+// nodes.
+void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3], double spacing = 4.0);
 
 // Builds Zc = P^T Z P from Z in CSR (pressure-node numbering) and inverts it
 // (Cholesky, FP64); with_w also keeps W = Z P in 27-tap boxes.  vox_of_p
@@ -37,6 +38,6 @@ void coarse_lattice(const int fd[3], int max_nodes, int cd[3], double h[3]);
 // to be factored and inverted elsewhere (on the device).
 int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_p, const std::vector<int>& rp,
                  const std::vector<int>& col, const std::vector<double>& val, CoarseSpace& cs, std::string& err,
-                 bool with_w = false, bool factor = true);
+                 bool with_w = false, bool factor = true, double spacing = 4.0);
 
 }  // namespace cfd

@@ -30,3 +30,19 @@ def test_bench_line_from_stand_in_solver():
     assert sr["bytes_per_step"] > 0 and abs(sr["frac"] * sr["peak"] - sr["achieved"]) <= 0.05 + 1e-3 * sr["achieved"]
     assert line["e2e"]["steps"] == line["steps"]
     assert line["roofline"]["kernel"] == "spmv_z"
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "fs_ref")),
+                    reason="the reference program was not built on this machine")
+def test_reference_arm_runs_the_reference_program():
+    """bench.py --impl reference on a 4^3 cavity: the reference's own program
+    (oracle/_ref/fs_ref) timed by its own TimeSpend column, one JSON line in
+    the contract's form."""
+    root = os.path.dirname(HERE)
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--n", "4",
+                        "--steps", "3", "--warmup", "3"], capture_output=True, text=True, timeout=300, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "steps/s" and line["value"] > 0
+    assert line["steps"] == 3 and line["cpu_baseline"]["kind"] == "reference"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
