@@ -522,12 +522,13 @@ class Solver:
                 for i, k in enumerate(self.KCLASS)}
 
 
-    FCG2L_PHASES = ["restrict", "coarse", "zphase", "nbwait", "spmv", "dotwait", "update"]
+    FCG2L_PHASES = ["restrict", "coarse", "zphase", "nbwait", "spmv", "dotwait", "update", "spmv_block_min",
+                    "spmv_block_mean", "spmv_block_max"]
 
     def profile_fcg2l(self) -> dict:
         """Phase times (ms, first block, summed) of the persistent two-level
         iteration while profiling was on."""
-        out = np.zeros(7)
+        out = np.zeros(10)
         self._check(self.L.cfd_profile_fcg2l(self.h, _p(out, C.c_double)))
         return dict(zip(self.FCG2L_PHASES, out.tolist()))
     def selftest_wait_timeout(self, ms: int) -> int:

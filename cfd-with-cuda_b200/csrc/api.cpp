@@ -206,7 +206,8 @@ struct cfd_ctx {
   int fcg2l_key[3] = {0, 0, 0};     // n, blocks, reach of the neighbour ranges in fcg2l_nb
   DevBuf<unsigned> fcg2l_sync;      // arrival counter + per-block progress
   DevBuf<int> fcg2l_nb;             // [lo (blocks), hi (blocks)]
-  DevBuf<double> fcg2l_part, fcg2l_time;
+  DevBuf<double> fcg2l_part, fcg2l_time;  // time: 7 phases of block 0, then one SpMV total per block
+  DevBuf<float> fcg2l_e;                   // coarse solution in pieces
   double unet_dscale = 1.0;  // median diagonal of Z (scale of the network's targets)
   double fcg_stall = 0.5;  // minimum residual reduction per window
 
@@ -759,7 +760,7 @@ CoarseArgs<VT> coarse_args(const cfd_ctx* c, bool with_coarse) {
 bool fcg2l_fits(const cfd_ctx* c, const FcgArgs<float>& a, const CoarseArgs<float>& ca) {
   if (!c->fcg_persist || !a.stencil || ca.pmap || a.st.m < 1 || a.st.m > 4) return false;
   if ((long long)ca.fd[0] * ca.fd[1] * ca.fd[2] != a.n || ca.fd[0] > 512) return false;
-  if (ca.ldinv % 8 || (size_t)ca.ldinv * sizeof(float) > fcg2l_smem_bytes()) return false;
+  if (ca.ldinv % 8 || fcg2l_pieces(ca.ldinv) == 0) return false;
   for (int ax = 1; ax < 3; ax++) {
     const double h = ca.cd[ax] > 1 ? (double)(ca.fd[ax] - 1) / (ca.cd[ax] - 1) : 1.0;
     if ((2 * h + 1) * (2 * h + 1) > 1024) return false;
@@ -782,18 +783,20 @@ int run_fcg2l(cfd_ctx* c, const FcgArgs<float>& a, const CoarseArgs<float>& ca) 
     CU(cudaMemcpy(c->fcg2l_nb.p, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice));
     CU(c->fcg2l_sync.alloc(1 + (size_t)G));
     CU(c->fcg2l_part.alloc(fcg2l_part_words(G)));
-    if (!c->fcg2l_time.p) {
-      CU(c->fcg2l_time.alloc(8));
-      CU(cudaMemset(c->fcg2l_time.p, 0, 8 * sizeof(double)));
-    }
+    CU(c->fcg2l_time.alloc(8 + (size_t)G));
+    CU(cudaMemset(c->fcg2l_time.p, 0, (8 + (size_t)G) * sizeof(double)));
     c->fcg2l_key[0] = a.n;
     c->fcg2l_key[1] = G;
     c->fcg2l_key[2] = reach;
   }
+  const int pieces = fcg2l_pieces(ca.ldinv);
+  if (c->fcg2l_e.n < (size_t)pieces * ca.nc) CU(c->fcg2l_e.alloc((size_t)pieces * ca.nc));
   CU(cudaMemsetAsync(c->fcg2l_sync.p, 0, (1 + (size_t)G) * sizeof(unsigned), s));
   Fcg2lArgs pa{};
   pa.c = c->cs_c32.p;
-  pa.e = c->cs_e32.p;
+  pa.e = c->fcg2l_e.p;
+  pa.pieces = pieces;
+  pa.tblock = c->prof_on ? c->fcg2l_time.p + 8 : nullptr;
   pa.sync = c->fcg2l_sync.p;
   pa.nb_lo = c->fcg2l_nb.p;
   pa.nb_hi = c->fcg2l_nb.p + G;
@@ -1847,18 +1850,32 @@ int cfd_profile(cfd_ctx* c, int on) {
   harvest(c);
   if (on) {
     std::memset(c->prof, 0, sizeof(c->prof));
-    if (c->fcg2l_time.p) CU(cudaMemset(c->fcg2l_time.p, 0, 8 * sizeof(double)));
+    if (c->fcg2l_time.p) CU(cudaMemset(c->fcg2l_time.p, 0, c->fcg2l_time.bytes()));
   }
   c->prof_on = on != 0;
   return CFD_OK;
 }
 
-int cfd_profile_fcg2l(cfd_ctx* c, double* out7) {
-  if (!c || !out7) return CFD_E_BADARG;
+int cfd_profile_fcg2l(cfd_ctx* c, double* out10) {
+  if (!c || !out10) return CFD_E_BADARG;
   CU(cudaStreamSynchronize(c->stream));
-  double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (c->fcg2l_time.p) CU(cudaMemcpy(t, c->fcg2l_time.p, sizeof(t), cudaMemcpyDeviceToHost));
-  for (int k = 0; k < 7; k++) out7[k] = t[k] * 1e-6;
+  for (int k = 0; k < 10; k++) out10[k] = 0.0;
+  if (!c->fcg2l_time.p) return CFD_OK;
+  std::vector<double> t(c->fcg2l_time.n);
+  CU(cudaMemcpy(t.data(), c->fcg2l_time.p, t.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 7; k++) out10[k] = t[k] * 1e-6;
+  const int G = (int)t.size() - 8;
+  if (G > 0) {
+    double mn = t[8], mx = t[8], sum = 0.0;
+    for (int b = 0; b < G; b++) {
+      mn = std::min(mn, t[8 + b]);
+      mx = std::max(mx, t[8 + b]);
+      sum += t[8 + b];
+    }
+    out10[7] = mn * 1e-6;
+    out10[8] = sum / G * 1e-6;
+    out10[9] = mx * 1e-6;
+  }
   return CFD_OK;
 }
 

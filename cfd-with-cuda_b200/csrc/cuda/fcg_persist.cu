@@ -189,6 +189,14 @@ __device__ void restrict_pair(const CoarseArgs<float>& a, const float* r, float*
   __syncthreads();
 }
 
+// 16-byte asynchronous copy global -> shared with an L2 cache policy
+__device__ __forceinline__ void cp_async16_hint(void* dst, const void* src, unsigned long long policy) {
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "l"(policy)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // sum of 8 FP16 entries packed in q times 8 FP32 values in shared memory
 __device__ __forceinline__ float dot8_smem(const uint4& q, const float* c) {
   const __half2* h = reinterpret_cast<const __half2*>(&q);
@@ -258,7 +266,12 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg2l(FcgArgs<float> a, Coar
     for (int pair = blockIdx.x; pair < ca.cd[1] * ca.cd[2]; pair += G) restrict_pair(ca, r, pa.c, pair, smem);
     lap(0);
     if (!grid_point(cnt, ++point * (unsigned)G, err, tmo)) break;
-    // (2) e = Zc^-1 c: c staged in shared memory, one warp per coarse row
+    // (2) e = Zc^-1 c: c staged in shared memory; each row of the FP16
+    // inverse split into pa.pieces pieces, a warp per piece: the piece is
+    // copied into the warp's shared-memory buffer by 16-byte asynchronous
+    // copies (about ten in flight per lane) and multiplied with c there.
+    // Piece p of row r goes to pa.e[p * nc + r]; (3) sums the pieces in
+    // order, so the result does not depend on which warp finishes first.
     {
       const unsigned long long keep = l2_evict_last();
       const float rscale = (float)(1.0 / ca.inv_scale);
@@ -266,19 +279,20 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg2l(FcgArgs<float> a, Coar
       for (int k = threadIdx.x; k < ca.nc; k += blockDim.x) cs[k] = __ldcg(pa.c + k);
       for (int k = ca.nc + threadIdx.x; k < ca.ldinv; k += blockDim.x) cs[k] = 0.f;
       __syncthreads();
-      const int nv8 = ca.ldinv >> 3;
-      for (int row = gw; row < ca.nc; row += W) {
+      const int nv8 = ca.ldinv >> 3, P = pa.pieces;
+      const int plen = (nv8 + P - 1) / P;  // 16-byte groups per piece
+      uint4* pb = reinterpret_cast<uint4*>(smem + ((ca.ldinv * 4 + 15) & ~15)) + (size_t)wib * plen;
+      for (int item = gw; item < P * ca.nc; item += W) {
+        const int row = item / P, piece = item % P;
+        const int j0 = piece * plen, j1 = min(nv8, j0 + plen);
         const uint4* ir = reinterpret_cast<const uint4*>(ca.inv16 + (size_t)row * ca.ldinv);
-        float s[2] = {0.f, 0.f};
-        int k = lane;
-        for (; k + 32 < nv8; k += 64) {
-          const uint4 q0 = ldg_hint(ir + k, keep), q1 = ldg_hint(ir + k + 32, keep);
-          s[0] += dot8_smem(q0, cs + 8 * k);
-          s[1] += dot8_smem(q1, cs + 8 * (k + 32));
-        }
-        if (k < nv8) s[0] += dot8_smem(ldg_hint(ir + k, keep), cs + 8 * k);
-        const float t = warp_sum(s[0] + s[1]);
-        if (lane == 0) pa.e[row] = t * rscale;
+        for (int j = j0 + lane; j < j1; j += 32) cp_async16_hint(pb + (j - j0), ir + j, keep);
+        cp_async_wait_all();  // this lane's own copies; it reads only those
+        float acc = 0.f;
+        for (int j = j0 + lane; j < j1; j += 32) acc += dot8_smem(pb[j - j0], cs + 8 * j);
+        acc = warp_sum(acc);
+        if (lane == 0) pa.e[(size_t)piece * ca.nc + row] = acc * rscale;
+        __syncwarp();
       }
     }
     // the first chunks of this iteration's matrix stream go out now and
@@ -318,7 +332,10 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg2l(FcgArgs<float> a, Coar
         const int dx = cnr & 1, dy = (cnr >> 1) & 1, dz = cnr >> 2;
         if ((dx && !bx) || (dy && !by) || (dz && !bz)) continue;
         const float wt = (dx ? wx : 1 - wx) * (dy ? wy : 1 - wy) * (dz ? wz : 1 - wz);
-        pe += wt * e0[dx + cx * dy + cxy * dz];
+        const float* ep = e0 + dx + cx * dy + cxy * dz;
+        float ev = ep[0];
+        for (int q = 1; q < pa.pieces; q++) ev += ep[(size_t)q * ca.nc];
+        pe += wt * ev;
       }
       z[i] = __ldg(a.dinv + i) * r[i] + pe;
     }
@@ -327,6 +344,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg2l(FcgArgs<float> a, Coar
     publish(prog, (unsigned)it + 1);
     if (!wait_blocks(prog, lo, hi, (unsigned)it + 1, err, tmo)) break;
     lap(3);
+    const unsigned long long t_spmv = threadIdx.x == 0 ? global_ns() : 0;
     // (4) w = Z z with the dot products; chunk k of the pass is the warp's
     // chunk kbase + k since launch, in buffer (kbase + k) % kStBuf, whose
     // completion is that buffer's phase (kbase + k) / kStBuf
@@ -365,6 +383,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg2l(FcgArgs<float> a, Coar
     // a chunk wait gave up in some warp: the whole block leaves together,
     // and the other blocks learn it from *err at their next wait
     if (!__syncthreads_and(ok)) break;
+    if (pa.tblock && threadIdx.x == 0) pa.tblock[blockIdx.x] += (double)(global_ns() - t_spmv);
     lap(4);
     ++point;
     post_block<NV>(v, pa.part + (size_t)(point & 1) * NV * G);
@@ -502,8 +521,16 @@ void fcg2l_neighbor_ranges(int n, int grid, int reach, int* lo, int* hi) {
   }
 }
 
+int fcg2l_pieces(int ldinv) {
+  const size_t cbytes = ((size_t)ldinv * 4 + 15) & ~(size_t)15, nv8 = (size_t)ldinv / 8;
+  for (int p = 1; p <= 4; p *= 2)
+    if (cbytes + (size_t)kPcgWarps * ((nv8 + p - 1) / p) * 16 <= (size_t)kPcgWarps * kStBuf * kStChunkBytes) return p;
+  return 0;
+}
+
 cudaError_t launch_fcg2l(const FcgArgs<float>& a, const CoarseArgs<float>& ca, const Fcg2lArgs& pa, int grid,
                          cudaStream_t s) {
+  if (pa.pieces < 1 || pa.pieces != fcg2l_pieces(ca.ldinv)) return cudaErrorInvalidValue;
   if (!a.stencil || ca.pmap || a.st.m < 1 || a.st.m > 4 || grid < 1) return cudaErrorInvalidValue;
   if ((long long)ca.fd[0] * ca.fd[1] * ca.fd[2] != a.n) return cudaErrorInvalidValue;
   if (ca.ldinv % 8 || ca.ldinv < ca.nc || (size_t)ca.ldinv * sizeof(float) > fcg2l_smem_bytes())

@@ -300,12 +300,17 @@ cudaError_t launch_fcg_combine(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, c
 // and written back to a.st.sc; a.dinv is the FP32 Jacobi diagonal.
 struct Fcg2lArgs {
   float* c;                  // coarse restriction, nc entries
-  float* e;                  // coarse solution, nc entries
+  float* e;                  // coarse solution in pieces (pieces x nc partial sums)
   unsigned* sync;            // 1 + grid words, zeroed before each launch: arrival counter, block progress
   const int *nb_lo, *nb_hi;  // per block: first and last block owning a row its SpMV gathers
   double* part;              // 2 x fcg2l_part_words / 2 partial sums
   double* timing;            // may be null: 7 phase times (ns) of block 0 added per launch
+  double* tblock;            // may be null: per block, the time (ns) of its SpMV phases added up
+  int pieces;                // fcg2l_pieces(ldinv): e holds pieces x nc partial products
 };
+// Pieces per row of the coarse inverse in the coarse solve (1, 2 or 4; 0:
+// the row buffers do not fit and the persistent iteration does not apply).
+int fcg2l_pieces(int ldinv);
 size_t fcg2l_smem_bytes();
 int fcg2l_grid(int device);                                    // co-resident blocks of the launch
 inline int fcg2l_part_words(int grid) { return 2 * (2 + 2 * 4) * grid; }

@@ -308,14 +308,15 @@ enum cfd_kernel_class {
  * {launches, total milliseconds, Krylov iterations inside those launches}. */
 int cfd_profile(cfd_ctx* ctx, int on);
 int cfd_profile_read(cfd_ctx* ctx, double* out);
-/* While profiling is on: the device time (milliseconds, read in the first
- * block of the launch, summed over launches) of each phase of the
- * persistent two-level iteration (class CFD_K_FCG2L): out7 = {restriction,
- * coarse solve, preconditioned residual, neighbour wait, structured SpMV
- * with its dot products, reduction of the dots, update with the (r,r)
- * reduction}; each phase's time includes the wait that ends it.  No
- * counterpart in the reference. */
-int cfd_profile_fcg2l(cfd_ctx* ctx, double* out7);
+/* While profiling is on: the device time (milliseconds, summed over
+ * launches) of the phases of the persistent two-level iteration (class
+ * CFD_K_FCG2L).  out10[0..6], read in the first block of the launch:
+ * restriction, coarse solve, preconditioned residual, neighbour wait,
+ * structured SpMV with its dot products, reduction of the dots, update with
+ * the (r,r) reduction (each phase's time includes the wait that ends it);
+ * out10[7..9]: the smallest, mean and largest over the blocks of each
+ * block's own SpMV time.  No counterpart in the reference. */
+int cfd_profile_fcg2l(cfd_ctx* ctx, double* out10);
 
 /* Inverse of a dense symmetric positive definite n x n matrix (host
  * buffers, row-major) computed on the given device in FP64: the blocked
