@@ -200,6 +200,9 @@ struct cfd_ctx {
   bool fcg_persist = true;
   // CFD_COARSE_HOST=1: factor and invert the coarse matrix on the host
   bool coarse_on_host = false;
+  // CFD_FCG2L_ZPIPE=0: the persistent iteration's SpMV loads each plane's
+  // gathers right before its products instead of one plane ahead
+  bool fcg2l_zpipe = true;
   // CFD_COARSE_SPACING=<s>: coarse-lattice spacing in voxels (default 4)
   double coarse_spacing = 4.0;
   int fcg2l_g = 0;                  // co-resident blocks of the launch
@@ -797,6 +800,7 @@ int run_fcg2l(cfd_ctx* c, const FcgArgs<float>& a, const CoarseArgs<float>& ca) 
   pa.e = c->fcg2l_e.p;
   pa.pieces = pieces;
   pa.tblock = c->prof_on ? c->fcg2l_time.p + 8 : nullptr;
+  pa.zpipe = c->fcg2l_zpipe ? 1 : 0;
   pa.sync = c->fcg2l_sync.p;
   pa.nb_lo = c->fcg2l_nb.p;
   pa.nb_hi = c->fcg2l_nb.p + G;
@@ -1249,6 +1253,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_PERSIST")) c->fcg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_HOST")) c->coarse_on_host = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_FCG2L_ZPIPE")) c->fcg2l_zpipe = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_SPACING")) c->coarse_spacing = std::atof(e);
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_ANCHOR")) c->fcg_anchor = std::atoi(e) != 0;
