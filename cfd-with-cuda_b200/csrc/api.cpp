@@ -15,6 +15,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -194,15 +195,16 @@ struct cfd_ctx {
       for (auto& gq : gp)
         for (auto& g : gq) g.reset();
   }
-  // persistent two-level iteration (fcg_persist.cu) for the FP32 inner
-  // solves on a structured grid; CFD_FCG_PERSIST=0 replays the per-kernel
-  // iteration graphs instead
-  bool fcg_persist = true;
+  // CFD_FCG_PERSIST=1: the persistent two-level iteration (fcg_persist.cu)
+  // for the FP32 inner solves on a structured grid instead of the per-kernel
+  // iteration graphs; measured slower on the 64^3 cavity (about 85 against
+  // 66 us per iteration: its grid-wide waits and serial small phases cost
+  // more than the launches they replace), so off by default
+  bool fcg_persist = false;
   // CFD_COARSE_HOST=1: factor and invert the coarse matrix on the host
   bool coarse_on_host = false;
-  // CFD_FCG2L_ZPIPE=0: the persistent iteration's SpMV loads each plane's
-  // gathers right before its products instead of one plane ahead
-  bool fcg2l_zpipe = true;
+  // CFD_L2_PERSIST=0: no persisting L2 window over the coarse inverse
+  bool l2_persist = true, l2_window = false;
   // CFD_COARSE_SPACING=<s>: coarse-lattice spacing in voxels (default 4)
   double coarse_spacing = 4.0;
   int fcg2l_g = 0;                  // co-resident blocks of the launch
@@ -580,6 +582,37 @@ constexpr int kCoarseMaxNodes = 6000;
 
 // Builds the coarse space on the host from the assembled Z and uploads the
 // hat tables and the inverse of P^T Z P (FP64, and FP32 for CFD_MIXED).
+// Keeps [p, p + bytes) in L2 across the kernels of the context's stream
+// (and the graphs captured from it): a persisting-access window with an L2
+// set-aside of at most the device's limit.  The coarse inverse is read once
+// per two-level iteration, between passes of the 137 MB structured-Z stream
+// that would otherwise push it out.  The set-aside belongs to this process's
+// context; cfd_destroy releases it.  CFD_L2_PERSIST=0 leaves L2 alone.
+// contexts of this process holding a persisting window (they share the
+// device's CUDA context and its set-aside)
+std::atomic<int> g_l2_users{0};
+
+int keep_in_l2(cfd_ctx* c, void* p, size_t bytes) {
+  if (!c->l2_persist || !p || bytes == 0) return CFD_OK;
+  int maxpersist = 0, maxwin = 0;
+  cudaDeviceGetAttribute(&maxpersist, cudaDevAttrMaxPersistingL2CacheSize, c->device);
+  cudaDeviceGetAttribute(&maxwin, cudaDevAttrMaxAccessPolicyWindowSize, c->device);
+  if (maxpersist <= 0 || maxwin <= 0) return CFD_OK;
+  const size_t win = std::min(bytes, (size_t)maxwin);
+  const size_t setaside = std::min(win, (size_t)maxpersist);
+  CU(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, setaside));
+  cudaStreamAttrValue v{};
+  v.accessPolicyWindow.base_ptr = p;
+  v.accessPolicyWindow.num_bytes = win;
+  v.accessPolicyWindow.hitRatio = std::min(1.0f, (float)setaside / (float)win);
+  v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  CU(cudaStreamSetAttribute(c->stream, cudaStreamAttributeAccessPolicyWindow, &v));
+  if (!c->l2_window) g_l2_users++;
+  c->l2_window = true;
+  return CFD_OK;
+}
+
 int ensure_coarse(cfd_ctx* c) {
   if (c->coarse_ready) return CFD_OK;
   int rc = ensure_grid(c);
@@ -683,6 +716,10 @@ int ensure_coarse(cfd_ctx* c) {
     CU(cudaMemcpy(c->cs_inv16.p, h16.data(), h16.size() * sizeof(__half), cudaMemcpyHostToDevice));
   }
   c->cs_ld = ld;
+  {
+    int rc = keep_in_l2(c, c->cs_inv16.p, (size_t)nc * ld * sizeof(__half));
+    if (rc) return rc;
+  }
   CU(c->cs_c32.alloc(ld));
   CU(cudaMemset(c->cs_c32.p, 0, ld * sizeof(float)));
   CU(c->cs_e64.alloc(nc));
@@ -800,7 +837,6 @@ int run_fcg2l(cfd_ctx* c, const FcgArgs<float>& a, const CoarseArgs<float>& ca) 
   pa.e = c->fcg2l_e.p;
   pa.pieces = pieces;
   pa.tblock = c->prof_on ? c->fcg2l_time.p + 8 : nullptr;
-  pa.zpipe = c->fcg2l_zpipe ? 1 : 0;
   pa.sync = c->fcg2l_sync.p;
   pa.nb_lo = c->fcg2l_nb.p;
   pa.nb_hi = c->fcg2l_nb.p + G;
@@ -1253,7 +1289,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_PERSIST")) c->fcg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_HOST")) c->coarse_on_host = std::atoi(e) != 0;
-  if (const char* e = std::getenv("CFD_FCG2L_ZPIPE")) c->fcg2l_zpipe = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_L2_PERSIST")) c->l2_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_SPACING")) c->coarse_spacing = std::atof(e);
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_ANCHOR")) c->fcg_anchor = std::atoi(e) != 0;
@@ -1268,6 +1304,16 @@ void cfd_destroy(cfd_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->stream2) cudaStreamSynchronize(c->stream2);
   if (c->h_small) cudaFreeHost(c->h_small);
+  if (c->l2_window) {
+    // release the persisting L2 lines and the set-aside this context took
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.num_bytes = 0;
+    if (c->stream) cudaStreamSetAttribute(c->stream, cudaStreamAttributeAccessPolicyWindow, &v);
+    if (--g_l2_users == 0) {
+      cudaCtxResetPersistingL2Cache();
+      cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+    }
+  }
   cudaStream_t s = c->stream, s2 = c->stream2;
   cudaEvent_t e1 = c->ev_fork, e2 = c->ev_join;
   delete c;

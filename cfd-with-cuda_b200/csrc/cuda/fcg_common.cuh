@@ -130,46 +130,5 @@ __device__ __forceinline__ void stencil_plane_shfl(const VT* q, const VT* __rest
   }
 }
 
-// The gathers of one dz plane into registers (lane l: z[rb(l) - 2] and, for
-// lanes 0..3, the four values past the warp's window, per dy row), and the
-// products of a plane from gathers loaded earlier: a loop can load the next
-// plane's values before it works on the current one, so the latency of the
-// gathers overlaps the arithmetic and the wait for the coefficients.
-template <bool CLAMP, bool NC, class VT>
-__device__ __forceinline__ void stencil_plane_load(const VT* __restrict__ z, int base, int fx, int n, int lane,
-                                                   VT (&w0)[5], VT (&w1)[5]) {
-#pragma unroll
-  for (int dy = -2; dy <= 2; dy++) {
-    const int rb = base + fx * dy;
-    int j0 = rb - 2, j1 = rb + 30;
-    if constexpr (CLAMP) {
-      j0 = j0 < 0 ? 0 : (j0 >= n ? n - 1 : j0);
-      j1 = j1 < 0 ? 0 : (j1 >= n ? n - 1 : j1);
-    }
-    w0[dy + 2] = ld_z<NC>(z, j0);
-    w1[dy + 2] = lane < 4 ? ld_z<NC>(z, j1) : (VT)0;
-  }
-}
-template <class VT>
-__device__ __forceinline__ void stencil_plane_fma(const VT* q, int lane, const VT (&w0)[5], const VT (&w1)[5],
-                                                  VT (&acc)[5]) {
-#pragma unroll
-  for (int dy = 0; dy < 5; dy++) {
-#pragma unroll
-    for (int dx = -2; dx <= 2; dx++) {
-      VT zv;
-      if (dx == -2) {
-        zv = w0[dy];
-      } else {
-        const int t = lane + dx + 2;
-        const VT lo = __shfl_sync(0xffffffffu, w0[dy], t & 31);
-        const VT hi = __shfl_sync(0xffffffffu, w1[dy], t & 31);
-        zv = t < 32 ? lo : hi;
-      }
-      acc[dy] += q[(dy * 5 + dx + 2) * 32] * zv;
-    }
-  }
-}
-
 }  // namespace
 }  // namespace cfd

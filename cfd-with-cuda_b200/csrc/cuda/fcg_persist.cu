@@ -354,48 +354,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg2l(FcgArgs<float> a, Coar
 #pragma unroll
     for (int k = 0; k < NV; k++) v[k] = 0.0;
     bool ok = true;
-    if (pa.zpipe) {
-      // the gathers of plane k + 1 go out before plane k is worked on
-      auto load_plane = [&](int kk, float (&w0)[5], float (&w1)[5]) {
-        const int sl = s0 + kk / 5, dz = kk % 5 - 2;
-        const int base = sl * 32 + lane + fxy * dz;
-        if (sl * 32 >= reach && sl * 32 + 31 + reach < n)
-          stencil_plane_load<false, false>(z, base, fx, n, lane, w0, w1);
-        else
-          stencil_plane_load<true, false>(z, base, fx, n, lane, w0, w1);
-      };
-      float cw0[5], cw1[5];
-      if (total > 0) load_plane(0, cw0, cw1);
-      float acc[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-      for (int k = 0; k < total; k++) {
-        float nw0[5], nw1[5];
-        if (k + 1 < total) load_plane(k + 1, nw0, nw1);
-        const int K = kbase + k, b = K % kStBuf;
-        if (!__all_sync(0xffffffffu, mbar_wait_bounded(mbar + b, (unsigned)((K / kStBuf) & 1), tmo))) {
-          ok = false;
-          if (lane == 0) atomicExch(err, 1);
-          break;
-        }
-        stencil_plane_fma(buf + (size_t)b * kStTaps * 32 + lane, lane, cw0, cw1, acc);
-        __syncwarp();
-        pend_lo = K + 1;
-        issue(k + kStBuf);
-        if (k + kStBuf < total) pend_hi = kbase + k + kStBuf + 1;
-        if (k % 5 == 4) {
-          const int i = (s0 + k / 5) * 32 + lane;
-          if (i < n) fcg_row_dots<MD>(a, i, z[i], ((acc[0] + acc[1]) + (acc[2] + acc[3])) + acc[4], nd, v);
-#pragma unroll
-          for (int d = 0; d < 5; d++) acc[d] = 0.f;
-        }
-        if (k + 1 < total) {
-#pragma unroll
-          for (int d = 0; d < 5; d++) {
-            cw0[d] = nw0[d];
-            cw1[d] = nw1[d];
-          }
-        }
-      }
-    } else {
+    {
       int k = 0;
       for (int sl = s0; sl < s1 && ok; sl++) {
         const int i = sl * 32 + lane;

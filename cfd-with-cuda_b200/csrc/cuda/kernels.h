@@ -306,7 +306,6 @@ struct Fcg2lArgs {
   double* part;              // 2 x fcg2l_part_words / 2 partial sums
   double* timing;            // may be null: 7 phase times (ns) of block 0 added per launch
   double* tblock;            // may be null: per block, the time (ns) of its SpMV phases added up
-  int zpipe;                 // 1: the SpMV loads the next plane's gathers before the current plane's products
   int pieces;                // fcg2l_pieces(ldinv): e holds pieces x nc partial products
 };
 // Pieces per row of the coarse inverse in the coarse solve (1, 2 or 4; 0:
