@@ -203,8 +203,11 @@ struct cfd_ctx {
   bool fcg_persist = false;
   // CFD_COARSE_HOST=1: factor and invert the coarse matrix on the host
   bool coarse_on_host = false;
-  // CFD_L2_PERSIST=0: no persisting L2 window over the coarse inverse
-  bool l2_persist = true, l2_window = false;
+  // CFD_PDL=1: the flexible-CG iteration kernels use programmatic dependent
+  // launch (each may start while the one before it drains)
+  bool pdl = false;
+  // CFD_L2_PERSIST=1: a persisting L2 window over the coarse inverse
+  bool l2_persist = false, l2_window = false;
   // CFD_COARSE_SPACING=<s>: coarse-lattice spacing in voxels (default 4)
   double coarse_spacing = 4.0;
   int fcg2l_g = 0;                  // co-resident blocks of the launch
@@ -580,14 +583,14 @@ int ensure_grid(cfd_ctx* c) {
 
 constexpr int kCoarseMaxNodes = 6000;
 
-// Builds the coarse space on the host from the assembled Z and uploads the
-// hat tables and the inverse of P^T Z P (FP64, and FP32 for CFD_MIXED).
-// Keeps [p, p + bytes) in L2 across the kernels of the context's stream
-// (and the graphs captured from it): a persisting-access window with an L2
-// set-aside of at most the device's limit.  The coarse inverse is read once
-// per two-level iteration, between passes of the 137 MB structured-Z stream
-// that would otherwise push it out.  The set-aside belongs to this process's
-// context; cfd_destroy releases it.  CFD_L2_PERSIST=0 leaves L2 alone.
+// With CFD_L2_PERSIST=1, keeps [p, p + bytes) in L2 across the kernels of
+// the context's stream (and the graphs captured from it): a
+// persisting-access window with an L2 set-aside of at most the device's
+// limit.  The coarse inverse is read once per two-level iteration, between
+// passes of the 137 MB structured-Z stream (read evict-first).  Measured on
+// the 64^3 cavity's two-level line the window made the steps slower (126.5
+// against 128.7 steps/s), so it is off by default.  The set-aside belongs
+// to this process's context; cfd_destroy releases it.
 // contexts of this process holding a persisting window (they share the
 // device's CUDA context and its set-aside)
 std::atomic<int> g_l2_users{0};
@@ -613,6 +616,8 @@ int keep_in_l2(cfd_ctx* c, void* p, size_t bytes) {
   return CFD_OK;
 }
 
+// Builds the coarse space from the assembled Z and puts on the device the
+// hat tables and the scaled FP16 inverse of P^T Z P.
 int ensure_coarse(cfd_ctx* c) {
   if (c->coarse_ready) return CFD_OK;
   int rc = ensure_grid(c);
@@ -938,12 +943,14 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   // the sequential form: its correction would need a second SpMV.
   const bool split = sizeof(VT) == 4 && a.stencil && c->cs_zp_ok && !pmap && c->fcg_split;
   a.dinv = dinv;
+  a.pdl = c->pdl ? 1 : 0;
   if (split) {
     if (!c->fcg_z1.p) CU(c->fcg_z1.alloc(n));
     a.z1 = reinterpret_cast<VT*>(c->fcg_z1.p);
   }
   KL(CFD_K_FCG, launch_fcg_start<VT>(a, warm, s));
-  const CoarseArgs<VT> ca = coarse_args<VT>(c, true);
+  CoarseArgs<VT> ca = coarse_args<VT>(c, true);
+  ca.pdl = a.pdl;
   // one flexible-CG iteration: preconditioner (U-Net, coarse restriction
   // and solve, combination), SpMV + dots + coefficients, update + tests
   auto iteration = [&](bool counted, bool with_net) -> int {
@@ -1289,6 +1296,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (const char* e = std::getenv("CFD_FCG_GRAPH")) c->fcg_use_graph = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_PERSIST")) c->fcg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_HOST")) c->coarse_on_host = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_PDL")) c->pdl = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_L2_PERSIST")) c->l2_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_SPACING")) c->coarse_spacing = std::atof(e);
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;

@@ -28,6 +28,8 @@ constexpr int kRestrictLines = 1024;  // y-z support lines per coarse pair at mo
 template <class VT>
 __global__ void __launch_bounds__(kRestrictThreads) k_restrict(CoarseArgs<VT> a, const VT* __restrict__ r,
                                                                float* __restrict__ c, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   extern __shared__ double sline[];  // G x fd[0] partial sums
   __shared__ double swt[kRestrictLines];
@@ -93,6 +95,8 @@ template <class VT>
 __global__ void __launch_bounds__(kMvThreads) k_coarse_mv(int nc, int ld, const __half* __restrict__ inv, float rscale,
                                                           const float* __restrict__ c, VT* __restrict__ e,
                                                           const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   const int row = blockIdx.x;
   const int nv8 = nc >> 3, tail = nc & 7;  // whole 8-entry groups inside the row, then a tail
@@ -126,6 +130,8 @@ __global__ void __launch_bounds__(256) k_precond(CoarseArgs<VT> a, int nv, const
                                                  const VT* __restrict__ dinv, const VT* __restrict__ e,
                                                  const float* __restrict__ y, const double* rr, double dscale,
                                                  VT* __restrict__ z, const int* done) {
+  pdl_wait();
+  pdl_trigger();
   if (done && *done) return;
   VT ys = 0;
   if (y) ys = (VT)(rr[0] > 0.0 ? sqrt(rr[0] / (double)nv) / dscale : 0.0);
@@ -171,22 +177,21 @@ cudaError_t launch_coarse_restrict(const CoarseArgs<VT>& a, const VT* r, float* 
   }
   const int G = a.fd[0] <= kRestrictThreads ? kRestrictThreads / a.fd[0] : 1;
   const size_t sm = (size_t)G * a.fd[0] * sizeof(double);
-  k_restrict<VT><<<a.cd[1] * a.cd[2], kRestrictThreads, sm, s>>>(a, r, c, done);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_restrict<VT>, dim3(a.cd[1] * a.cd[2]), dim3(kRestrictThreads), sm, s, a, r, c, done);
 }
 
 template <class VT>
 cudaError_t launch_coarse_solve(const CoarseArgs<VT>& a, const float* c, VT* e, const int* done, cudaStream_t s) {
   if (a.ldinv % 8 || a.ldinv < a.nc) return cudaErrorInvalidValue;
-  k_coarse_mv<VT><<<a.nc, kMvThreads, 0, s>>>(a.nc, a.ldinv, a.inv16, (float)(1.0 / a.inv_scale), c, e, done);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_coarse_mv<VT>, dim3(a.nc), dim3(kMvThreads), 0, s, a.nc, a.ldinv, a.inv16,
+                  (float)(1.0 / a.inv_scale), c, e, done);
 }
 
 template <class VT>
 cudaError_t launch_precond(const CoarseArgs<VT>& a, int nv, const VT* r, const VT* dinv, const VT* e, const float* y,
                            const double* rr, double dscale, VT* z, const int* done, cudaStream_t s) {
-  k_precond<VT><<<grid_of(nv, 256), 256, 0, s>>>(a, nv, r, dinv, e, y, rr, dscale, z, done);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_precond<VT>, dim3(grid_of(nv, 256)), dim3(256), 0, s, a, nv, r, dinv, e, y, rr,
+                  dscale, z, done);
 }
 
 template cudaError_t launch_coarse_restrict<float>(const CoarseArgs<float>&, const float*, float*, const int*,

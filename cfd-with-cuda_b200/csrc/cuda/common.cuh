@@ -124,6 +124,15 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* err, unsigned l
   return s_ok != 0;
 }
 
+// Programmatic dependent launch (sm_90 and newer).  A kernel launched with
+// launch_k(pdl = true, ...) may start while the kernel before it on the
+// stream is still running: pdl_wait() returns once that kernel has finished
+// and its writes are visible (at once for a launch without the attribute),
+// and pdl_trigger() lets the kernel after this one launch as soon as every
+// block of this one has reached it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 // Read-only 32-byte load of a double4 node value (two 16-byte loads of the
 // same aligned sector).
 __device__ __forceinline__ double4 ldg4(const double4* p) {
@@ -222,6 +231,29 @@ __device__ __forceinline__ int bsearch_slot(const int* __restrict__ col, int b, 
     if (c < key) lo = mid + 1; else hi = mid - 1;
   }
   return -1;
+}
+
+// Kernel launch, with the programmatic-stream-serialisation attribute when
+// pdl is set (the kernel must then call pdl_wait() before it reads what the
+// previous kernel wrote).
+template <typename... Params, typename... Args>
+inline cudaError_t launch_k(bool pdl, void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                            cudaStream_t s, Args... args) {
+  if (!pdl) {
+    kernel<<<grid, block, smem, s>>>(args...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 #endif  // __CUDACC__

@@ -111,6 +111,8 @@ __device__ __forceinline__ void fcg_spmv_finish(const FcgArgs<VT>& a, double (&v
 // block initialises the state words.
 template <class VT>
 __global__ void __launch_bounds__(kFcgThreads) k_fcg_start(FcgArgs<VT> a, int warm) {
+  pdl_wait();
+  pdl_trigger();
   double v[2] = {0, 0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
     const VT bi = a.b[i];
@@ -160,6 +162,8 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_start(FcgArgs<VT> a, int wa
 // 32-row slices, lane = row.
 template <class VT, int MD>
 __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
+  pdl_wait();
+  pdl_trigger();
   if (*a.st.done) return;
   extern __shared__ __align__(16) unsigned char smem[];
   const double* sc = a.st.sc;
@@ -209,6 +213,8 @@ __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv(FcgArgs<VT> a) {
 // DOTS = false: w = Z z only (the Jacobi part of the split iteration).
 template <class VT, int MD, bool DOTS>
 __global__ void __launch_bounds__(kPcgThreads, 2) k_fcg_spmv_stencil(FcgArgs<VT> a) {
+  pdl_wait();
+  pdl_trigger();
   if (*a.st.done) return;
   extern __shared__ __align__(16) unsigned char smem[];
   const double* sc = a.st.sc;
@@ -300,6 +306,8 @@ __global__ void __launch_bounds__(kCombineThreads) k_fcg_combine(FcgArgs<VT> a, 
                                                                  const float* __restrict__ wst,
                                                                  const int* __restrict__ wlo,
                                                                  const VT* __restrict__ e) {
+  pdl_wait();
+  pdl_trigger();
   if (*a.st.done) return;
   const double* sc = a.st.sc;
   const int m = (int)sc[kFcgM], it = (int)sc[kFcgIt];
@@ -340,6 +348,8 @@ __global__ void __launch_bounds__(kCombineThreads) k_fcg_combine(FcgArgs<VT> a, 
 
 template <class VT>
 __global__ void __launch_bounds__(kFcgThreads) k_fcg_update(FcgArgs<VT> a) {
+  pdl_wait();
+  pdl_trigger();
   if (*a.st.done) return;
   const double* sc = a.st.sc;
   const int m = (int)sc[kFcgM], it = (int)sc[kFcgIt];
@@ -429,8 +439,7 @@ template <class VT>
 cudaError_t launch_fcg_start(const FcgArgs<VT>& a, int warm, cudaStream_t s) {
   if (a.st.m < 1 || a.st.m > kFcgMaxM) return cudaErrorInvalidValue;
   if (a.st.anchor < 0 || (a.st.anchor > 0 && a.st.m != a.st.anchor + 1)) return cudaErrorInvalidValue;
-  k_fcg_start<VT><<<nblocks(a.n), kFcgThreads, 0, s>>>(a, warm);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_fcg_start<VT>, dim3(nblocks(a.n)), dim3(kFcgThreads), 0, s, a, warm);
 }
 
 template <class VT, int MD, bool DOTS>
@@ -440,8 +449,7 @@ cudaError_t launch_stencil_kernel(const FcgArgs<VT>& a, cudaStream_t s) {
   cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv_stencil<VT, MD, DOTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
-  k_fcg_spmv_stencil<VT, MD, DOTS><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_fcg_spmv_stencil<VT, MD, DOTS>, dim3(a.spmv_grid), dim3(kPcgThreads), smem, s, a);
 }
 
 template <class VT, int MD>
@@ -450,8 +458,7 @@ cudaError_t launch_fcg_spmv_md(const FcgArgs<VT>& a, cudaStream_t s) {
   const size_t smem = pcg_smem_bytes<VT>();
   cudaError_t e = cudaFuncSetAttribute(k_fcg_spmv<VT, MD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k_fcg_spmv<VT, MD><<<a.spmv_grid, kPcgThreads, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_fcg_spmv<VT, MD>, dim3(a.spmv_grid), dim3(kPcgThreads), smem, s, a);
 }
 
 // the SpMV's dot partials are sized for the solve's window m: 1 (CG with a
@@ -478,8 +485,8 @@ cudaError_t launch_fcg_spmv_jacobi(const FcgArgs<VT>& a, cudaStream_t s) {
 template <class VT, int MD>
 cudaError_t launch_combine_md(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, const float* wst, const int* wlo,
                               const VT* e, cudaStream_t s) {
-  k_fcg_combine<VT, MD><<<nblocks(a.n), kCombineThreads, 0, s>>>(a, ca, wst, wlo, e);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_fcg_combine<VT, MD>, dim3(nblocks(a.n)), dim3(kCombineThreads), 0, s, a, ca, wst,
+                  wlo, e);
 }
 
 template <class VT>
@@ -494,8 +501,7 @@ cudaError_t launch_fcg_combine(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, c
 
 template <class VT>
 cudaError_t launch_fcg_update(const FcgArgs<VT>& a, cudaStream_t s) {
-  k_fcg_update<VT><<<nblocks(a.n), kFcgThreads, 0, s>>>(a);
-  return cudaGetLastError();
+  return launch_k(a.pdl != 0, k_fcg_update<VT>, dim3(nblocks(a.n)), dim3(kFcgThreads), 0, s, a);
 }
 
 template <class VT>

@@ -197,7 +197,7 @@ struct PcgArgs {
 // whole solve and every later direction overwrites slot a, so each new
 // direction is orthogonalised against the first a and the previous one.
 constexpr int kFcgMaxM = 8;        // directions kept at most
-constexpr int kFcgMaxBlocks = 444;  // grid of the iteration kernels (3 per SM)
+constexpr int kFcgMaxBlocks = 1184;  // grid cap of the iteration kernels (8 blocks of 256 per SM on 148 SMs: one row per thread at 65^3)
 enum {
   kFcgRR = 0, kFcgBB, kFcgAlpha, kFcgIt, kFcgStatus, kFcgRRMark, kFcgRtol, kFcgStall2, kFcgMaxit, kFcgWindow,
   kFcgM, kFcgAnchor, kFcgPQ0 = 12, kFcgBeta0 = kFcgPQ0 + kFcgMaxM, kFcgScalars = kFcgBeta0 + kFcgMaxM
@@ -234,6 +234,7 @@ template <class VT> struct FcgArgs {
   FcgState st;
   VT* z1;
   const VT* dinv;
+  int pdl;  // 1: the iteration kernels launch with programmatic dependent launch
 };
 struct Int3 {
   int v[3];
@@ -263,6 +264,7 @@ template <class VT> struct CoarseArgs {
   const int *rx, *ry, *rz;
   const __half* inv16;
   double inv_scale;
+  int pdl;  // 1: the coarse kernels launch with programmatic dependent launch
 };
 // c = P^T r (FP32 coarse vector), e = Zc^-1 c
 template <class VT>
