@@ -287,16 +287,23 @@ def run_ours(args, rank, world, local_rank):
                          precond=pc_of[precond], fcg_net_iters=args.net_iters)
         t0 = time.time()
         s.load(deck)
+        t1 = time.time()
         s.step0()
+        t2 = time.time()
         if precond == "learned":
             s.load_unet(args.weights)
         if precond != "jacobi":
             s.precond_apply(np.zeros(s.refresh().NNp))  # builds the coarse space (set-up)
-        setup_s = time.time() - t0
+        t3 = time.time()
+        setup_s = t3 - t0
+        # deck reading and host preprocessing (numbering, patterns) plus the
+        # upload; step0's operator assembly on the device; the network's
+        # weights and the coarse space (Galerkin product, factorisation)
+        setup_parts = {"load": round(t1 - t0, 3), "step0": round(t2 - t1, 3), "precond": round(t3 - t2, 3)}
         for _ in range(warmup):
             s.run(1)
         if steps == 0:
-            return s, dict(setup_s=setup_s)
+            return s, dict(setup_s=setup_s, setup_parts=setup_parts)
         stream = torch.cuda.ExternalStream(s.stream_ptr, device=local_rank)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         n0 = s.launch_count()
@@ -310,7 +317,8 @@ def run_ours(args, rank, world, local_rank):
         barrier()
         ms = ev0.elapsed_time(ev1)
         launches = s.launch_count() - n0
-        return s, dict(ms=ms, st=st, launches=launches, clocks=clk.summary(), setup_s=setup_s)
+        return s, dict(ms=ms, st=st, launches=launches, clocks=clk.summary(), setup_s=setup_s,
+                       setup_parts=setup_parts)
 
     precision = cfdfs.MIXED if args.precision == "mixed" else cfdfs.FP64
     # the cavity's pressure nodes form an identity-numbered cube, so the
@@ -482,7 +490,7 @@ def run_ours(args, rank, world, local_rank):
                        "ngp": 8, "cg_rtol": 1e-8, "cg_x0": "zero",
                        "timed_steps": f"steps {args.warmup + 1}..{args.warmup + args.steps} of the run from rest",
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush needed)",
-                       "setup_s": round(r["setup_s"], 2)},
+                       "setup_s": round(r["setup_s"], 2), "setup_parts_s": r["setup_parts"]},
             "cg_iters_per_step": round(r["st"].cg_iters / max(1, r["st"].steps), 1),
             "subiters_per_step": round(r["st"].subiters / max(1, r["st"].steps), 2),
             "pressure_fallbacks": int(r["st"].fallbacks),  # solves that fell back to Jacobi-PCG
@@ -677,7 +685,6 @@ def main():
                     help="learned preconditioner: network in the first this-many iterations of a solve (0 = all)")
     ap.add_argument("--fp64-steps", type=int, default=1, help="0 skips the FP64 Jacobi-PCG comparison run")
     ap.add_argument("--profile-steps", type=int, default=2)
-    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cg-maxit", type=int, default=5000)
     ap.add_argument("--cpu-budget", type=float, default=90.0,
                     help="seconds of timed reference steps before the reference arm stops")

@@ -130,6 +130,7 @@ _PROTOS = {
     "cfd_profile_read": (C.c_int, [_vp, _dp]),
     "cfd_profile_fcg2l": (C.c_int, [_vp, _dp]),
     "cfd_spd_inverse": (C.c_int, [C.c_int, _dp, C.c_int, _dp]),
+    "cfd_coarse_matrix": (C.c_int, [C.c_int, _ip, _ip, _ip, _dp, C.c_double, _ip, _dp]),
     "cfd_selftest_wait_timeout": (C.c_int, [_vp, C.c_int]),
     "cfd_pcg_solve_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_double, C.c_int, _vp, _dp,
                                         C.c_char_p, C.c_int]),
@@ -142,6 +143,7 @@ _PROTOS = {
     "cfdh_get_pattern": (C.c_int, [_vp, C.c_int, _ip, _ip]),
     "cfdh_write_tecplot": (C.c_int, [_vp, _dp, _dp, _cp, _cp]),
     "cfdh_coarse_inverse": (C.c_int, [_ip, _ip, _ip, _dp, _ip, _dp]),
+    "cfdh_coarse_matrix": (C.c_int, [_ip, _ip, _ip, _dp, C.c_double, _ip, _dp]),
     "cfdh_element_colors": (C.c_int, [_vp, _ip, _ip]),
 }
 
@@ -685,6 +687,38 @@ def coarse_inverse(dims, rowptr, col, val):
     if rc != CFD_OK:
         raise CfdError(rc, "cfdh_coarse_inverse: the coarse matrix is not positive definite")
     return tuple(int(v) for v in cd), inv
+
+
+def coarse_matrix(dims, rowptr, col, val, spacing: float = 4.0, device=None):
+    """Galerkin coarse matrix P^T Z P of the two-level preconditioner for the
+    CSR matrix Z on the grid dims, dense: (coarse nodes per axis, Zc).  Built
+    on the host, or on the given device (the solver's build, bit-identical
+    to the host's)."""
+    L = lib()
+    d = np.ascontiguousarray(dims, dtype=np.int32)
+    rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+    cl = np.ascontiguousarray(col, dtype=np.int32)
+    vl = np.ascontiguousarray(val, dtype=np.float64)
+    cd = np.zeros(3, dtype=np.int32)
+
+    def call(out):
+        ptr = None if out is None else _p(out, C.c_double)
+        if device is None:
+            return L.cfdh_coarse_matrix(_p(d, C.c_int), _p(rp, C.c_int), _p(cl, C.c_int), _p(vl, C.c_double),
+                                        float(spacing), _p(cd, C.c_int), ptr)
+        return L.cfd_coarse_matrix(int(device), _p(d, C.c_int), _p(rp, C.c_int), _p(cl, C.c_int),
+                                   _p(vl, C.c_double), float(spacing), _p(cd, C.c_int), ptr)
+
+    rc = call(None)
+    if rc != CFD_OK:
+        raise CfdError(rc, "coarse_matrix: bad arguments")
+    nc = int(np.prod(cd))
+    zc = np.zeros((nc, nc))
+    rc = call(zc)
+    if rc != CFD_OK:
+        raise CfdError(rc, "coarse_matrix: a row of Z reaches more than 3 coarse nodes per axis"
+                       if rc == CFD_E_BADINPUT else "coarse_matrix failed")
+    return tuple(int(v) for v in cd), zc
 
 
 NOALLOC_MAX_N = 524288

@@ -616,6 +616,37 @@ int keep_in_l2(cfd_ctx* c, void* p, size_t bytes) {
   return CFD_OK;
 }
 
+// Hat functions of the coarse lattice along one axis of n fine nodes and ncd
+// coarse nodes h apart: fine index x lies in coarse cell i0[x] with weight
+// 1 - f[x] on node i0 and f[x] on node i0 + 1 (the tables of coarse.cpp);
+// rng[2k], rng[2k + 1] = the first and last fine index in node k's support.
+void hat_tables(int n, int ncd, double h, std::vector<int>& i0, std::vector<double>& f, std::vector<int>& rng) {
+  i0.assign(n, 0);
+  f.assign(n, 0.0);
+  rng.assign(2 * (size_t)ncd, 0);
+  for (int i = 0; i < ncd; i++) {
+    rng[2 * i] = n;
+    rng[2 * i + 1] = -1;
+  }
+  for (int x = 0; x < n; x++) {
+    int i = 0;
+    double fr = 0.0;
+    if (ncd >= 2) {
+      const double t = x / h;
+      i = std::min(std::max((int)std::floor(t), 0), ncd - 2);
+      fr = std::min(std::max(t - i, 0.0), 1.0);
+    }
+    i0[x] = i;
+    f[x] = fr;
+    for (int k = i; k <= std::min(i + 1, ncd - 1); k++) {
+      rng[2 * k] = std::min(rng[2 * k], x);
+      rng[2 * k + 1] = std::max(rng[2 * k + 1], x);
+    }
+  }
+  for (int i = 0; i < ncd; i++)
+    if (rng[2 * i + 1] < rng[2 * i]) rng[2 * i] = rng[2 * i + 1] = 0;
+}
+
 // Builds the coarse space from the assembled Z and puts on the device the
 // hat tables and the scaled FP16 inverse of P^T Z P.
 int ensure_coarse(cfd_ctx* c) {
@@ -624,52 +655,19 @@ int ensure_coarse(cfd_ctx* c) {
   if (rc) return rc;
   const double t0 = wall_seconds();
   const HostProblem& P = c->P;
-  std::vector<double> zv(P.z_col.size());
-  CU(cudaStreamSynchronize(c->stream));
-  CU(cudaMemcpy(zv.data(), c->zval.p, zv.size() * sizeof(double), cudaMemcpyDeviceToHost));
-  std::vector<int> vox;
-  if (!c->h_pmap.empty()) {
-    vox.assign(c->h_pmap.size(), 0);
-    for (size_t v = 0; v < c->h_pmap.size(); v++) vox[c->h_pmap[v]] = (int)v;
-  }
+  const int np = P.NNp;
   CoarseSpace cs;
-  std::string err;
-  // Z P for the split FP32 iteration (structured form, identity numbering)
-  const bool want_zp = mixed(c) && c->h_pmap.empty();
-  // the dense factorisation and inverse of Zc run on the device unless
-  // CFD_COARSE_HOST=1 keeps them on the host
-  const bool on_device = !c->coarse_on_host;
-  if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err, want_zp, !on_device,
-                   c->coarse_spacing))
-    return fail(c, CFD_E_NONFINITE, "%s", err.c_str());
+  for (int a = 0; a < 3; a++) cs.fd[a] = c->udims[a];
+  coarse_lattice(c->udims, kCoarseMaxNodes, cs.cd, cs.h, c->coarse_spacing);
+  cs.nc = cs.cd[0] * cs.cd[1] * cs.cd[2];
   const int nc = cs.nc;
   for (int a = 0; a < 3; a++) {
     c->cs_fd[a] = cs.fd[a];
     c->cs_cd[a] = cs.cd[a];
     const int n = cs.fd[a], ncd = cs.cd[a];
-    std::vector<int> i0(n), rng(2 * (size_t)ncd);
-    std::vector<double> f(n);
-    for (int i = 0; i < ncd; i++) {
-      rng[2 * i] = n;
-      rng[2 * i + 1] = -1;
-    }
-    for (int x = 0; x < n; x++) {
-      int i = 0;
-      double fr = 0.0;
-      if (ncd >= 2) {
-        const double t = x / cs.h[a];
-        i = std::min(std::max((int)std::floor(t), 0), ncd - 2);
-        fr = std::min(std::max(t - i, 0.0), 1.0);
-      }
-      i0[x] = i;
-      f[x] = fr;
-      for (int k = i; k <= std::min(i + 1, ncd - 1); k++) {
-        rng[2 * k] = std::min(rng[2 * k], x);
-        rng[2 * k + 1] = std::max(rng[2 * k + 1], x);
-      }
-    }
-    for (int i = 0; i < ncd; i++)
-      if (rng[2 * i + 1] < rng[2 * i]) rng[2 * i] = rng[2 * i + 1] = 0;
+    std::vector<int> i0, rng;
+    std::vector<double> f;
+    hat_tables(n, ncd, cs.h[a], i0, f, rng);
     CU(c->cs_i0[a].alloc(n));
     CU(c->cs_f[a].alloc(n));
     CU(c->cs_r[a].alloc(2 * (size_t)ncd));
@@ -678,24 +676,115 @@ int ensure_coarse(cfd_ctx* c) {
     CU(cudaMemcpy(c->cs_r[a].p, rng.data(), rng.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
   c->cs_nc = nc;
+  std::vector<int> vox;  // pressure node -> voxel (empty: identity)
+  if (!c->h_pmap.empty()) {
+    vox.assign(c->h_pmap.size(), 0);
+    for (size_t v = 0; v < c->h_pmap.size(); v++) vox[c->h_pmap[v]] = (int)v;
+  }
+  // Z P for the split FP32 iteration (structured form, identity numbering)
+  const bool want_zp = mixed(c) && c->h_pmap.empty();
+  c->cs_zp_ok = false;
+  c->cs_zp.reset();
+  c->cs_wlo.reset();
+  // The Galerkin product, the dense factorisation and the inverse of Zc run
+  // on the device unless CFD_COARSE_HOST=1 keeps them on the host.  A grid
+  // whose rows reach more than 3 coarse nodes per axis (a lattice finer
+  // than Z's reach) builds Zc on the host and factors it on the device.
+  const bool on_device = !c->coarse_on_host;
+  const int ldd = spd_inverse_ld(nc);
+  DevBuf<double> dA, dW;
+  bool zc_on_device = false;
+  if (on_device) {
+    CU(dA.alloc((size_t)ldd * ldd));
+    DevBuf<double> w27;
+    DevBuf<int> dvox, bad, wlo;
+    CU(w27.alloc(27 * (size_t)np));
+    CU(bad.alloc(1));
+    CU(cudaMemsetAsync(bad.p, 0, sizeof(int), c->stream));
+    if (want_zp) {
+      CU(c->cs_zp.alloc(zp_elems(np)));
+      CU(c->cs_wlo.alloc(np));
+    } else {
+      CU(wlo.alloc(np));
+    }
+    if (!vox.empty()) {
+      CU(dvox.alloc(np));
+      CU(cudaMemcpyAsync(dvox.p, vox.data(), np * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    }
+    GalerkinArgs g{};
+    for (int a = 0; a < 3; a++) {
+      g.fd[a] = cs.fd[a];
+      g.cd[a] = cs.cd[a];
+    }
+    g.np = np;
+    g.nc = nc;
+    g.i0x = c->cs_i0[0].p;
+    g.i0y = c->cs_i0[1].p;
+    g.i0z = c->cs_i0[2].p;
+    g.fx = c->cs_f[0].p;
+    g.fy = c->cs_f[1].p;
+    g.fz = c->cs_f[2].p;
+    g.rx = c->cs_r[0].p;
+    g.ry = c->cs_r[1].p;
+    g.rz = c->cs_r[2].p;
+    g.rp = c->z_rp.p;
+    g.col = c->z_col.p;
+    g.val = c->zval.p;
+    g.vox = dvox.p;
+    g.pofv = c->upmap.p;
+    g.w27 = w27.p;
+    g.wlo = want_zp ? c->cs_wlo.p : wlo.p;
+    g.zp = want_zp ? c->cs_zp.p : nullptr;
+    g.bad = bad.p;
+    g.zc = dA.p;
+    g.ld = ldd;
+    CU(launch_galerkin(g, c->stream));
+    int hb = 1;
+    CU(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CU(cudaStreamSynchronize(c->stream));
+    zc_on_device = hb == 0;
+    c->cs_zp_ok = zc_on_device && want_zp;
+    if (!c->cs_zp_ok) {
+      c->cs_zp.reset();
+      c->cs_wlo.reset();
+    }
+  }
+  if (!zc_on_device) {
+    std::vector<double> zv(P.z_col.size());
+    CU(cudaStreamSynchronize(c->stream));
+    CU(cudaMemcpy(zv.data(), c->zval.p, zv.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    std::string err;
+    if (coarse_build(c->udims, kCoarseMaxNodes, vox, P.z_rp, P.z_col, zv, cs, err, want_zp, !on_device,
+                     c->coarse_spacing))
+      return fail(c, CFD_E_NONFINITE, "%s", err.c_str());
+    if (cs.nc != nc) return fail(c, CFD_E_BADARG, "coarse lattice mismatch");
+    if (on_device)
+      CU(cudaMemcpy2D(dA.p, ldd * sizeof(double), cs.inv.data(), nc * sizeof(double), nc * sizeof(double), nc,
+                      cudaMemcpyHostToDevice));
+    if (want_zp && cs.w_ok) {
+      std::vector<float> zp(zp_elems(np), 0.f);
+      for (int p = 0; p < np; p++)
+        for (int t = 0; t < 27; t++)
+          zp[((size_t)(p >> 5) * 27 + t) * 32 + (p & 31)] = (float)cs.w27[27 * (size_t)p + t];
+      CU(c->cs_zp.alloc(zp.size()));
+      CU(cudaMemcpy(c->cs_zp.p, zp.data(), zp.size() * sizeof(float), cudaMemcpyHostToDevice));
+      CU(c->cs_wlo.alloc(np));
+      CU(cudaMemcpy(c->cs_wlo.p, cs.wlo.data(), np * sizeof(int), cudaMemcpyHostToDevice));
+      c->cs_zp_ok = true;
+    }
+  }
   // the inverse goes to the device in FP16 (rows padded to 8 entries),
   // scaled so its largest entry sits near the top of the FP16 range: the
   // coarse correction only has to be close, and halving the bytes of the
   // one dense operand of the iteration matters more
   const int ld = (nc + 7) & ~7;
   if (on_device) {
-    // Zc to the device (leading dimension padded to the factorisation's
-    // tile), Cholesky and inverse in FP64, the scaled FP16 copy in place
-    const int ldd = spd_inverse_ld(nc);
-    DevBuf<double> dA, dW;
+    // Cholesky and inverse in FP64, the scaled FP16 copy in place
     DevBuf<int> dinfo;
     DevBuf<unsigned long long> dmax;
-    CU(dA.alloc((size_t)ldd * ldd));
     CU(dW.alloc((size_t)ldd * ldd));
     CU(dinfo.alloc(1));
     CU(dmax.alloc(1));
-    CU(cudaMemcpy2D(dA.p, ldd * sizeof(double), cs.inv.data(), nc * sizeof(double), nc * sizeof(double), nc,
-                    cudaMemcpyHostToDevice));
     CU(spd_inverse_device(dA.p, dW.p, nc, ldd, dinfo.p, c->stream));
     CU(c->cs_inv16.alloc((size_t)nc * ld));
     CU(spd_inverse_to_half(dA.p, nc, ldd, dmax.p, ld, c->cs_inv16.p, c->stream));
@@ -734,20 +823,6 @@ int ensure_coarse(cfd_ctx* c) {
     const size_t pad = 2 + 2 * (size_t)cs.cd[0] + 2 * (size_t)cs.cd[0] * cs.cd[1];
     CU(c->cs_e32.alloc(nc + pad));
     CU(cudaMemset(c->cs_e32.p, 0, (nc + pad) * sizeof(float)));
-  }
-  c->cs_zp_ok = false;
-  c->cs_zp.reset();
-  c->cs_wlo.reset();
-  if (want_zp && cs.w_ok) {
-    const int np = P.NNp;
-    std::vector<float> zp(zp_elems(np), 0.f);
-    for (int p = 0; p < np; p++)
-      for (int t = 0; t < 27; t++) zp[((size_t)(p >> 5) * 27 + t) * 32 + (p & 31)] = (float)cs.w27[27 * (size_t)p + t];
-    CU(c->cs_zp.alloc(zp.size()));
-    CU(cudaMemcpy(c->cs_zp.p, zp.data(), zp.size() * sizeof(float), cudaMemcpyHostToDevice));
-    CU(c->cs_wlo.alloc(np));
-    CU(cudaMemcpy(c->cs_wlo.p, cs.wlo.data(), np * sizeof(int), cudaMemcpyHostToDevice));
-    c->cs_zp_ok = true;
   }
   // FP32 inner solves on an identity-numbered grid stream Z without column
   // indices (125 coefficients per row) when every coupling stays within two
@@ -1966,6 +2041,76 @@ int cfd_spd_inverse(int device, const double* a, int n, double* inv) {
                      cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return CFD_E_CUDA;
   return info == 0 ? CFD_OK : CFD_E_NONFINITE;
+}
+
+int cfd_coarse_matrix(int device, const int dims[3], const int* rowptr, const int* col, const double* val,
+                      double spacing, int* cd, double* zc) {
+  if (!dims || !rowptr || !col || !val || !cd) return CFD_E_BADARG;
+  const long long n = (long long)dims[0] * dims[1] * dims[2];
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || n > (1LL << 30)) return CFD_E_BADARG;
+  double h[3];
+  coarse_lattice(dims, kCoarseMaxNodes, cd, h, spacing);
+  if (!zc) return CFD_OK;
+  if (cudaSetDevice(device) != cudaSuccess) return CFD_E_CUDA;
+  const int np = (int)n, nc = cd[0] * cd[1] * cd[2];
+  const long long nnz = rowptr[np];
+  if (nnz < 0 || nnz > (1LL << 31) - 1) return CFD_E_BADARG;
+  DevBuf<int> i0[3], rng[3], drp, dcol, wlo, bad;
+  DevBuf<double> f[3], dval, w27, dzc;
+  cudaError_t e = cudaSuccess;
+  for (int a = 0; a < 3 && e == cudaSuccess; a++) {
+    std::vector<int> hi0, hrng;
+    std::vector<double> hf;
+    hat_tables(dims[a], cd[a], h[a], hi0, hf, hrng);
+    e = i0[a].alloc(dims[a]);
+    if (e == cudaSuccess) e = f[a].alloc(dims[a]);
+    if (e == cudaSuccess) e = rng[a].alloc(hrng.size());
+    if (e == cudaSuccess) e = cudaMemcpy(i0[a].p, hi0.data(), dims[a] * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(f[a].p, hf.data(), dims[a] * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(rng[a].p, hrng.data(), hrng.size() * sizeof(int), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = drp.alloc(np + 1);
+  if (e == cudaSuccess) e = dcol.alloc(std::max<long long>(nnz, 1));
+  if (e == cudaSuccess) e = dval.alloc(std::max<long long>(nnz, 1));
+  if (e == cudaSuccess) e = w27.alloc(27 * (size_t)np);
+  if (e == cudaSuccess) e = wlo.alloc(np);
+  if (e == cudaSuccess) e = bad.alloc(1);
+  if (e == cudaSuccess) e = dzc.alloc((size_t)nc * nc);
+  if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? CFD_E_NOMEM : CFD_E_CUDA;
+  e = cudaMemcpy(drp.p, rowptr, (np + 1) * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dcol.p, col, nnz * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dval.p, val, nnz * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(bad.p, 0, sizeof(int));
+  GalerkinArgs g{};
+  for (int a = 0; a < 3; a++) {
+    g.fd[a] = dims[a];
+    g.cd[a] = cd[a];
+  }
+  g.np = np;
+  g.nc = nc;
+  g.i0x = i0[0].p;
+  g.i0y = i0[1].p;
+  g.i0z = i0[2].p;
+  g.fx = f[0].p;
+  g.fy = f[1].p;
+  g.fz = f[2].p;
+  g.rx = rng[0].p;
+  g.ry = rng[1].p;
+  g.rz = rng[2].p;
+  g.rp = drp.p;
+  g.col = dcol.p;
+  g.val = dval.p;
+  g.w27 = w27.p;
+  g.wlo = wlo.p;
+  g.bad = bad.p;
+  g.zc = dzc.p;
+  g.ld = nc;
+  if (e == cudaSuccess) e = launch_galerkin(g, nullptr);
+  int hb = 1;
+  if (e == cudaSuccess) e = cudaMemcpy(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && hb == 0) e = cudaMemcpy(zc, dzc.p, (size_t)nc * nc * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return CFD_E_CUDA;
+  return hb == 0 ? CFD_OK : CFD_E_BADINPUT;
 }
 
 int cfd_selftest_wait_timeout(cfd_ctx* c, int timeout_ms) {

@@ -321,6 +321,28 @@ void fcg2l_neighbor_ranges(int n, int grid, int reach, int* lo, int* hi);
 cudaError_t launch_fcg2l(const FcgArgs<float>& a, const CoarseArgs<float>& ca, const Fcg2lArgs& pa, int grid,
                          cudaStream_t s);
 
+// Galerkin coarse matrix on the device (galerkin.cu): W = Z P in 27-tap
+// boxes and Zc = P^T W, dense and symmetrised, summed in the host build's
+// order (bit-identical to coarse_build on an identity-numbered grid).
+struct GalerkinArgs {
+  int fd[3], cd[3];                // voxel grid, coarse lattice
+  int np, nc;                      // pressure rows, coarse nodes
+  const int *i0x, *i0y, *i0z;      // hat tables per axis (fd entries)
+  const double *fx, *fy, *fz;
+  const int *rx, *ry, *rz;         // per coarse node: first and last fine index of its support
+  const int *rp, *col;             // Z in CSR (pressure numbering)
+  const double* val;
+  const int* vox;                  // pressure node -> voxel (null: identity)
+  const int* pofv;                 // voxel -> pressure node (null: identity)
+  double* w27;                     // np x 27 work: W row by row
+  int* wlo;                        // np: coarse index of each row's box origin
+  float* zp;                       // may be null: W in FP32, 32-row slices (split iteration)
+  int* bad;                        // set when some row's box is wider than 3 nodes
+  double* zc;                      // nc rows of ld doubles (zeroed by the launch)
+  int ld;
+};
+cudaError_t launch_galerkin(const GalerkinArgs& g, cudaStream_t s);
+
 // Dense SPD inverse on the device (dense_chol.cu): A (row-major, leading
 // dimension ld = spd_inverse_ld(n), the n x n matrix in its top-left corner)
 // is replaced by its inverse; work holds ld x ld doubles; *info (device) =

@@ -213,7 +213,9 @@ int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_
     z = v / (fd[0] * fd[1]);
   };
   // W = Z P, row by row: the coarse nodes a row reaches form a small box,
-  // accumulated densely; rows are independent.
+  // accumulated densely; rows are independent.  Both products below use
+  // explicit fused multiply-adds, so the device build (galerkin.cu) can
+  // take the same sums in the same order.
   std::vector<int> lo(3 * (size_t)np), bx(3 * (size_t)np);
   size_t wmax = 1;
 #pragma omp parallel for reduction(max : wmax)
@@ -254,7 +256,8 @@ int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_
         const double wt = (dx ? fx : 1 - fx) * (dy ? fy : 1 - fy) * (dz ? fz : 1 - fz);
         if (wt == 0.0) continue;
         const int jx = ix + dx - l[0], jy = iy + dy - l[1], jz = iz + dz - l[2];
-        w[jx + b[0] * (jy + b[1] * jz)] += val[k] * wt;
+        double& acc = w[jx + b[0] * (jy + b[1] * jz)];
+        acc = std::fma(val[k], wt, acc);
       }
     }
   }
@@ -303,7 +306,8 @@ int coarse_build(const int fd[3], int max_nodes, const std::vector<int>& vox_of_
           for (int jx = 0; jx < b[0]; jx++) {
             const double v = w[jx + b[0] * (jy + b[1] * jz)];
             if (v == 0.0) continue;
-            zi[(l[0] + jx) + cs.cd[0] * ((l[1] + jy) + cs.cd[1] * (l[2] + jz))] += wt * v;
+            double& acc = zi[(l[0] + jx) + cs.cd[0] * ((l[1] + jy) + cs.cd[1] * (l[2] + jz))];
+            acc = std::fma(wt, v, acc);
           }
     }
   }

@@ -116,4 +116,27 @@ int cfdh_coarse_inverse(const int dims[3], const int* rowptr, const int* col, co
   return CFD_OK;
 }
 
+int cfdh_coarse_matrix(const int dims[3], const int* rowptr, const int* col, const double* val, double spacing,
+                       int* cd, double* zc) {
+  if (!dims || !rowptr || !col || !val || !cd) return CFD_E_BADARG;
+  const long long n = (long long)dims[0] * dims[1] * dims[2];
+  if (dims[0] < 1 || dims[1] < 1 || dims[2] < 1 || n > (1LL << 30)) return CFD_E_BADARG;
+  const int kMaxNodes = 6000;
+  if (!zc) {
+    double h[3];
+    cfd::coarse_lattice(dims, kMaxNodes, cd, h, spacing);
+    return CFD_OK;
+  }
+  std::vector<int> rp(rowptr, rowptr + n + 1);
+  std::vector<int> cl(col, col + rp[n]);
+  std::vector<double> vl(val, val + rp[n]);
+  cfd::CoarseSpace cs;
+  std::string err;
+  if (cfd::coarse_build(dims, kMaxNodes, std::vector<int>(), rp, cl, vl, cs, err, false, false, spacing))
+    return CFD_E_NONFINITE;
+  for (int a = 0; a < 3; a++) cd[a] = cs.cd[a];
+  std::copy(cs.inv.begin(), cs.inv.end(), zc);
+  return CFD_OK;
+}
+
 }  // extern "C"

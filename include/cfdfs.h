@@ -325,6 +325,19 @@ int cfd_profile_fcg2l(cfd_ctx* ctx, double* out10);
  * positive.  No counterpart in the reference. */
 int cfd_spd_inverse(int device, const double* a, int n, double* inv);
 
+/* Galerkin coarse matrix Zc = P^T Z P of the two-level preconditioner built
+ * on the given device, for a CSR matrix Z (host buffers, n rows, FP64) on a
+ * structured grid dims (product = n, identity numbering x + nx (y + ny z)),
+ * with a coarse lattice of about `spacing` fine steps (4 in the solver).
+ * cd receives the coarse nodes per axis; zc (NULL: only the sizes) the
+ * dense nc x nc matrix, nc = cd[0] cd[1] cd[2] (at most 6000), summed in
+ * the order of cfdh_coarse_matrix and bit-identical to it.
+ * CFD_E_BADINPUT when a row of Z reaches more than 3 coarse nodes per axis
+ * (the solver then builds Zc on the host).  No counterpart in the
+ * reference. */
+int cfd_coarse_matrix(int device, const int dims[3], const int* rowptr, const int* col, const double* val,
+                      double spacing, int* cd, double* zc);
+
 /* Runs one small kernel whose bounded wait watches a flag nothing sets, with
  * the given limit in milliseconds.  Returns CFD_E_TIMEOUT when the wait gave
  * up as designed (the context stays usable), CFD_OK otherwise. */
@@ -374,6 +387,11 @@ int cfdh_get_bcnodes(const cfd_host* h, int* out);  /* nBCnodes x 2 (node, bc) *
  * (at most 6000).  Host only; no counterpart in the reference. */
 int cfdh_coarse_inverse(const int dims[3], const int* rowptr, const int* col, const double* val, int* cd,
                         double* inv);
+/* The same coarse space's matrix Zc = P^T Z P itself (dense, symmetrised),
+ * with the coarse spacing given (4 in the solver): the host counterpart of
+ * cfd_coarse_matrix.  Host only; no counterpart in the reference. */
+int cfdh_coarse_matrix(const int dims[3], const int* rowptr, const int* col, const double* val, double spacing,
+                       int* cd, double* zc);
 /* Element colouring of the deterministic mode (setupMeshColoring,
  * blascoCodinaHuerta.cpp:853-947): returns the number of colours C (or -1
  * beyond 64); order (NE, may be NULL) lists the elements colour by colour,

@@ -67,3 +67,53 @@ def test_twolevel_run_device_coarse_matches_host_coarse(tmp_path):
     (sa, Ua, Pa), (sb, Ub, Pb) = out
     assert sa.subiters == sb.subiters and abs(sa.cg_iters - sb.cg_iters) <= sa.subiters
     assert rel_l2(Ua, Ub) < 1e-5 and rel_l2(Pa, Pb) < 1e-5
+
+
+@pytest.mark.parametrize("case", ["cavity", "duct", "laplace65", "laplace_ragged"])
+def test_device_coarse_matrix_is_bit_identical(case, tmp_path, oracle_mod):
+    """The Galerkin product on the device (galerkin.cu) against the host
+    build: the same sums in the same order, so the same bits."""
+    import cfdfs
+    from cfdfs import meshgen
+    if case in ("cavity", "duct"):
+        if case == "cavity":
+            deck = meshgen.write_cavity(str(tmp_path / "c.inp"), meshgen.CavitySpec(12, re=100, dt=0.01, steps=2))
+            dims = (13, 13, 13)
+        else:
+            deck = meshgen.write_duct(str(tmp_path / "d.inp"), n_cross=4, n_axial=24, steps=2, dt=0.01)
+            dims = meshgen.duct_grid_dims(4, 24)
+        o = oracle_mod.Oracle(deck)
+        o.step0()
+        Z = o.csr("Z").tocsr()
+        o.close()
+    else:
+        dims = (65, 65, 65) if case == "laplace65" else (29, 21, 17)
+        Z = _laplace7(dims, 0.05)
+        Z.sort_indices()
+        rng = np.random.default_rng(7)
+        Z.data = Z.data * (1.0 + 1e-3 * rng.standard_normal(Z.data.size))
+    rp, cl = Z.indptr.astype(np.int32), Z.indices.astype(np.int32)
+    cd_h, zc_h = cfdfs.coarse_matrix(dims, rp, cl, Z.data)
+    cd_d, zc_d = cfdfs.coarse_matrix(dims, rp, cl, Z.data, device=0)
+    assert cd_h == cd_d
+    assert np.array_equal(zc_h, zc_d)
+
+
+def test_device_coarse_matrix_rejects_a_fine_lattice(tmp_path, oracle_mod):
+    """A lattice finer than Z's reach (spacing 1.5 voxels against a matrix
+    that couples nodes two voxels apart) leaves rows reaching more than 3
+    coarse nodes per axis: the device build reports it, the host build
+    still works."""
+    import cfdfs
+    from cfdfs import meshgen
+    deck = meshgen.write_cavity(str(tmp_path / "c.inp"), meshgen.CavitySpec(6, re=100, dt=0.01, steps=2))
+    dims = (7, 7, 7)
+    o = oracle_mod.Oracle(deck)
+    o.step0()
+    Z = o.csr("Z").tocsr()
+    o.close()
+    rp, cl = Z.indptr.astype(np.int32), Z.indices.astype(np.int32)
+    with pytest.raises(cfdfs.CfdError):
+        cfdfs.coarse_matrix(dims, rp, cl, Z.data, spacing=1.5, device=0)
+    cd, zc = cfdfs.coarse_matrix(dims, rp, cl, Z.data, spacing=1.5)
+    assert np.array_equal(zc, zc.T)

@@ -91,3 +91,31 @@ def test_coarse_inverse_multi_panel(dims):
     assert int(np.prod(cd)) > 96 * 2
     ref = np.linalg.inv((P.T @ Z @ P).toarray())
     assert rel_l2(inv, ref) < 1e-10
+
+
+def _hats_s(n, s):
+    return _hats(n, s)
+
+
+@pytest.mark.parametrize("case,spacing", [("cavity", 4.0), ("duct", 4.0), ("cavity", 3.0)])
+def test_coarse_matrix_matches_scipy(case, spacing, tmp_path, oracle_mod):
+    """The Galerkin product itself (cfdh_coarse_matrix, the host build that
+    the device build reproduces bit for bit) against SciPy's P^T Z P."""
+    import cfdfs
+    from cfdfs import meshgen
+    if case == "cavity":
+        deck = meshgen.write_cavity(str(tmp_path / "c.inp"), meshgen.CavitySpec(12, re=100, dt=0.01, steps=2, ngp=8))
+        dims = (13, 13, 13)
+    else:
+        deck = meshgen.write_duct(str(tmp_path / "d.inp"), n_cross=4, n_axial=24, steps=2, dt=0.01)
+        dims = meshgen.duct_grid_dims(4, 24)
+    o = oracle_mod.Oracle(deck)
+    o.step0()
+    Z = o.csr("Z").tocsr()
+    o.close()
+    cd, zc = cfdfs.coarse_matrix(dims, Z.indptr, Z.indices, Z.data, spacing=spacing)
+    P = sp.kron(_hats_s(dims[2], spacing), sp.kron(_hats_s(dims[1], spacing), _hats_s(dims[0], spacing))).tocsr()
+    assert cd == tuple(_hats_s(n, spacing).shape[1] for n in dims)
+    ref = (P.T @ Z @ P).toarray()
+    assert rel_l2(zc, ref) < 1e-13
+    assert np.array_equal(zc, zc.T)
