@@ -9,14 +9,24 @@
 //   c_k^d  = u0_k . grad(uprev^d)(k)       (u0_k interpolated from Un)
 //   R1e_i^d = sum_k Sv_i(k) detJ_k w_k c_k^d
 // with grad(uprev^d)(k) = J_k^{-1} (sum_j dSv_j(k) uprev_j^d), J_k rebuilt
-// from the 8 corner coordinates.  One thread per (element, Gauss point);
-// elements and their gathered nodal values sit in shared memory; results are
-// scattered with FP64 atomics (no element colouring; in mixed precision as
-// one FP32 16-byte vector reduction per element node into an FP32 copy of
-// the term), or, in deterministic mode, one colour per launch with plain
-// adds in a fixed order.  Work per element is
-// about 30x fewer flops than the Ae form, so the kernel is bound by the
-// gathers of Un / UnpHalf_prev and the atomic scatter, not by arithmetic.
+// from the 8 corner coordinates.  Work per element is about 30x fewer flops
+// than the Ae form, so the kernel is bound by the L1 data pipe: the gathers
+// of Un / UnpHalf_prev and the shared-memory operand reads of the
+// Gauss-point sums.  The layout keeps both low:
+// - a block takes EPB consecutive elements; their connectivity is read
+//   element by element (27 contiguous ints), then the nodal values and
+//   corner coordinates are gathered with consecutive threads on consecutive
+//   elements at the same local node, which for a structured numbering are
+//   neighbouring nodes (few cache lines per warp request);
+// - TPE threads share an element, each owning GPT Gauss points: a nodal
+//   value read from shared memory serves GPT Gauss points, and a warp reads
+//   the basis values of only TPE Gauss points per node at a time;
+// - the scatter again runs consecutive threads over consecutive elements.
+// Results are scattered with FP64 atomics (no element colouring; in mixed
+// precision as one FP32 16-byte vector reduction per element node into an
+// FP32 copy of the term), or, in deterministic mode, one colour per launch
+// with plain adds.  Every sum runs in the same order whatever the layout:
+// over nodes j for a Gauss point, over Gauss points k for a node.
 #include "kernels.h"
 
 namespace cfd {
@@ -38,33 +48,50 @@ struct alignas(4 * sizeof(T)) Quad {
   T x, y, z, w;
 };
 
-template <class T, int TPE>
+// Shared-memory carve-up of one block (byte offsets, each a multiple of 32,
+// the alignment of Quad<double>).
+constexpr size_t round32(size_t b) { return (b + 31) & ~size_t(31); }
+template <class T, int TPE, int GPT>
+struct ConvSmem {
+  static constexpr int EPB = kConvThreads / TPE;
+  static constexpr int NG = TPE * GPT;  // Gauss points a block can hold
+  static constexpr int NGP = NG + 1;    // padded row of cc (no bank conflicts across elements)
+  static constexpr size_t sB = 0;                                                // Quad<T>[NG][27]
+  static constexpr size_t sdSp = sB + round32(sizeof(Quad<T>) * NG * 27);       // T[3][NG][8]
+  static constexpr size_t sw = sdSp + round32(sizeof(T) * 3 * NG * 8);           // T[NG]
+  static constexpr size_t u0 = sw + round32(sizeof(T) * NG);                     // Quad<T>[EPB][27]
+  static constexpr size_t up = u0 + round32(sizeof(Quad<T>) * EPB * 27);         // Quad<T>[EPB][27]
+  static constexpr size_t cc = up + round32(sizeof(Quad<T>) * EPB * 27);         // Quad<T>[EPB][NGP]
+  static constexpr size_t X = cc + round32(sizeof(Quad<T>) * EPB * NGP);         // T[EPB][25]
+  static constexpr size_t lt = X + round32(sizeof(T) * EPB * 25);                // int[EPB][27]
+  static constexpr size_t bytes = lt + round32(sizeof(int) * EPB * 27);
+};
+
+template <class T, int TPE, int GPT>
 __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
-  constexpr int EPB = kConvThreads / TPE;
-  constexpr int NG = TPE < kMaxNGP ? TPE : kMaxNGP;
-  // operands of the Gauss-point loops packed four to a vector load: the
-  // loops are bound by shared-memory instructions, not by their FMAs
-  __shared__ Quad<T> sB[NG][27];  // {Sv, dSv/dxi, dSv/deta, dSv/dzeta}
-  __shared__ T sdSp[3][NG][8];
-  __shared__ T sw[NG];
-  __shared__ Quad<T> u0[EPB][27];
-  __shared__ Quad<T> up[EPB][27];
-  __shared__ T X[EPB][8][3];
-  __shared__ Quad<T> cc[EPB][NG];
-  __shared__ int lt[EPB][27];
+  using L = ConvSmem<T, TPE, GPT>;
+  constexpr int EPB = L::EPB, NG = L::NG, NGP = L::NGP;
+  extern __shared__ __align__(32) unsigned char smem[];
+  auto sB = reinterpret_cast<Quad<T>(*)[27]>(smem + L::sB);  // {Sv, dSv/dxi, dSv/deta, dSv/dzeta}
+  auto sdSp = reinterpret_cast<T(*)[NG][8]>(smem + L::sdSp);
+  T* sw = reinterpret_cast<T*>(smem + L::sw);
+  auto u0 = reinterpret_cast<Quad<T>(*)[27]>(smem + L::u0);
+  auto up = reinterpret_cast<Quad<T>(*)[27]>(smem + L::up);
+  auto cc = reinterpret_cast<Quad<T>(*)[NGP]>(smem + L::cc);
+  auto X = reinterpret_cast<T(*)[25]>(smem + L::X);  // corner m, coordinate d at 3 m + d
+  auto lt = reinterpret_cast<int(*)[27]>(smem + L::lt);
   const int t = threadIdx.x, ngp = a.ngp;
   const Basis* B = a.basis;
-  for (int i = t; i < ngp * 27; i += blockDim.x) {
-    int k = i / 27, j = i % 27;
-    sB[k][j] = Quad<T>{(T)B->Sv[k][j], (T)B->dSv[0][k][j], (T)B->dSv[1][k][j], (T)B->dSv[2][k][j]};
+  for (int i = t; i < NG * 27; i += blockDim.x) {
+    const int k = i / 27, j = i % 27;
+    sB[k][j] = k < ngp ? Quad<T>{(T)B->Sv[k][j], (T)B->dSv[0][k][j], (T)B->dSv[1][k][j], (T)B->dSv[2][k][j]}
+                       : Quad<T>{T(0), T(0), T(0), T(0)};
   }
-  for (int i = t; i < ngp * 8; i += blockDim.x) {
-    int k = i / 8, m = i % 8;
-    sdSp[0][k][m] = (T)B->dSp[0][k][m];
-    sdSp[1][k][m] = (T)B->dSp[1][k][m];
-    sdSp[2][k][m] = (T)B->dSp[2][k][m];
+  for (int i = t; i < NG * 8; i += blockDim.x) {
+    const int k = i / 8, m = i % 8;
+    for (int d = 0; d < 3; d++) sdSp[d][k][m] = k < ngp ? (T)B->dSp[d][k][m] : T(0);
   }
-  for (int i = t; i < ngp; i += blockDim.x) sw[i] = (T)B->w[i];
+  for (int i = t; i < NG; i += blockDim.x) sw[i] = i < ngp ? (T)B->w[i] : T(0);
   const int el = t / TPE, tk = t % TPE;
   // element of local slot l in this pass (-1 past the range)
   auto elem_of = [&](int p0, int l) -> int {
@@ -73,115 +100,156 @@ __global__ void __launch_bounds__(kConvThreads) k_convect(ConvArgs<T> a) {
   };
   for (int p0 = a.e_begin + blockIdx.x * EPB; p0 < a.e_end; p0 += gridDim.x * EPB) {
     __syncthreads();
+    // connectivity, element by element (contiguous rows of ltog)
     for (int idx = t; idx < EPB * 27; idx += blockDim.x) {
-      int l = idx / 27, i = idx % 27, e = elem_of(p0, l);
-      if (e >= 0) {
-        int node = __ldg(a.ltog + (size_t)e * 27 + i);
-        lt[l][i] = node;
+      const int l = idx / 27, i = idx % 27, e = elem_of(p0, l);
+      lt[l][i] = e >= 0 ? __ldg(a.ltog + (size_t)e * 27 + i) : 0;
+    }
+    __syncthreads();
+    // nodal values and corner coordinates, consecutive threads on
+    // consecutive elements at one local node
+    for (int idx = t; idx < EPB * 27; idx += blockDim.x) {
+      const int l = idx % EPB, i = idx / EPB;
+      if (elem_of(p0, l) >= 0) {
+        const int node = lt[l][i];
         const auto u = ldgv(a.un + node);
         const auto p = ldgv(a.uprev + node);
         u0[l][i] = Quad<T>{(T)u.x, (T)u.y, (T)u.z, T(0)};
         up[l][i] = Quad<T>{(T)p.x, (T)p.y, (T)p.z, T(0)};
       }
     }
-    __syncthreads();
     for (int idx = t; idx < EPB * 24; idx += blockDim.x) {
-      int l = idx / 24, r = idx % 24, e = elem_of(p0, l);
-      if (e >= 0) X[l][r / 3][r % 3] = (T)__ldg(a.coord + 3 * (size_t)lt[l][r / 3] + r % 3);
+      const int l = idx % EPB, r = idx / EPB;
+      if (elem_of(p0, l) >= 0) X[l][r] = (T)__ldg(a.coord + 3 * (size_t)lt[l][r / 3] + r % 3);
     }
     __syncthreads();
     const int e = elem_of(p0, el);
-    if (e >= 0 && tk < ngp) {
-      const int k = tk;
-      // Jacobian of the trilinear corner map at Gauss point k
-      T J[3][3];
+    if (e >= 0) {
+      // u0 at the thread's Gauss points k = tk + TPE g and reference-space
+      // gradients of uprev (g[.][a][d] = d uprev^d / d xi_a), summed over j
+      T uk[GPT][3], gr[GPT][3][3];
 #pragma unroll
-      for (int i = 0; i < 3; i++)
+      for (int g = 0; g < GPT; g++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) {
-          T s = 0;
-#pragma unroll
-          for (int m = 0; m < 8; m++) s += sdSp[i][k][m] * X[el][m][j];
-          J[i][j] = s;
+        for (int d = 0; d < 3; d++) {
+          uk[g][d] = 0;
+          gr[g][0][d] = gr[g][1][d] = gr[g][2][d] = 0;
         }
-      T det = J[0][0] * (J[1][1] * J[2][2] - J[2][1] * J[1][2]) + J[0][1] * (J[1][2] * J[2][0] - J[1][0] * J[2][2]) +
-              J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
-      T inv = T(1) / det;
-      T iJ[3][3];
-      iJ[0][0] = (J[1][1] * J[2][2] - J[2][1] * J[1][2]) * inv;
-      iJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) * inv;
-      iJ[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * inv;
-      iJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) * inv;
-      iJ[1][1] = (J[2][2] * J[0][0] - J[2][0] * J[0][2]) * inv;
-      iJ[1][2] = -(J[1][2] * J[0][0] - J[1][0] * J[0][2]) * inv;
-      iJ[2][0] = (J[1][0] * J[2][1] - J[2][0] * J[1][1]) * inv;
-      iJ[2][1] = -(J[2][1] * J[0][0] - J[2][0] * J[0][1]) * inv;
-      iJ[2][2] = (J[1][1] * J[0][0] - J[1][0] * J[0][1]) * inv;
-      // u0 at the Gauss point and reference-space gradients of uprev
-      T uk[3] = {0, 0, 0};
-      T g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};  // g[a][d] = d uprev^d / d xi_a
 #pragma unroll 3
       for (int j = 0; j < 27; j++) {
-        const Quad<T> bs = sB[k][j], ua = u0[el][j], ub = up[el][j];
-        const T sv = bs.x, d0 = bs.y, d1 = bs.z, d2 = bs.w;
-        const T a0 = ua.x, a1 = ua.y, a2 = ua.z;
-        const T b0 = ub.x, b1 = ub.y, b2 = ub.z;
-        uk[0] += sv * a0; uk[1] += sv * a1; uk[2] += sv * a2;
-        g[0][0] += d0 * b0; g[0][1] += d0 * b1; g[0][2] += d0 * b2;
-        g[1][0] += d1 * b0; g[1][1] += d1 * b1; g[1][2] += d1 * b2;
-        g[2][0] += d2 * b0; g[2][1] += d2 * b1; g[2][2] += d2 * b2;
-      }
-      const T f = det * sw[k];
-      T ck[3];
+        const Quad<T> ua = u0[el][j], ub = up[el][j];
 #pragma unroll
-      for (int d = 0; d < 3; d++) {
-        // physical gradient of uprev^d: grad_i = sum_a iJ[i][a] g[a][d]
-        T gx = iJ[0][0] * g[0][d] + iJ[0][1] * g[1][d] + iJ[0][2] * g[2][d];
-        T gy = iJ[1][0] * g[0][d] + iJ[1][1] * g[1][d] + iJ[1][2] * g[2][d];
-        T gz = iJ[2][0] * g[0][d] + iJ[2][1] * g[1][d] + iJ[2][2] * g[2][d];
-        ck[d] = (uk[0] * gx + uk[1] * gy + uk[2] * gz) * f;
+        for (int g = 0; g < GPT; g++) {
+          const Quad<T> bs = sB[tk + TPE * g][j];
+          uk[g][0] += bs.x * ua.x; uk[g][1] += bs.x * ua.y; uk[g][2] += bs.x * ua.z;
+          gr[g][0][0] += bs.y * ub.x; gr[g][0][1] += bs.y * ub.y; gr[g][0][2] += bs.y * ub.z;
+          gr[g][1][0] += bs.z * ub.x; gr[g][1][1] += bs.z * ub.y; gr[g][1][2] += bs.z * ub.z;
+          gr[g][2][0] += bs.w * ub.x; gr[g][2][1] += bs.w * ub.y; gr[g][2][2] += bs.w * ub.z;
+        }
       }
-      cc[el][k] = Quad<T>{ck[0], ck[1], ck[2], T(0)};
+#pragma unroll
+      for (int g = 0; g < GPT; g++) {
+        const int k = tk + TPE * g;
+        if (k >= ngp) {
+          cc[el][k] = Quad<T>{T(0), T(0), T(0), T(0)};
+          continue;
+        }
+        // Jacobian of the trilinear corner map at Gauss point k
+        T J[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int jj = 0; jj < 3; jj++) {
+            T s = 0;
+#pragma unroll
+            for (int m = 0; m < 8; m++) s += sdSp[i][k][m] * X[el][3 * m + jj];
+            J[i][jj] = s;
+          }
+        const T det = J[0][0] * (J[1][1] * J[2][2] - J[2][1] * J[1][2]) +
+                      J[0][1] * (J[1][2] * J[2][0] - J[1][0] * J[2][2]) +
+                      J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+        const T inv = T(1) / det;
+        T iJ[3][3];
+        iJ[0][0] = (J[1][1] * J[2][2] - J[2][1] * J[1][2]) * inv;
+        iJ[0][1] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]) * inv;
+        iJ[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * inv;
+        iJ[1][0] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]) * inv;
+        iJ[1][1] = (J[2][2] * J[0][0] - J[2][0] * J[0][2]) * inv;
+        iJ[1][2] = -(J[1][2] * J[0][0] - J[1][0] * J[0][2]) * inv;
+        iJ[2][0] = (J[1][0] * J[2][1] - J[2][0] * J[1][1]) * inv;
+        iJ[2][1] = -(J[2][1] * J[0][0] - J[2][0] * J[0][1]) * inv;
+        iJ[2][2] = (J[1][1] * J[0][0] - J[1][0] * J[0][1]) * inv;
+        const T f = det * sw[k];
+        T ck[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          // physical gradient of uprev^d: grad_i = sum_a iJ[i][a] g[a][d]
+          const T gx = iJ[0][0] * gr[g][0][d] + iJ[0][1] * gr[g][1][d] + iJ[0][2] * gr[g][2][d];
+          const T gy = iJ[1][0] * gr[g][0][d] + iJ[1][1] * gr[g][1][d] + iJ[1][2] * gr[g][2][d];
+          const T gz = iJ[2][0] * gr[g][0][d] + iJ[2][1] * gr[g][1][d] + iJ[2][2] * gr[g][2][d];
+          ck[d] = (uk[g][0] * gx + uk[g][1] * gy + uk[g][2] * gz) * f;
+        }
+        cc[el][k] = Quad<T>{ck[0], ck[1], ck[2], T(0)};
+      }
     }
     __syncthreads();
-    if (e >= 0) {
-      for (int i = tk; i < 27; i += TPE) {
-        T s0 = 0, s1 = 0, s2 = 0;
-        for (int k = 0; k < ngp; k++) {
-          const T sv = sB[k][i].x;
-          const Quad<T> ck = cc[el][k];
-          s0 += sv * ck.x;
-          s1 += sv * ck.y;
-          s2 += sv * ck.z;
-        }
-        if constexpr (sizeof(T) == 4) {
-          if (a.r1f) {
-            float4* df = a.r1f + lt[el][i];
-            if (a.plain) {
-              float4 o = *df;
-              o.x -= (float)s0;
-              o.y -= (float)s1;
-              o.z -= (float)s2;
-              *df = o;
-            } else {
-              red_add_v4_f32(df, -(float)s0, -(float)s1, -(float)s2, 0.f);
-            }
-            continue;
+    // R1e_i^d = sum_k Sv_i(k) c_k^d, consecutive threads on consecutive
+    // elements at one local node
+    for (int idx = t; idx < EPB * 27; idx += blockDim.x) {
+      const int l = idx % EPB, i = idx / EPB;
+      if (elem_of(p0, l) < 0) continue;
+      T s0 = 0, s1 = 0, s2 = 0;
+      for (int k = 0; k < ngp; k++) {
+        const T sv = sB[k][i].x;
+        const Quad<T> ck = cc[l][k];
+        s0 += sv * ck.x;
+        s1 += sv * ck.y;
+        s2 += sv * ck.z;
+      }
+      const int node = lt[l][i];
+      if constexpr (sizeof(T) == 4) {
+        if (a.r1f) {
+          float4* df = a.r1f + node;
+          if (a.plain) {
+            float4 o = *df;
+            o.x -= (float)s0;
+            o.y -= (float)s1;
+            o.z -= (float)s2;
+            *df = o;
+          } else {
+            red_add_v4_f32(df, -(float)s0, -(float)s1, -(float)s2, 0.f);
           }
+          continue;
         }
-        double4* dst = a.r1 + lt[el][i];
-        if (a.plain) {  // one colour per launch: no other element of it touches this node
-          dst->x -= (double)s0;
-          dst->y -= (double)s1;
-          dst->z -= (double)s2;
-        } else {
-          atomicAdd(&dst->x, -(double)s0);
-          atomicAdd(&dst->y, -(double)s1);
-          atomicAdd(&dst->z, -(double)s2);
-        }
+      }
+      double4* dst = a.r1 + node;
+      if (a.plain) {  // one colour per launch: no other element of it touches this node
+        dst->x -= (double)s0;
+        dst->y -= (double)s1;
+        dst->z -= (double)s2;
+      } else {
+        atomicAdd(&dst->x, -(double)s0);
+        atomicAdd(&dst->y, -(double)s1);
+        atomicAdd(&dst->z, -(double)s2);
       }
     }
   }
+}
+
+template <class T, int TPE, int GPT>
+cudaError_t launch_convect_cfg(const ConvArgs<T>& a, int ne, int num_sms, cudaStream_t s) {
+  using L = ConvSmem<T, TPE, GPT>;
+  auto k = k_convect<T, TPE, GPT>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::bytes);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kConvThreads, L::bytes);
+  if (e != cudaSuccess) return e;
+  int grid = (ne + L::EPB - 1) / L::EPB;
+  const int cap = num_sms * (per_sm > 0 ? per_sm : 1);
+  if (grid > cap) grid = cap;
+  k<<<grid, kConvThreads, L::bytes, s>>>(a);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -190,18 +258,11 @@ template <class T>
 cudaError_t launch_convect(const ConvArgs<T>& a, int num_sms, cudaStream_t s) {
   const int ne = a.e_end - a.e_begin;
   if (ne <= 0) return cudaSuccess;
-  if (a.ngp <= 8) {
-    constexpr int EPB = kConvThreads / 8;
-    int grid = (ne + EPB - 1) / EPB;
-    if (grid > num_sms * 12) grid = num_sms * 12;
-    k_convect<T, 8><<<grid, kConvThreads, 0, s>>>(a);
-  } else {
-    constexpr int EPB = kConvThreads / 32;
-    int grid = (ne + EPB - 1) / EPB;
-    if (grid > num_sms * 12) grid = num_sms * 12;
-    k_convect<T, 32><<<grid, kConvThreads, 0, s>>>(a);
-  }
-  return cudaGetLastError();
+  if (a.ngp > kMaxNGP || a.ngp < 1) return cudaErrorInvalidValue;
+  // 4 threads per element, 32 elements per block: 2 Gauss points per thread
+  // at NGP 8, 7 at NGP 27
+  if (a.ngp <= 8) return launch_convect_cfg<T, 4, 2>(a, ne, num_sms, s);
+  return launch_convect_cfg<T, 4, 7>(a, ne, num_sms, s);
 }
 
 template cudaError_t launch_convect<double>(const ConvArgs<double>&, int, cudaStream_t);
