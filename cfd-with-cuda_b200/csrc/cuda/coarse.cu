@@ -19,39 +19,62 @@ namespace cfd {
 
 namespace {
 
-// c = P^T r: one warp per coarse node.  The lanes stride over the node's
-// support box (at most (2h + 1)^3 fine nodes, x fastest), each adding
-// w(x) w(y) w(z) r in FP64 in a fixed order, then a warp sum.  4913 warps
-// at 65^3 are resident at once, so the launch is a single wave.
-constexpr int kRestrictThreads = 256;
+// c = P^T r, separably: one block per coarse (iy, iz) pair.  The block's
+// fine x-lines (the y-z support of the pair, weights wy wz kept in shared
+// memory) are summed by G groups of fd[0] threads, each thread one fine x
+// over every G-th line (independent loads), the group partials are added,
+// and warps restrict the resulting fine x-line onto the coarse x-nodes.
+constexpr int kRestrictThreads = 512;
+constexpr int kRestrictLines = 1024;  // y-z support lines per coarse pair at most
 template <class VT>
 __global__ void __launch_bounds__(kRestrictThreads) k_restrict(CoarseArgs<VT> a, const VT* __restrict__ r,
                                                                float* __restrict__ c, const int* done) {
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
-  const int node = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (node >= a.nc) return;
+  extern __shared__ double sline[];  // G x fd[0] partial sums
+  __shared__ double swt[kRestrictLines];
+  __shared__ int sbase[kRestrictLines];
   const int cx = a.cd[0], cy = a.cd[1];
-  const int ix = node % cx, iy = (node / cx) % cy, iz = node / (cx * cy);
-  const int x0 = a.rx[2 * ix], nx = a.rx[2 * ix + 1] - x0 + 1;
+  const int iy = blockIdx.x % cy, iz = blockIdx.x / cy;
   const int y0 = a.ry[2 * iy], ny = a.ry[2 * iy + 1] - y0 + 1;
   const int z0 = a.rz[2 * iz], nz = a.rz[2 * iz + 1] - z0 + 1;
-  const int nxy = nx * ny, S = nxy * nz;
   const int fx = a.fd[0], fxy = a.fd[0] * a.fd[1];
-  double acc = 0.0;
-#pragma unroll 4
-  for (int t = lane; t < S; t += 32) {
-    const int z = z0 + t / nxy, rem = t - (t / nxy) * nxy;
-    const int y = y0 + rem / nx, x = x0 + rem - (rem / nx) * nx;
-    const double wx = a.i0x[x] == ix ? 1.0 - a.fx[x] : (a.i0x[x] + 1 == ix ? a.fx[x] : 0.0);
+  const int nl = ny * nz;
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) {
+    const int y = y0 + l % ny, z = z0 + l / ny;
     const double wy = a.i0y[y] == iy ? 1.0 - a.fy[y] : (a.i0y[y] + 1 == iy ? a.fy[y] : 0.0);
     const double wz = a.i0z[z] == iz ? 1.0 - a.fz[z] : (a.i0z[z] + 1 == iz ? a.fz[z] : 0.0);
-    const int v = x + fx * y + fxy * z;
-    acc += (wx * wy * wz) * (double)r[a.pmap ? a.pmap[v] : v];
+    swt[l] = wy * wz;
+    sbase[l] = fx * y + fxy * z;
   }
-  acc = warp_sum(acc);
-  if (lane == 0) c[node] = (float)acc;
+  __syncthreads();
+  const int G = fx <= (int)blockDim.x ? (int)blockDim.x / fx : 1;
+  const int g = threadIdx.x / fx;
+  for (int x = threadIdx.x % fx; g < G && x < fx; x += (G == 1 ? (int)blockDim.x : fx)) {
+    double acc = 0.0;
+#pragma unroll 4
+    for (int l = g; l < nl; l += G) {
+      const int v = sbase[l] + x;
+      acc += swt[l] * (double)r[a.pmap ? a.pmap[v] : v];
+    }
+    sline[g * fx + x] = acc;
+    if (G != 1) break;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int ix = warp; ix < cx; ix += blockDim.x >> 5) {
+    const int x0 = a.rx[2 * ix], x1 = a.rx[2 * ix + 1];
+    double acc = 0.0;
+    for (int x = x0 + lane; x <= x1; x += 32) {
+      const double wx = a.i0x[x] == ix ? 1.0 - a.fx[x] : (a.i0x[x] + 1 == ix ? a.fx[x] : 0.0);
+      double sx = 0.0;
+      for (int gg = 0; gg < G; gg++) sx += sline[gg * fx + x];
+      acc += wx * sx;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) c[ix + cx * (iy + cy * iz)] = (float)acc;
+  }
 }
 
 // sum_i h[i] c[i] over 8 FP16 entries packed in q and 8 FP32 values at c
@@ -63,12 +86,12 @@ __device__ __forceinline__ float dot8(const uint4& q, const float* c) {
          (f3.x * c1.z + f3.y * c1.w);
 }
 
-// e = inv c: one warp per row (eight rows per block), each lane with up to
-// eight 16-byte loads (8 FP16 entries each) in flight, FP32 products with c
-// (read through L1), warp sum.  All rows' warps are resident at once (4913
-// at 65^3), so the launch is a single wave.  The inverse is read with an
-// evict-last L2 policy (the SpMV's matrix stream is evict-first).
-constexpr int kMvThreads = 256;
+// e = inv c: one block of four warps per row, every thread with its share
+// of the row's 16-byte loads (8 FP16 entries each) in flight at once, FP32
+// products with c (read through L1), block sum.  The inverse is read with
+// an evict-last L2 policy (the SpMV's matrix stream is evict-first), so it
+// stays in L2 from one flexible-CG iteration to the next.
+constexpr int kMvThreads = 128;
 template <class VT>
 __global__ void __launch_bounds__(kMvThreads) k_coarse_mv(int nc, int ld, const __half* __restrict__ inv, float rscale,
                                                           const float* __restrict__ c, VT* __restrict__ e,
@@ -76,24 +99,31 @@ __global__ void __launch_bounds__(kMvThreads) k_coarse_mv(int nc, int ld, const 
   pdl_wait();
   pdl_trigger();
   if (done && *done) return;
-  const int row = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (row >= nc) return;
+  const int row = blockIdx.x;
   const int nv8 = nc >> 3, tail = nc & 7;  // whole 8-entry groups inside the row, then a tail
   const uint4* ir = reinterpret_cast<const uint4*>(inv + (size_t)row * ld);
   const unsigned long long keep = l2_evict_last();
   float s[4] = {0.f, 0.f, 0.f, 0.f};
-  int k = lane;
-  for (; k + 7 * 32 < nv8; k += 8 * 32) {
-    uint4 q[8];
+  int k = threadIdx.x;
+  for (; k + 3 * kMvThreads < nv8; k += 4 * kMvThreads) {
+    uint4 q[4];
 #pragma unroll
-    for (int u = 0; u < 8; u++) q[u] = ldg_hint(ir + k + u * 32, keep);
+    for (int u = 0; u < 4; u++) q[u] = ldg_hint(ir + k + u * kMvThreads, keep);
 #pragma unroll
-    for (int u = 0; u < 8; u++) s[u & 3] += dot8(q[u], c + 8 * (k + u * 32));
+    for (int u = 0; u < 4; u++) s[u] += dot8(q[u], c + 8 * (k + u * kMvThreads));
   }
-  for (; k < nv8; k += 32) s[0] += dot8(ldg_hint(ir + k, keep), c + 8 * k);
-  if (lane < tail) s[1] += __half2float(inv[(size_t)row * ld + 8 * nv8 + lane]) * c[8 * nv8 + lane];
-  const float t = warp_sum((s[0] + s[1]) + (s[2] + s[3]));
-  if (lane == 0) e[row] = (VT)(t * rscale);
+  for (; k < nv8; k += kMvThreads) s[0] += dot8(ldg_hint(ir + k, keep), c + 8 * k);
+  if (threadIdx.x < tail) s[1] += __half2float(inv[(size_t)row * ld + 8 * nv8 + threadIdx.x]) * c[8 * nv8 + threadIdx.x];
+  float t = warp_sum((s[0] + s[1]) + (s[2] + s[3]));
+  __shared__ float sw[kMvThreads / 32];
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float tot = 0.f;
+#pragma unroll
+    for (int w = 0; w < kMvThreads / 32; w++) tot += sw[w];
+    e[row] = (VT)(tot * rscale);
+  }
 }
 
 template <class VT>
@@ -140,17 +170,22 @@ int grid_of(long long n, int threads) {
 
 template <class VT>
 cudaError_t launch_coarse_restrict(const CoarseArgs<VT>& a, const VT* r, float* c, const int* done, cudaStream_t s) {
-  const int warps = kRestrictThreads / 32;
-  return launch_k(a.pdl != 0, k_restrict<VT>, dim3((a.nc + warps - 1) / warps), dim3(kRestrictThreads), 0, s, a, r,
-                  c, done);
+  // shared memory: G groups x fd[0] partials (G = 1 once fd[0] exceeds the block)
+  if (a.fd[0] > 4096) return cudaErrorInvalidValue;
+  for (int ax = 1; ax < 3; ax++) {  // support lines of a coarse pair: at most (2 h + 1)^2
+    const double h = a.cd[ax] > 1 ? (double)(a.fd[ax] - 1) / (a.cd[ax] - 1) : 1.0;
+    if (h > 15.0) return cudaErrorInvalidValue;
+  }
+  const int G = a.fd[0] <= kRestrictThreads ? kRestrictThreads / a.fd[0] : 1;
+  const size_t sm = (size_t)G * a.fd[0] * sizeof(double);
+  return launch_k(a.pdl != 0, k_restrict<VT>, dim3(a.cd[1] * a.cd[2]), dim3(kRestrictThreads), sm, s, a, r, c, done);
 }
 
 template <class VT>
 cudaError_t launch_coarse_solve(const CoarseArgs<VT>& a, const float* c, VT* e, const int* done, cudaStream_t s) {
   if (a.ldinv % 8 || a.ldinv < a.nc) return cudaErrorInvalidValue;
-  const int warps = kMvThreads / 32;
-  return launch_k(a.pdl != 0, k_coarse_mv<VT>, dim3((a.nc + warps - 1) / warps), dim3(kMvThreads), 0, s, a.nc,
-                  a.ldinv, a.inv16, (float)(1.0 / a.inv_scale), c, e, done);
+  return launch_k(a.pdl != 0, k_coarse_mv<VT>, dim3(a.nc), dim3(kMvThreads), 0, s, a.nc, a.ldinv, a.inv16,
+                  (float)(1.0 / a.inv_scale), c, e, done);
 }
 
 template <class VT>
