@@ -296,6 +296,31 @@ cudaError_t upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
   return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
+// SELL-32 copy of a CSR pattern already on the device: slice widths on the
+// device, their prefix sum on the host (nrows / 32 entries), the padded
+// columns on the device.  entries = stored entries (slices x 32 x width).
+int sell_pattern(cfd_ctx* c, int nrows, const int* rp, const int* col, DevBuf<int>& off, DevBuf<int>& scol,
+                 size_t& entries) {
+  const int ns = (nrows + 31) / 32;
+  DevBuf<int> width;
+  CU(width.alloc(ns));
+  CU(launch_sell_widths(nrows, rp, width.p, c->stream));
+  std::vector<int> w(ns), h(ns + 1, 0);
+  CU(cudaMemcpyAsync(w.data(), width.p, ns * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CU(cudaStreamSynchronize(c->stream));
+  long long total = 0;
+  for (int i = 0; i < ns; i++) {
+    total += 32LL * w[i];
+    if (total >= (1LL << 31)) return fail(c, CFD_E_BADINPUT, "an operator exceeds 2^31 stored entries");
+    h[i + 1] = (int)total;
+  }
+  CU(upload(off, h, c->stream));
+  CU(scol.alloc((size_t)total));
+  CU(launch_sell_cols(nrows, rp, col, off.p, scol.p, c->stream));
+  entries = (size_t)total;
+  return CFD_OK;
+}
+
 int set_device(cfd_ctx* c) {
   CU(cudaSetDevice(c->device));
   return CFD_OK;
@@ -391,14 +416,15 @@ int upload_problem(cfd_ctx* c) {
   CU(upload(c->gt_pos, P.gt_pos, s));
   CU(upload(c->z_rp, P.z_rp, s));
   CU(upload(c->z_col, P.z_col, s));
-  CU(upload(c->ks_off, P.k_soff, s));
-  CU(upload(c->ks_col, P.k_scol, s));
-  CU(upload(c->gs_off, P.g_soff, s));
-  CU(upload(c->gs_col, P.g_scol, s));
-  CU(upload(c->gts_off, P.gt_soff, s));
-  CU(upload(c->gts_col, P.gt_scol, s));
-  CU(upload(c->zs_off, P.z_soff, s));
-  CU(upload(c->zs_col, P.z_scol, s));
+  // SELL-32 copies of the patterns, built on the device
+  size_t sK = 0, sG = 0, sGt = 0, sZ = 0;
+  {
+    int rc = sell_pattern(c, (int)P.NN, c->k_rp.p, c->k_col.p, c->ks_off, c->ks_col, sK);
+    if (!rc) rc = sell_pattern(c, (int)P.NN, c->g_rp.p, c->g_col.p, c->gs_off, c->gs_col, sG);
+    if (!rc) rc = sell_pattern(c, (int)P.NNp, c->gt_rp.p, c->gt_col.p, c->gts_off, c->gts_col, sGt);
+    if (!rc) rc = sell_pattern(c, (int)P.NNp, c->z_rp.p, c->z_col.p, c->zs_off, c->zs_col, sZ);
+    if (rc) return rc;
+  }
   std::vector<unsigned char> mask(P.NN, 0);
   std::vector<double> bcv(3 * P.bcnode.size());
   for (size_t i = 0; i < P.bcnode.size(); i++) {
@@ -415,7 +441,6 @@ int upload_problem(cfd_ctx* c) {
   CU(c->zval.alloc(nnzZ));
   for (auto* b : {&c->zdiag, &c->zdinv}) CU(b->alloc(NNp));
   for (auto* b : {&c->msum, &c->minv_orig, &c->minv_free}) CU(b->alloc(NN));
-  const size_t sK = P.k_scol.size(), sG = P.g_scol.size(), sGt = P.gt_scol.size(), sZ = P.z_scol.size();
   CU(c->ks_val.alloc(sK));
   for (auto* b : {&c->gs1, &c->gs2, &c->gs3}) CU(b->alloc(sG));
   for (auto* b : {&c->gts1, &c->gts2, &c->gts3}) CU(b->alloc(sGt));
@@ -461,7 +486,7 @@ int upload_problem(cfd_ctx* c) {
   for (int pass = 0; pass < 2; pass++) {
     const int grid = pass == 0 ? c->pcg_grid64 : c->pcg_grid32;
     std::vector<int> nb(2 * (size_t)grid);
-    pcg_neighbor_ranges((int)NNp, grid, P.z_soff.data(), P.z_scol.data(), nb.data(), nb.data() + grid);
+    pcg_neighbor_ranges((int)NNp, grid, P.z_rp.data(), P.z_col.data(), nb.data(), nb.data() + grid);
     CU(upload(pass == 0 ? c->nb64 : c->nb32, nb, s));
   }
   CU(c->cg_res.alloc(8));

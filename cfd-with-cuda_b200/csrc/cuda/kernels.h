@@ -354,7 +354,11 @@ cudaError_t spd_inverse_device(double* A, double* work, int n, int ld, int* info
 cudaError_t spd_inverse_to_half(const double* inv, int n, int ld, unsigned long long* amax_bits, int ldh, __half* out,
                                 cudaStream_t s);
 
-void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi);
+// Per block of k_pcg (grid blocks over the SELL-32 slices of n rows): the
+// first and last block owning a column its slices read, from the CSR
+// pattern (rp, col; rows sorted ascending) with the SELL padding's column 0
+// for empty rows.
+void pcg_neighbor_ranges(int n, int grid, const int* rp, const int* col, int* lo, int* hi);
 template <class VT>
 cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s);
 template <class VT>
@@ -372,6 +376,12 @@ cudaError_t launch_sum_partials(const double* part, int n, double* out, cudaStre
 // CSR values -> SELL-32 values (padding entries set to 0).
 template <class T>
 cudaError_t launch_csr_to_sell(int nrows, const int* rp, const double* csr, const int* off, T* sell, cudaStream_t s);
+// SELL-32 pattern on the device: width[s] = longest row of slice s; then,
+// with off = 32 x the exclusive prefix sum of the widths (nslices + 1
+// entries), the columns slice-column-major (short rows padded with their
+// last column, empty rows with 0).
+cudaError_t launch_sell_widths(int nrows, const int* rp, int* width, cudaStream_t s);
+cudaError_t launch_sell_cols(int nrows, const int* rp, const int* col, const int* off, int* scol, cudaStream_t s);
 
 cudaError_t launch_wait_selftest(const int* flag, int* err, unsigned long long timeout_ns, cudaStream_t s);
 

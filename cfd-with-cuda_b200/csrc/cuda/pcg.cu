@@ -400,7 +400,7 @@ int pcg_max_grid(int n, int device) {
   return (int)std::min(cap, want);
 }
 
-void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int* lo, int* hi) {
+void pcg_neighbor_ranges(int n, int grid, const int* rp, const int* col, int* lo, int* hi) {
   const int ns = (n + 31) / 32;
   const long long W = (long long)grid * kPcgWarps;
   std::vector<int> owner(ns);
@@ -411,11 +411,26 @@ void pcg_neighbor_ranges(int n, int grid, const int* soff, const int* scol, int*
   for (int b = 0; b < grid; b++) {
     const int s0 = (int)(ns * (kPcgWarps * (long long)b) / W), s1 = (int)(ns * (kPcgWarps * (long long)(b + 1)) / W);
     int cmin = n, cmax = -1;
-    for (int s = s0; s < s1; s++)
-      for (int e = soff[s]; e < soff[s + 1]; e++) {
-        cmin = std::min(cmin, scol[e]);
-        cmax = std::max(cmax, scol[e]);
+    for (int s = s0; s < s1; s++) {
+      // the slice's stored columns: every row's own, and column 0 as the
+      // padding of its empty rows (rows past n included) when any row of
+      // the slice is non-empty
+      int w = 0;
+      bool empty_row = false;
+      for (int r = 32 * s; r < 32 * s + 32; r++) {
+        const int len = r < n ? rp[r + 1] - rp[r] : 0;
+        w = std::max(w, len);
+        empty_row = empty_row || len == 0;
+        if (len > 0) {  // rows are sorted ascending
+          cmin = std::min(cmin, col[rp[r]]);
+          cmax = std::max(cmax, col[rp[r + 1] - 1]);
+        }
       }
+      if (w > 0 && empty_row) {
+        cmin = std::min(cmin, 0);
+        cmax = std::max(cmax, 0);
+      }
+    }
     if (cmax < 0) {
       lo[b] = b;
       hi[b] = b - 1;  // no neighbours

@@ -248,6 +248,30 @@ __global__ void k_csr_to_sell(int nrows, const int* __restrict__ rp, const doubl
   for (int j = 0; j < w; j++) sell[b + 32 * j] = j < len ? (T)csr[cb + j] : (T)0;
 }
 
+// SELL-32 pattern of a CSR pattern: slice widths (longest row of each
+// 32-row slice), then the columns slice-column-major, a row shorter than its
+// slice padded with its last column (0 for an empty row or a row past the
+// end).
+__global__ void k_sell_widths(int nrows, const int* __restrict__ rp, int* __restrict__ width) {
+  const int ns = (nrows + 31) >> 5;
+  for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < ns; sl += gridDim.x * blockDim.x) {
+    int w = 0;
+    for (int r = 32 * sl; r < min(nrows, 32 * sl + 32); r++) w = max(w, rp[r + 1] - rp[r]);
+    width[sl] = w;
+  }
+}
+__global__ void k_sell_cols(int nrows, const int* __restrict__ rp, const int* __restrict__ col,
+                            const int* __restrict__ off, int* __restrict__ scol) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nslices = (nrows + 31) >> 5;
+  if (row >= nslices * 32) return;
+  const int sl = row >> 5, l = row & 31;
+  const int b = off[sl] + l, w = (off[sl + 1] - off[sl]) >> 5;
+  const int cb = row < nrows ? rp[row] : 0, len = row < nrows ? rp[row + 1] - cb : 0;
+  const int padc = len > 0 ? col[cb + len - 1] : 0;
+  for (int j = 0; j < w; j++) scol[b + 32 * j] = j < len ? col[cb + j] : padc;
+}
+
 __global__ void k_blocks_to_vec4(int NN, const double* __restrict__ b, double4* v) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < NN; i += gridDim.x * blockDim.x)
     v[i] = make_double4(b[i], b[(size_t)NN + i], b[2 * (size_t)NN + i], 0.0);
@@ -304,6 +328,16 @@ cudaError_t launch_pressure_update(int NNp, double dt, const double* pn, const d
 cudaError_t launch_reduce_norms(const double* upart, int nub, const double* ppart, int npb, double* out,
                                 cudaStream_t s) {
   k_reduce_norms<<<1, 1024, 0, s>>>(upart, nub, ppart, npb, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_sell_widths(int nrows, const int* rp, int* width, cudaStream_t s) {
+  const int ns = (nrows + 31) / 32;
+  k_sell_widths<<<rows_grid(ns) < 4096 ? rows_grid(ns) : 4096, kRowThreads, 0, s>>>(nrows, rp, width);
+  return cudaGetLastError();
+}
+cudaError_t launch_sell_cols(int nrows, const int* rp, const int* col, const int* off, int* scol, cudaStream_t s) {
+  const int nslices = (nrows + 31) / 32;
+  k_sell_cols<<<rows_grid((long long)nslices * 32), kRowThreads, 0, s>>>(nrows, rp, col, off, scol);
   return cudaGetLastError();
 }
 template <class T>

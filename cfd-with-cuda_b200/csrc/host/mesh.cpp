@@ -358,32 +358,6 @@ void build_pattern(int nrows, const std::vector<int>& inc_rp, const std::vector<
 
 }  // namespace
 
-bool build_sell(int nrows, const std::vector<int>& rp, const std::vector<int>& col, std::vector<int>& off,
-                std::vector<int>& scol) {
-  const int ns = (nrows + 31) / 32;
-  off.assign(ns + 1, 0);
-  long long total = 0;
-  for (int s = 0; s < ns; s++) {
-    int w = 0;
-    for (int r = 32 * s; r < std::min(nrows, 32 * s + 32); r++) w = std::max(w, rp[r + 1] - rp[r]);
-    total += 32LL * w;
-    if (total >= (1LL << 31)) return false;
-    off[s + 1] = (int)total;
-  }
-  scol.assign((size_t)total, 0);
-#pragma omp parallel for schedule(static)
-  for (int s = 0; s < ns; s++) {
-    const int w = (off[s + 1] - off[s]) / 32;
-    for (int l = 0; l < 32; l++) {
-      const int r = 32 * s + l;
-      const int len = r < nrows ? rp[r + 1] - rp[r] : 0;
-      const int padc = len > 0 ? col[rp[r] + len - 1] : 0;
-      for (int j = 0; j < w; j++) scol[(size_t)off[s] + 32 * j + l] = j < len ? col[rp[r] + j] : padc;
-    }
-  }
-  return true;
-}
-
 int preprocess(HostProblem& P, std::string& err) {
   const int NE = P.NE, NCN = P.NCN;
   // ---- mid-edge nodes (first appearance in element-then-edge order) ----
@@ -557,12 +531,6 @@ int preprocess(HostProblem& P, std::string& err) {
   }
   if ((long long)P.k_rp[P.NN] >= (1LL << 31) - 1) {
     err = "K has more than 2^31 non-zeros";
-    return CFD_E_BADINPUT;
-  }
-  if (!build_sell(P.NN, P.k_rp, P.k_col, P.k_soff, P.k_scol) || !build_sell(P.NN, P.g_rp, P.g_col, P.g_soff, P.g_scol) ||
-      !build_sell(P.NNp, P.gt_rp, P.gt_col, P.gt_soff, P.gt_scol) ||
-      !build_sell(P.NNp, P.z_rp, P.z_col, P.z_soff, P.z_scol)) {
-    err = "an operator exceeds 2^31 stored entries";
     return CFD_E_BADINPUT;
   }
   return CFD_OK;

@@ -36,16 +36,7 @@ struct HostProblem {
   std::vector<int> gt_rp, gt_col, gt_pos; // NNp x NN; gt_pos = index of (v,p) in G
   std::vector<int> z_rp, z_col;           // NNp x NNp
   int maxZrow = 0, maxKrow = 0, maxGrow = 0, maxGtrow = 0;
-
-  // SELL-32 copies of the same patterns: slice offsets (nslices+1, in
-  // entries) and columns in slice-column-major order, padded with a valid
-  // column of the row (or 0) where the row is shorter than its slice.
-  std::vector<int> k_soff, k_scol, g_soff, g_scol, gt_soff, gt_scol, z_soff, z_scol;
 };
-
-// SELL-32 layout of a CSR pattern; returns false if it exceeds 2^31 entries.
-bool build_sell(int nrows, const std::vector<int>& rp, const std::vector<int>& col, std::vector<int>& off,
-                std::vector<int>& scol);
 
 // readInputFile semantics (blascoCodinaHuerta.cpp:528-725).  Returns 0 or a
 // negative cfd_status; err receives a message.
