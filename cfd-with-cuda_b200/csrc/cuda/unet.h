@@ -79,6 +79,10 @@ cudaError_t f32_to_bf16(long long n, const float* a, __nv_bfloat16* b, cudaStrea
 // ---- tensor-core path (unet_tc.cu): stride-1 and stride-2 convolutions,
 // cin in {16, 32, 64}, cout in {16, 32, 64} ----
 struct ConvTcParams {
+  // TMA descriptor of the input (channels-last BF16, dims cin, x, y, z):
+  // box of 8 channels x the halo brick, traversal stride 1 (stride-1
+  // layers) or 2 along x, y, z (one parity phase of a stride-2 layer)
+  CUtensorMap tmap;
   int dims[3];      // output grid
   int in_dims[3];   // input grid (stride 2: 2 dims - 1 per axis)
   const __nv_bfloat16* in;  // input tensor, channels-last, cin channels

@@ -2,10 +2,11 @@
 // inference path.
 //
 // Implicit GEMM without an im2col buffer.  A CTA owns a brick of output
-// voxels; its threads gather the brick plus a one-voxel halo into shared
-// memory with 16-byte cp.async copies (zero-filled outside the grid), one
-// plane per 8 input channels, each halo voxel one 16-byte row of the plane
-// (rows numbered hx + HX (hy + HY hz) over the halo box).  In that numbering
+// voxels; one thread brings the brick plus a one-voxel halo into shared
+// memory with TMA tensor copies (zero-filled outside the grid), one plane
+// per 8 input channels, each halo voxel one 16-byte row of the plane (rows
+// numbered hx + HX (hy + HY hz) over the halo box, the order in which the
+// tensor copy lays out its box).  In that numbering
 // every tap (dx, dy, dz) is a constant row shift, so the A operand of tap k
 // for 128 consecutive rows is the plane itself at a shifted start address:
 // no data is copied per tap.  Rows that fall on the halo ring compute
@@ -14,8 +15,9 @@
 // tensor core's canonical K-major layout and brought in by one bulk copy.
 //
 // Stride 2 (the U-Net's down-sampling layers) runs on the same machinery:
-// the gather splits the fine input into its 8 parity phases (voxel (2i+px,
-// 2j+py, 2k+pz) -> phase px + 2py + 4pz at (i, j, k)), and tap d of output X
+// the copies split the fine input into its 8 parity phases (voxel (2i+px,
+// 2j+py, 2k+pz) -> phase px + 2py + 4pz at (i, j, k); a traversal stride of
+// 2 along x, y and z), and tap d of output X
 // reads phase (d != 0) at coarse index X + (d == -1 ? -1 : 0), again a
 // constant row shift inside that phase's planes (low-side halo only).
 //
@@ -102,55 +104,40 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// 16-byte asynchronous copy global -> shared; src_bytes = 0 writes zeros.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, unsigned src_bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
-               : "memory");
+// One TMA tensor copy of a 4-D box (coordinates innermost first) into shared
+// memory, completing on the mbarrier (no multicast).
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
 }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Warp-cooperative gather of the halo brick: one x-run (HX voxels x NCH
-// 16-byte chunks) per warp step, runs (phase, hz, hy) dealt round-robin over
-// the warps, lane constants precomputed, zero fill outside the grid.
+// The halo brick by TMA: one copy per (phase, 8-channel chunk), each a box
+// of HX x HY x HZ voxels starting one voxel below the brick (stride 1), or
+// at phase (px, py, pz) of the voxel pairs below it (stride 2: coordinate
+// 2 (x0 - 1) + px with traversal stride 2).  Called by one thread after the
+// expect_tx of their bytes on bar.
 template <int NCH, int STRIDE>
-__device__ __forceinline__ void gather_halo(const ConvTcParams& p, unsigned char* A, int x0, int y0, int z0) {
+__device__ __forceinline__ void load_halo(const ConvTcParams& p, unsigned char* A, int x0, int y0, int z0,
+                                          unsigned long long* bar) {
   constexpr int NPH = STRIDE == 2 ? 8 : 1;
-  const int HX = p.halo[0], HY = p.halo[1], HZ = p.halo[2];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int fx = p.in_dims[0], fy = p.in_dims[1], fz = p.in_dims[2];
-  const int items = HX * NCH;  // per x-run
-  const int runs = NPH * HZ * HY;
-  for (int r = warp; r < runs; r += kTcThreads / 32) {
-    const int hy = r % HY, t = r / HY, hz = t % HZ, ph = t / HZ;
-    int gy = y0 - 1 + hy, gz = z0 - 1 + hz;
-    bool yz_ok = gy >= 0 && gz >= 0;
-    if (STRIDE == 2) {
-      gy = 2 * gy + ((ph >> 1) & 1);
-      gz = 2 * gz + (ph >> 2);
-    }
-    yz_ok = yz_ok && gy < fy && gz < fz;
-    const long long rowbase = (long long)fx * (gy + (long long)fy * gz);
-    const int row0 = HX * (hy + HY * hz);
-    for (int i = lane; i < items; i += 32) {
-      const int c = i % NCH, hx = i / NCH;
-      int gx = x0 - 1 + hx;
-      bool ok = yz_ok && gx >= 0;
-      if (STRIDE == 2) gx = 2 * gx + (ph & 1);
-      ok = ok && gx < fx;
-      const __nv_bfloat16* src = ok ? p.in + ((gx + rowbase) * (NCH * 8) + 8 * c) : p.in;
-      cp_async16(A + (size_t)(ph * NCH + c) * p.plane_bytes + (size_t)(row0 + hx) * 16, src, ok ? 16u : 0u);
-    }
-  }
-  // read slack past the halo box: zeros
-  const int nbox = HX * HY * HZ, slack = p.rows - nbox;
-  for (int i = threadIdx.x; i < NPH * NCH * slack; i += kTcThreads) {
-    const int pl = i / slack, row = nbox + i % slack;
-    *(uint4*)(A + (size_t)pl * p.plane_bytes + (size_t)row * 16) = make_uint4(0, 0, 0, 0);
+#pragma unroll 1
+  for (int ph = 0; ph < NPH; ph++) {
+    const int px = ph & 1, py = (ph >> 1) & 1, pz = ph >> 2;
+    const int cx = STRIDE == 2 ? 2 * (x0 - 1) + px : x0 - 1;
+    const int cy = STRIDE == 2 ? 2 * (y0 - 1) + py : y0 - 1;
+    const int cz = STRIDE == 2 ? 2 * (z0 - 1) + pz : z0 - 1;
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+      tma_load_4d(A + (size_t)(ph * NCH + c) * p.plane_bytes, &p.tmap, 8 * c, cx, cy, cz, bar);
   }
 }
 
 template <int CIN, int STRIDE>
-__global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvTcParams p) {
+__global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ ConvTcParams p) {
   constexpr int NCH = CIN / 8, KSTEPS = CIN / 16, NPH = STRIDE == 2 ? 8 : 1;
   constexpr int NWARP = kTcThreads / 32;
   if (p.skip && *p.skip) return;
@@ -183,11 +170,19 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(ConvTcParams p) {
     sbias[i] = co < p.cout ? p.bias[co] : 0.f;
   }
   if (threadIdx.x == 0) {
-    mbar_expect_tx(&bars[0], wbytes);
+    const unsigned abytes = (unsigned)NPH * NCH * 16u * (unsigned)(HX * HY * p.halo[2]);
+    mbar_expect_tx(&bars[0], wbytes + abytes);
     bulk_g2s(W, p.wpack + (size_t)slice * 27 * CIN * p.N, wbytes, &bars[0]);
+    load_halo<NCH, STRIDE>(p, A, x0, y0, z0, &bars[0]);
   }
-  gather_halo<NCH, STRIDE>(p, A, x0, y0, z0);
-  cp_async_wait_all();
+  {
+    // rows past the halo box that tap shifts of the last tiles can read: zeros
+    const int nbox = HX * HY * p.halo[2], slack = p.rows - nbox;
+    for (int i = threadIdx.x; i < NPH * NCH * slack; i += kTcThreads) {
+      const int pl = i / slack, row = nbox + i % slack;
+      *(uint4*)(A + (size_t)pl * p.plane_bytes + (size_t)row * 16) = make_uint4(0, 0, 0, 0);
+    }
+  }
   fence_proxy_async_smem();
   bool ok = __syncthreads_and(mbar_wait_bounded(&bars[0], 0, kTcWaitNs));
   bool loads_done = ok, mma_done = true;
@@ -346,6 +341,46 @@ __global__ void k_pack_tc(const __nv_bfloat16* __restrict__ w, int cin, int cout
 
 int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// cuTensorMapEncodeTiled from the driver, found through the runtime (no link
+// against libcuda)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+// The input's TMA descriptor: dims (cin, x, y, z) of the channels-last BF16
+// input; box 8 channels x the halo brick, with a traversal stride of 2 along
+// x, y, z for stride 2 (the box then spans 2 x halo voxels per axis and
+// loads halo of them).  Returns false when a limit of the copy is not met.
+bool encode_input_map(ConvTcParams& p) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) return false;
+  if (reinterpret_cast<uintptr_t>(p.in) % 16 != 0 || p.cin % 8 != 0) return false;
+  const int s = p.stride;
+  cuuint64_t gdim[4] = {(cuuint64_t)p.cin, (cuuint64_t)p.in_dims[0], (cuuint64_t)p.in_dims[1],
+                        (cuuint64_t)p.in_dims[2]};
+  cuuint64_t gstride[3] = {(cuuint64_t)p.cin * 2, (cuuint64_t)p.cin * 2 * p.in_dims[0],
+                           (cuuint64_t)p.cin * 2 * p.in_dims[0] * p.in_dims[1]};
+  cuuint32_t box[4] = {8, (cuuint32_t)(s * p.halo[0]), (cuuint32_t)(s * p.halo[1]), (cuuint32_t)(s * p.halo[2])};
+  cuuint32_t estride[4] = {1, (cuuint32_t)s, (cuuint32_t)s, (cuuint32_t)s};
+  for (int a = 1; a < 4; a++)
+    if (box[a] < 1 || box[a] > 256) return false;
+  const CUresult r = enc(&p.tmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(p.in), gdim,
+                         gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 int conv_tc_slice_width(int cin, int cout, int stride) {
@@ -437,6 +472,7 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
       return -5;
   }
   p.nb[2] = ceil_div(p.dims[2], p.brick[2]);
+  if (!encode_input_map(p)) return -6;
   p.wpack = wpack;
   p.bias = d.bias;
   p.out = d.out;
