@@ -131,82 +131,69 @@ __global__ void __launch_bounds__(k16X * k16Y * k16Z) k_conv_16to1(ConvDesc d) {
   d.out_f32[(size_t)x + (size_t)nx * (y + (size_t)ny * z)] = acc;
 }
 
-// Single-input-channel convolution (the first layer) with 16 outputs: one
-// thread per XB consecutive output voxels along x (each weight row and input
-// value serves XB voxels), weights as float4 rows in shared memory, two
-// 16-byte stores per voxel.  All 9 x (XB + 2) inputs of a thread are loaded
-// before any product, so their latencies overlap.
-__global__ void __launch_bounds__(256, 2) k_conv_c1to16(ConvDesc d) {
-  constexpr int XB = 2;  // consecutive voxels along x per thread: weights and inputs reused
+// Single-input-channel convolution (the first layer) with 16 outputs.  A
+// block computes a 16 x 4 x 4 tile of output voxels, one per thread: the
+// tile's input plus a one-voxel halo (18 x 6 x 6 values, zero outside the
+// grid) is staged in shared memory as FP32, the 27 x 16 weights as float4
+// rows (each read is a broadcast), and a thread keeps its 16 sums in
+// registers.  The taps are summed in order 0..26 per channel, starting from
+// the bias, as a direct loop over them.
+__global__ void __launch_bounds__(k16X * k16Y * k16Z) k_conv_c1to16(ConvDesc d) {
+  constexpr int HX = k16X + 2, HY = k16Y + 2, HZ = k16Z + 2;
+  __shared__ float tile[HX * HY * HZ];
   __shared__ float4 sw[27 * 4];
   __shared__ float sb[16];
   if (d.skip && *d.skip) return;
   for (int i = threadIdx.x; i < 27 * 16; i += blockDim.x) ((float*)sw)[i] = bf(d.w[i]);
   if (threadIdx.x < 16) sb[threadIdx.x] = d.bias[threadIdx.x];
-  __syncthreads();
   const int nx = d.out_dims[0], ny = d.out_dims[1], nz = d.out_dims[2];
-  const int gx = (nx + XB - 1) / XB;
-  const int ng = gx * ny * nz;
-  for (int gidx = blockIdx.x * blockDim.x + threadIdx.x; gidx < ng; gidx += gridDim.x * blockDim.x) {
-    const int xg = gidx % gx, t = gidx / gx, y = t % ny, z = t / ny;
-    const int x0 = xg * XB;
-    // inputs x0-1 .. x0+XB of the 9 (dy, dz) rows, zero outside the grid
-    float in[9][XB + 2];
+  const int tbx = (nx + k16X - 1) / k16X, tby = (ny + k16Y - 1) / k16Y;
+  const int bx = blockIdx.x % tbx, by = (blockIdx.x / tbx) % tby, bz = blockIdx.x / (tbx * tby);
+  const int x0 = bx * k16X, y0 = by * k16Y, z0 = bz * k16Z;
+  for (int i = threadIdx.x; i < HX * HY * HZ; i += blockDim.x) {
+    const int hx = i % HX, hy = (i / HX) % HY, hz = i / (HX * HY);
+    const int gx = x0 - 1 + hx, gy = y0 - 1 + hy, gz = z0 - 1 + hz;
+    float u = 0.f;
+    if (gx >= 0 && gy >= 0 && gz >= 0 && gx < nx && gy < ny && gz < nz)
+      u = bf(d.inA[(size_t)gx + (size_t)nx * (gy + (size_t)ny * gz)]);
+    tile[i] = u;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x % k16X, ty = (threadIdx.x / k16X) % k16Y, tz = threadIdx.x / (k16X * k16Y);
+  const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
+  if (x >= nx || y >= ny || z >= nz) return;
+  float acc[16];
 #pragma unroll
-    for (int dzy = 0; dzy < 9; dzy++) {
-      const int iy = y + dzy % 3 - 1, iz = z + dzy / 3 - 1;
-      const bool row_ok = iy >= 0 && iz >= 0 && iy < ny && iz < nz;
-      const __nv_bfloat16* row = d.inA + (size_t)nx * ((row_ok ? iy : 0) + (size_t)ny * (row_ok ? iz : 0));
+  for (int c = 0; c < 16; c++) acc[c] = sb[c];
+#pragma unroll 3
+  for (int k = 0; k < 27; k++) {
+    const float a = tile[(tx + k % 3) + HX * ((ty + (k / 3) % 3) + HY * (tz + k / 9))];
 #pragma unroll
-      for (int k = 0; k < XB + 2; k++) {
-        const int ix = x0 - 1 + k;
-        in[dzy][k] = (row_ok && ix >= 0 && ix < nx) ? bf(row[ix]) : 0.f;
-      }
-    }
-    float acc[XB][16];
-#pragma unroll
-    for (int u = 0; u < XB; u++)
-#pragma unroll
-      for (int c = 0; c < 16; c++) acc[u][c] = sb[c];
-#pragma unroll
-    for (int dzy = 0; dzy < 9; dzy++) {
-#pragma unroll
-      for (int dx = 0; dx < 3; dx++) {
-        const int tap = dx + 3 * dzy;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const float4 w = sw[4 * tap + q];
-#pragma unroll
-          for (int u = 0; u < XB; u++) {
-            const float a = in[dzy][u + dx];
-            acc[u][4 * q] += a * w.x;
-            acc[u][4 * q + 1] += a * w.y;
-            acc[u][4 * q + 2] += a * w.z;
-            acc[u][4 * q + 3] += a * w.w;
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < XB; u++) {
-      if (x0 + u >= nx) break;
-      __align__(16) __nv_bfloat16 o[16];
-#pragma unroll
-      for (int c = 0; c < 16; c++) {
-        float yv = acc[u][c];
-        if (d.act && yv < 0.f) yv *= kLeaky;
-        o[c] = __float2bfloat16(yv);
-      }
-      const size_t v = (size_t)(x0 + u) + (size_t)nx * (y + (size_t)ny * z);
-      uint4* dst = (uint4*)(d.out + v * 16);
-      dst[0] = ((const uint4*)o)[0];
-      dst[1] = ((const uint4*)o)[1];
+    for (int q = 0; q < 4; q++) {
+      const float4 w = sw[4 * k + q];
+      acc[4 * q] += a * w.x;
+      acc[4 * q + 1] += a * w.y;
+      acc[4 * q + 2] += a * w.z;
+      acc[4 * q + 3] += a * w.w;
     }
   }
+  __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+  for (int c = 0; c < 16; c++) {
+    float yv = acc[c];
+    if (d.act && yv < 0.f) yv *= kLeaky;
+    o[c] = __float2bfloat16(yv);
+  }
+  const size_t v = (size_t)x + (size_t)nx * (y + (size_t)ny * z);
+  uint4* dst = (uint4*)(d.out + v * 16);
+  dst[0] = ((const uint4*)o)[0];
+  dst[1] = ((const uint4*)o)[1];
 }
 
 // Prolongation plus skip for CH channels: one thread per fine voxel, 16-byte
-// vector loads and stores, 32-bit index arithmetic.
+// vector loads and stores, 32-bit index arithmetic.  The corners are summed
+// in the order (z, y, x) of the coarse cell, as the trilinear weights of the
+// fine index pick them.
 template <int CH>
 __global__ void __launch_bounds__(256) k_up_fwd_v(Dims3 g, const __nv_bfloat16* __restrict__ in,
                                                   const __nv_bfloat16* __restrict__ skip, __nv_bfloat16* out,
@@ -219,21 +206,31 @@ __global__ void __launch_bounds__(256) k_up_fwd_v(Dims3 g, const __nv_bfloat16* 
     float acc[CH];
 #pragma unroll
     for (int c = 0; c < CH; c++) acc[c] = 0.f;
-    const int nxs = (X & 1) ? 2 : 1, nys = (Y & 1) ? 2 : 1, nzs = (Z & 1) ? 2 : 1;
     const float w = ((X & 1) ? 0.5f : 1.f) * ((Y & 1) ? 0.5f : 1.f) * ((Z & 1) ? 0.5f : 1.f);
-    for (int zz = 0; zz < nzs; zz++)
-      for (int yy = 0; yy < nys; yy++)
-        for (int xx = 0; xx < nxs; xx++) {
-          const int c0 = ((X >> 1) + xx) + cx * (((Y >> 1) + yy) + cy * ((Z >> 1) + zz));
-          const uint4* src = (const uint4*)(in + (size_t)c0 * CH);
+    // the (up to) 8 coarse corners, all loads issued before any sum; a
+    // corner an even fine index does not use is read at a clamped index and
+    // adds zero
+    uint4 u[8][CH / 8];
 #pragma unroll
-          for (int q = 0; q < CH / 8; q++) {
-            uint4 u = src[q];
-            const __nv_bfloat16* h = (const __nv_bfloat16*)&u;
+    for (int cnr = 0; cnr < 8; cnr++) {
+      const int xx = cnr & 1, yy = (cnr >> 1) & 1, zz = cnr >> 2;
+      const int ix = min((X >> 1) + xx, cx - 1), iy = min((Y >> 1) + yy, cy - 1);
+      const int iz = min((Z >> 1) + zz, g.c[2] - 1);
+      const uint4* src = (const uint4*)(in + (size_t)(ix + cx * (iy + cy * iz)) * CH);
 #pragma unroll
-            for (int i = 0; i < 8; i++) acc[8 * q + i] += bf(h[i]);
-          }
-        }
+      for (int q = 0; q < CH / 8; q++) u[cnr][q] = src[q];
+    }
+#pragma unroll
+    for (int cnr = 0; cnr < 8; cnr++) {
+      const int xx = cnr & 1, yy = (cnr >> 1) & 1, zz = cnr >> 2;
+      const bool used = (!xx || (X & 1)) && (!yy || (Y & 1)) && (!zz || (Z & 1));
+#pragma unroll
+      for (int q = 0; q < CH / 8; q++) {
+        const __nv_bfloat16* h = (const __nv_bfloat16*)&u[cnr][q];
+#pragma unroll
+        for (int i = 0; i < 8; i++) acc[8 * q + i] += used ? bf(h[i]) : 0.f;
+      }
+    }
     const uint4* sk = (const uint4*)(skip + (size_t)v * CH);
     uint4* dst = (uint4*)(out + (size_t)v * CH);
 #pragma unroll
@@ -526,8 +523,9 @@ cudaError_t conv3_forward(const ConvDesc& d, cudaStream_t s) {
   const long long nv = (long long)d.out_dims[0] * d.out_dims[1] * d.out_dims[2];
   const int gx = grid1(nv, 128);
   if (cin == 1 && d.cout == 16 && d.stride == 1 && d.out && !d.out_f32 && nv < (1LL << 31)) {
-    const long long ng = (long long)((d.out_dims[0] + 1) / 2) * d.out_dims[1] * d.out_dims[2];
-    k_conv_c1to16<<<grid1(ng, 256), 256, 0, s>>>(d);
+    const long long tiles = (long long)((d.out_dims[0] + k16X - 1) / k16X) * ((d.out_dims[1] + k16Y - 1) / k16Y) *
+                            ((d.out_dims[2] + k16Z - 1) / k16Z);
+    k_conv_c1to16<<<(unsigned)tiles, k16X * k16Y * k16Z, 0, s>>>(d);
     return cudaGetLastError();
   }
   if (d.ca == 16 && d.cb == 0 && d.cout == 1 && d.stride == 1 && d.out_f32 && !d.out && nv < (1LL << 31)) {

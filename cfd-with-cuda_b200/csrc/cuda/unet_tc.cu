@@ -396,10 +396,13 @@ bool conv_tc_supported(const ConvDesc& d) {
   bool dims_ok = true;
   for (int a = 0; a < 3; a++)
     dims_ok = dims_ok && (d.stride == 1 ? d.in_dims[a] == d.out_dims[a] : d.in_dims[a] == 2 * d.out_dims[a] - 1);
-  // (the single-output last layer runs on CUDA cores: a 16-column MMA would
-  // compute 15 unused channels)
+  // The single-output last layer (FP32 output, no activation) runs as a
+  // 16-column MMA whose first column is stored: the 15 unused columns cost
+  // little next to the shared-memory reads of the A operand, which the
+  // CUDA-core form of that layer is bound by.
+  const bool last = d.cout == 1 && d.out_f32 && !d.out && !d.act;
   return (d.stride == 1 || d.stride == 2) && dims_ok && d.cb == 0 && (d.ca == 16 || d.ca == 32 || d.ca == 64) &&
-         (d.cout == 16 || d.cout == 32 || d.cout == 64);
+         (d.cout == 16 || d.cout == 32 || d.cout == 64 || last);
 }
 
 cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
