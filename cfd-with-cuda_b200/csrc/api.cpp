@@ -223,6 +223,7 @@ struct cfd_ctx {
   // the two-level preconditioners
   bool grid_set = false;
   std::vector<int> h_pmap;  // voxel -> pressure node (empty: identity)
+  std::vector<int> h_zfirst, h_zlast;  // first / last column of each row of Z
   bool coarse_ready = false;
   int coarse_gen = 0;  // bumped on every rebuild (captured graphs key on it)
   int cs_fd[3] = {0, 0, 0}, cs_cd[3] = {0, 0, 0}, cs_nc = 0;
@@ -321,6 +322,155 @@ int sell_pattern(cfd_ctx* c, int nrows, const int* rp, const int* col, DevBuf<in
   return CFD_OK;
 }
 
+// Exclusive prefix sum of n counts into n + 1 row pointers (host);
+// false when the total reaches 2^31.
+bool row_pointers(const std::vector<int>& len, std::vector<int>& rp, int& maxlen) {
+  rp.assign(len.size() + 1, 0);
+  long long t = 0;
+  maxlen = 0;
+  for (size_t i = 0; i < len.size(); i++) {
+    t += len[i];
+    if (t >= (1LL << 31) - 1) return false;
+    rp[i + 1] = (int)t;
+    maxlen = std::max(maxlen, len[i]);
+  }
+  return true;
+}
+
+// The CSR patterns of K, G, G^T (with gt_pos) and Z built on the device from
+// the uploaded element map (patterns.cu), with the row pointers kept on the
+// host too (P.k_rp ...; the columns stay on the device until
+// ensure_host_columns).  built = false, with nothing changed, when a row has
+// more candidates than the device build holds: the caller builds them on the
+// host.
+int device_patterns(cfd_ctx* c, bool& built) {
+  built = false;
+  HostProblem& P = c->P;
+  cudaStream_t s = c->stream;
+  const int NN = P.NN, NNp = P.NNp, NE = P.NE;
+  const long long nent = 27LL * NE;
+  DevBuf<int> cnt, inc_rp, inc_el, pos, len, flag, adj_rp, adj_col;
+  CU(cnt.alloc(NN));
+  CU(cudaMemsetAsync(cnt.p, 0, (size_t)NN * sizeof(int), s));
+  CU(launch_incidence_count(nent, c->ltog.p, cnt.p, s));
+  std::vector<int> h(NN), hrp;
+  CU(cudaMemcpyAsync(h.data(), cnt.p, (size_t)NN * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  int maxdeg = 0;
+  if (!row_pointers(h, hrp, maxdeg)) return fail(c, CFD_E_BADINPUT, "element map too large");
+  CU(upload(inc_rp, hrp, s));
+  CU(upload(pos, hrp, s));
+  CU(inc_el.alloc((size_t)nent));
+  CU(launch_incidence_fill(nent, c->ltog.p, pos.p, inc_el.p, s));
+  CU(flag.alloc(1));
+  CU(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+  CU(len.alloc(std::max(NN, NE)));
+  PatArgs a{};
+  a.ltog = c->ltog.p;
+  a.inc_rp = inc_rp.p;
+  a.inc_el = inc_el.p;
+  a.len = len.p;
+  a.overflow = flag.p;
+  // one pattern: pass 0 (lengths), host row pointers, pass 1 (columns)
+  auto one = [&](int mode, int nrows, DevBuf<int>& drp, DevBuf<int>& dcol, std::vector<int>& rp, int& maxlen,
+                 bool& ok) -> int {
+    ok = false;
+    a.rp = nullptr;
+    a.col = nullptr;
+    CU(launch_pattern_rows(a, mode, nrows, 0, c->num_sms, s));
+    std::vector<int> hl(nrows);
+    int hf = 0;
+    CU(cudaMemcpyAsync(hl.data(), len.p, (size_t)nrows * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&hf, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (hf) return CFD_OK;
+    if (!row_pointers(hl, rp, maxlen)) return fail(c, CFD_E_BADINPUT, "an operator has more than 2^31 non-zeros");
+    CU(upload(drp, rp, s));
+    CU(dcol.alloc((size_t)rp[nrows]));
+    a.rp = drp.p;
+    a.col = dcol.p;
+    CU(launch_pattern_rows(a, mode, nrows, 1, c->num_sms, s));
+    ok = true;
+    return CFD_OK;
+  };
+  bool ok = false;
+  std::vector<int> k_rp, g_rp, z_rp, adj_h;
+  int maxK = 0, maxG = 0, maxZ = 0, maxA = 0;
+  int rc = one(0, NN, c->k_rp, c->k_col, k_rp, maxK, ok);
+  if (rc || !ok) return rc;
+  rc = one(1, NN, c->g_rp, c->g_col, g_rp, maxG, ok);
+  if (rc || !ok) return rc;
+  rc = one(2, NE, adj_rp, adj_col, adj_h, maxA, ok);
+  if (rc || !ok) return rc;
+  a.adj_rp = adj_rp.p;
+  a.adj_col = adj_col.p;
+  rc = one(3, NNp, c->z_rp, c->z_col, z_rp, maxZ, ok);
+  if (rc || !ok) return rc;
+  // G^T is K's first NNp rows (pressure nodes are the corner nodes 0 .. NNp)
+  const long long nnzG = g_rp[NN], nnzGt = k_rp[NNp];
+  if (nnzGt != nnzG) return fail(c, CFD_E_BADINPUT, "inconsistent G and G^T patterns");
+  std::vector<int> gt_rp(k_rp.begin(), k_rp.begin() + NNp + 1);
+  CU(upload(c->gt_rp, gt_rp, s));
+  CU(c->gt_col.alloc((size_t)nnzG));
+  CU(cudaMemcpyAsync(c->gt_col.p, c->k_col.p, (size_t)nnzG * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  CU(c->gt_pos.alloc((size_t)nnzG));
+  CU(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+  CU(launch_gt_pos(NNp, c->gt_rp.p, c->gt_col.p, c->g_rp.p, c->g_col.p, c->gt_pos.p, flag.p, s));
+  // first / last column of Z's rows (the k_pcg neighbour ranges)
+  DevBuf<int> zf, zl;
+  CU(zf.alloc(NNp));
+  CU(zl.alloc(NNp));
+  CU(launch_row_ends(NNp, c->z_rp.p, c->z_col.p, zf.p, zl.p, s));
+  c->h_zfirst.resize(NNp);
+  c->h_zlast.resize(NNp);
+  int hbad = 0;
+  CU(cudaMemcpyAsync(c->h_zfirst.data(), zf.p, (size_t)NNp * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(c->h_zlast.data(), zl.p, (size_t)NNp * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(&hbad, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  if (hbad) return fail(c, CFD_E_BADINPUT, "inconsistent G and G^T patterns");
+  int maxGt = 0;
+  for (int r = 0; r < NNp; r++) maxGt = std::max(maxGt, k_rp[r + 1] - k_rp[r]);
+  P.k_rp.swap(k_rp);
+  P.g_rp.swap(g_rp);
+  P.gt_rp.swap(gt_rp);
+  P.z_rp.swap(z_rp);
+  P.k_col.clear();
+  P.g_col.clear();
+  P.gt_col.clear();
+  P.gt_pos.clear();
+  P.z_col.clear();
+  P.maxKrow = maxK;
+  P.maxGrow = maxG;
+  P.maxGtrow = maxGt;
+  P.maxZrow = maxZ;
+  P.nnzK = P.k_rp[NN];
+  P.nnzG = nnzG;
+  P.nnzZ = P.z_rp[NNp];
+  built = true;
+  return CFD_OK;
+}
+
+// The host copies of the pattern columns, downloaded from the device when the
+// patterns were built there (for cfd_download_matrix and the host build of
+// the coarse space).
+int ensure_host_columns(cfd_ctx* c) {
+  HostProblem& P = c->P;
+  if (!P.k_col.empty() || P.nnzK == 0) return CFD_OK;
+  P.k_col.resize((size_t)P.nnzK);
+  P.g_col.resize((size_t)P.nnzG);
+  P.gt_col.resize((size_t)P.nnzG);
+  P.gt_pos.resize((size_t)P.nnzG);
+  P.z_col.resize((size_t)P.nnzZ);
+  CU(cudaStreamSynchronize(c->stream));
+  CU(cudaMemcpy(P.k_col.data(), c->k_col.p, P.k_col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(P.g_col.data(), c->g_col.p, P.g_col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(P.gt_col.data(), c->gt_col.p, P.gt_col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(P.gt_pos.data(), c->gt_pos.p, P.gt_pos.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(P.z_col.data(), c->z_col.p, P.z_col.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  return CFD_OK;
+}
+
 int set_device(cfd_ctx* c) {
   CU(cudaSetDevice(c->device));
   return CFD_OK;
@@ -407,15 +557,35 @@ int upload_problem(cfd_ctx* c) {
       c->color_off.clear();
     }
   }
-  CU(upload(c->k_rp, P.k_rp, s));
-  CU(upload(c->k_col, P.k_col, s));
-  CU(upload(c->g_rp, P.g_rp, s));
-  CU(upload(c->g_col, P.g_col, s));
-  CU(upload(c->gt_rp, P.gt_rp, s));
-  CU(upload(c->gt_col, P.gt_col, s));
-  CU(upload(c->gt_pos, P.gt_pos, s));
-  CU(upload(c->z_rp, P.z_rp, s));
-  CU(upload(c->z_col, P.z_col, s));
+  // CSR patterns: built on the device unless the host already has them (or
+  // a row exceeds what the device build holds)
+  bool on_device = false;
+  if (P.k_rp.empty()) {
+    int rc = device_patterns(c, on_device);
+    if (rc) return rc;
+    if (!on_device) {
+      rc = build_patterns(P, c->err);
+      if (rc) return rc;
+    }
+  }
+  if (!on_device) {
+    CU(upload(c->k_rp, P.k_rp, s));
+    CU(upload(c->k_col, P.k_col, s));
+    CU(upload(c->g_rp, P.g_rp, s));
+    CU(upload(c->g_col, P.g_col, s));
+    CU(upload(c->gt_rp, P.gt_rp, s));
+    CU(upload(c->gt_col, P.gt_col, s));
+    CU(upload(c->gt_pos, P.gt_pos, s));
+    CU(upload(c->z_rp, P.z_rp, s));
+    CU(upload(c->z_col, P.z_col, s));
+    c->h_zfirst.resize(P.NNp);
+    c->h_zlast.resize(P.NNp);
+    for (int r = 0; r < P.NNp; r++) {
+      const int b = P.z_rp[r], e = P.z_rp[r + 1];
+      c->h_zfirst[r] = b < e ? P.z_col[b] : 0;
+      c->h_zlast[r] = b < e ? P.z_col[e - 1] : -1;
+    }
+  }
   // SELL-32 copies of the patterns, built on the device
   size_t sK = 0, sG = 0, sGt = 0, sZ = 0;
   {
@@ -435,7 +605,7 @@ int upload_problem(cfd_ctx* c) {
   CU(upload(c->bcnodes, P.bcnode, s));
   CU(upload(c->bcvals, bcv, s));
   const size_t NN = P.NN, NNp = P.NNp;
-  const size_t nnzK = P.k_col.size(), nnzG = P.g_col.size(), nnzZ = P.z_col.size();
+  const size_t nnzK = (size_t)P.nnzK, nnzG = (size_t)P.nnzG, nnzZ = (size_t)P.nnzZ;
   for (auto* b : {&c->kval}) CU(b->alloc(nnzK));
   for (auto* b : {&c->g1, &c->g2, &c->g3, &c->gt1, &c->gt2, &c->gt3}) CU(b->alloc(nnzG));
   CU(c->zval.alloc(nnzZ));
@@ -486,7 +656,7 @@ int upload_problem(cfd_ctx* c) {
   for (int pass = 0; pass < 2; pass++) {
     const int grid = pass == 0 ? c->pcg_grid64 : c->pcg_grid32;
     std::vector<int> nb(2 * (size_t)grid);
-    pcg_neighbor_ranges((int)NNp, grid, P.z_rp.data(), P.z_col.data(), nb.data(), nb.data() + grid);
+    pcg_neighbor_ranges((int)NNp, grid, c->h_zfirst.data(), c->h_zlast.data(), nb.data(), nb.data() + grid);
     CU(upload(pass == 0 ? c->nb64 : c->nb32, nb, s));
   }
   CU(c->cg_res.alloc(8));
@@ -775,7 +945,9 @@ int ensure_coarse(cfd_ctx* c) {
     }
   }
   if (!zc_on_device) {
-    std::vector<double> zv(P.z_col.size());
+    int rc = ensure_host_columns(c);
+    if (rc) return rc;
+    std::vector<double> zv((size_t)P.nnzZ);
     CU(cudaStreamSynchronize(c->stream));
     CU(cudaMemcpy(zv.data(), c->zval.p, zv.size() * sizeof(double), cudaMemcpyDeviceToHost));
     std::string err;
@@ -1460,7 +1632,7 @@ int cfd_load_inp(cfd_ctx* c, const char* path) {
   c->P = HostProblem();
   rc = read_inp(path, c->P, c->err);
   if (rc) return rc;
-  rc = preprocess(c->P, c->err);
+  rc = preprocess(c->P, c->err, false);
   if (rc) return rc;
   return upload_problem(c);
 }
@@ -1500,7 +1672,7 @@ int cfd_load_mesh(cfd_ctx* c, const cfd_problem_info* info, const double* coords
          "velocity face out of range");
   }
   for (int d = 0; d < 3; d++) P.mon[d] = monitor[d];
-  rc = preprocess(P, c->err);
+  rc = preprocess(P, c->err, false);
   if (rc) return rc;
   return upload_problem(c);
 }
@@ -1510,7 +1682,7 @@ int cfd_info(const cfd_ctx* c, cfd_problem_info* i) {
   const HostProblem& P = c->P;
   std::memset(i, 0, sizeof(*i));
   i->NE = P.NE; i->NCN = P.NCN; i->NN = P.NN; i->NNp = P.NNp; i->NGP = P.NGP; i->maxIter = P.maxIter;
-  i->nnzK = (long long)P.k_col.size(); i->nnzG = (long long)P.g_col.size(); i->nnzZ = (long long)P.z_col.size();
+  i->nnzK = P.nnzK; i->nnzG = P.nnzG; i->nnzZ = P.nnzZ;
   i->nBCnodes = (int)P.bcnode.size(); i->monPoint = P.monPoint; i->zeroPressureNode = P.zeroP;
   i->dt = P.dt; i->t_ini = P.t_ini; i->t_final = P.t_final; i->tolerance = P.tolerance;
   i->convergence = P.convergence; i->density = P.density; i->viscosity = P.viscosity;
@@ -1546,7 +1718,7 @@ int cfd_step0(cfd_ctx* c) {
     a.e_end = P.NE;
     CU(launch_assemble(a, c->num_sms, s));
   }
-  CU(launch_fill_gt((long long)P.gt_col.size(), c->gt_pos.p, c->g1.p, c->g2.p, c->g3.p, c->gt1.p, c->gt2.p,
+  CU(launch_fill_gt(P.nnzG, c->gt_pos.p, c->g1.p, c->g2.p, c->g3.p, c->gt1.p, c->gt2.p,
                     c->gt3.p, s));
   CU(launch_md_finalize(P.NN, c->msum.p, c->bcmask.p, c->minv_orig.p, c->minv_free.p, s));
   ZArgs z{};
@@ -1917,6 +2089,10 @@ int cfd_download_vector(cfd_ctx* c, int which, double* out) {
 
 int cfd_download_matrix(cfd_ctx* c, int which, long long* nnz, int* rowptr, int* col, double* val) {
   if (!c || !c->loaded) return CFD_E_BADARG;
+  if (col) {
+    int rc = ensure_host_columns(c);
+    if (rc) return rc;
+  }
   const HostProblem& P = c->P;
   const std::vector<int>* rp = nullptr;
   const std::vector<int>* cl = nullptr;
@@ -1928,7 +2104,7 @@ int cfd_download_matrix(cfd_ctx* c, int which, long long* nnz, int* rowptr, int*
     case CFD_M_Z: rp = &P.z_rp; cl = &P.z_col; v[0] = c->zval.p; break;
     default: return fail(c, CFD_E_BADARG, "unknown matrix id %d", which);
   }
-  const size_t n = cl->size();
+  const size_t n = which == CFD_M_K ? (size_t)P.nnzK : which == CFD_M_Z ? (size_t)P.nnzZ : (size_t)P.nnzG;
   if (nnz) *nnz = (long long)n;
   if (rowptr) std::copy(rp->begin(), rp->end(), rowptr);
   if (col) std::copy(cl->begin(), cl->end(), col);

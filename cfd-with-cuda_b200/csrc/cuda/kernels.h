@@ -343,6 +343,30 @@ struct GalerkinArgs {
 };
 cudaError_t launch_galerkin(const GalerkinArgs& g, cudaStream_t s);
 
+// CSR patterns on the device (patterns.cu).  Node -> element incidence:
+// counts, then (after an exclusive prefix sum of the counts into pos) the
+// element of every ltog entry at pos[node]++ (order within a node arbitrary).
+cudaError_t launch_incidence_count(long long nent, const int* ltog, int* cnt, cudaStream_t s);
+cudaError_t launch_incidence_fill(long long nent, const int* ltog, int* pos, int* inc_el, cudaStream_t s);
+struct PatArgs {
+  const int *ltog, *inc_rp, *inc_el;  // element map, node -> element incidence
+  const int *adj_rp, *adj_col;        // element adjacency (mode 3)
+  const int* rp;                      // row pointers of the pattern written in pass 1
+  int* col;                           // its columns (pass 1)
+  int* len;                           // row lengths (pass 0)
+  int* overflow;                      // set when a row has more candidates than a block holds
+};
+// mode 0: K rows (nodes of the elements around a node), 1: G rows (their
+// corners), 2: element adjacency (elements sharing a node with an element),
+// 3: Z rows (corners of the elements adjacent to the elements around a
+// pressure node).  pass 0 writes len, pass 1 the sorted distinct columns.
+cudaError_t launch_pattern_rows(const PatArgs& a, int mode, int nrows, int pass, int num_sms, cudaStream_t s);
+// gt_pos[t] = index in G's columns of the entry (v, p) of G^T entry t = (p, v)
+cudaError_t launch_gt_pos(int nnp, const int* gt_rp, const int* gt_col, const int* g_rp, const int* g_col, int* gt_pos,
+                          int* bad, cudaStream_t s);
+// first / last column of each row (0 / -1 for an empty row)
+cudaError_t launch_row_ends(int n, const int* rp, const int* col, int* first, int* last, cudaStream_t s);
+
 // Dense SPD inverse on the device (dense_chol.cu): A (row-major, leading
 // dimension ld = spd_inverse_ld(n), the n x n matrix in its top-left corner)
 // is replaced by its inverse; work holds ld x ld doubles; *info (device) =
@@ -355,10 +379,10 @@ cudaError_t spd_inverse_to_half(const double* inv, int n, int ld, unsigned long 
                                 cudaStream_t s);
 
 // Per block of k_pcg (grid blocks over the SELL-32 slices of n rows): the
-// first and last block owning a column its slices read, from the CSR
-// pattern (rp, col; rows sorted ascending) with the SELL padding's column 0
-// for empty rows.
-void pcg_neighbor_ranges(int n, int grid, const int* rp, const int* col, int* lo, int* hi);
+// first and last block owning a column its slices read, from each row's
+// first and last column (rows sorted ascending; last < first for an empty
+// row) with the SELL padding's column 0 for empty rows.
+void pcg_neighbor_ranges(int n, int grid, const int* first, const int* last, int* lo, int* hi);
 template <class VT>
 cudaError_t launch_pcg(const PcgArgs<VT>& a, int grid, cudaStream_t s);
 template <class VT>

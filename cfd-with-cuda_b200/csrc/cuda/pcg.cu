@@ -400,7 +400,7 @@ int pcg_max_grid(int n, int device) {
   return (int)std::min(cap, want);
 }
 
-void pcg_neighbor_ranges(int n, int grid, const int* rp, const int* col, int* lo, int* hi) {
+void pcg_neighbor_ranges(int n, int grid, const int* first, const int* last, int* lo, int* hi) {
   const int ns = (n + 31) / 32;
   const long long W = (long long)grid * kPcgWarps;
   std::vector<int> owner(ns);
@@ -418,12 +418,12 @@ void pcg_neighbor_ranges(int n, int grid, const int* rp, const int* col, int* lo
       int w = 0;
       bool empty_row = false;
       for (int r = 32 * s; r < 32 * s + 32; r++) {
-        const int len = r < n ? rp[r + 1] - rp[r] : 0;
-        w = std::max(w, len);
-        empty_row = empty_row || len == 0;
-        if (len > 0) {  // rows are sorted ascending
-          cmin = std::min(cmin, col[rp[r]]);
-          cmax = std::max(cmax, col[rp[r + 1] - 1]);
+        const bool has = r < n && last[r] >= first[r];
+        w = std::max(w, has ? 1 : 0);
+        empty_row = empty_row || !has;
+        if (has) {
+          cmin = std::min(cmin, first[r]);
+          cmax = std::max(cmax, last[r]);
         }
       }
       if (w > 0 && empty_row) {

@@ -358,7 +358,7 @@ void build_pattern(int nrows, const std::vector<int>& inc_rp, const std::vector<
 
 }  // namespace
 
-int preprocess(HostProblem& P, std::string& err) {
+int preprocess(HostProblem& P, std::string& err, bool patterns) {
   const int NE = P.NE, NCN = P.NCN;
   // ---- mid-edge nodes (first appearance in element-then-edge order) ----
   std::vector<uint64_t> ekeys((size_t)NE * 12);
@@ -456,6 +456,11 @@ int preprocess(HostProblem& P, std::string& err) {
       }
     }
   }
+  return patterns ? build_patterns(P, err) : CFD_OK;
+}
+
+int build_patterns(HostProblem& P, std::string& err) {
+  const int NE = P.NE;
   // ---- node -> element incidence ----
   std::vector<int> inc_rp(P.NN + 1, 0), inc_el((size_t)NE * 27);
   for (size_t t = 0; t < P.ltog.size(); t++) inc_rp[P.ltog[t] + 1]++;
@@ -533,6 +538,9 @@ int preprocess(HostProblem& P, std::string& err) {
     err = "K has more than 2^31 non-zeros";
     return CFD_E_BADINPUT;
   }
+  P.nnzK = (long long)P.k_col.size();
+  P.nnzG = (long long)P.g_col.size();
+  P.nnzZ = (long long)P.z_col.size();
   return CFD_OK;
 }
 

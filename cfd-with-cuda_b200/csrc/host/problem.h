@@ -36,14 +36,20 @@ struct HostProblem {
   std::vector<int> gt_rp, gt_col, gt_pos; // NNp x NN; gt_pos = index of (v,p) in G
   std::vector<int> z_rp, z_col;           // NNp x NNp
   int maxZrow = 0, maxKrow = 0, maxGrow = 0, maxGtrow = 0;
+  // stored entries of K, G (= G^T) and Z, whichever side built the patterns
+  long long nnzK = 0, nnzG = 0, nnzZ = 0;
 };
 
 // readInputFile semantics (blascoCodinaHuerta.cpp:528-725).  Returns 0 or a
 // negative cfd_status; err receives a message.
 int read_inp(const std::string& path, HostProblem& P, std::string& err);
 
-// Fills NN, coord, ltog (mid nodes), bcnode/bcid, monPoint and all patterns.
-int preprocess(HostProblem& P, std::string& err);
+// Fills NN, coord, ltog (mid nodes), bcnode/bcid, monPoint and, with
+// patterns, every CSR pattern (the solver builds them on the device
+// instead and calls build_patterns only as a fallback).
+int preprocess(HostProblem& P, std::string& err, bool patterns = true);
+// The CSR patterns of K, G, G^T (with gt_pos) and Z from ltog.
+int build_patterns(HostProblem& P, std::string& err);
 
 // Conflict-free greedy colouring of the elements over their corner nodes
 // (elements that share a node get different colours): order lists the
