@@ -231,6 +231,15 @@ struct cfd_ctx {
   DevBuf<double> cs_f[3], cs_e64;
   DevBuf<float> cs_c32, cs_e32;  // coarse right-hand side (both precisions), FP32 coarse solution
   DevBuf<__half> cs_inv16;
+
+  // blocks of the flexible-CG update kernel, four entries per thread:
+  // 4 per SM by default (fewer partial sums for the last block to add than
+  // one thread per entry; 131.5 against 127.9 steps/s on the 64^3 two-level
+  // line); CFD_FCG_UPDATE_BLOCKS overrides it, 0 = one thread per entry
+  int upd_grid = -1;
+  // CFD_HOST_PATTERNS=1: the CSR patterns are built on the host (the
+  // fallback of the device build)
+  bool host_patterns = false;
   DevBuf<float> zst32;  // Z in structured (125-tap) form for the FP32 inner solves, when it applies
   bool zst_ok = false;
   int cs_ld = 0;
@@ -561,7 +570,7 @@ int upload_problem(cfd_ctx* c) {
   // a row exceeds what the device build holds)
   bool on_device = false;
   if (P.k_rp.empty()) {
-    int rc = device_patterns(c, on_device);
+    int rc = c->host_patterns ? CFD_OK : device_patterns(c, on_device);
     if (rc) return rc;
     if (!on_device) {
       rc = build_patterns(P, c->err);
@@ -1216,6 +1225,7 @@ int run_fcg(cfd_ctx* c, const VT* b, VT* x, int warm, double rtol, int maxit, do
   const bool split = sizeof(VT) == 4 && a.stencil && c->cs_zp_ok && !pmap && c->fcg_split;
   a.dinv = dinv;
   a.pdl = c->pdl ? 1 : 0;
+  a.upd_grid = c->upd_grid >= 0 ? c->upd_grid : 4 * c->num_sms;
   if (split) {
     if (!c->fcg_z1.p) CU(c->fcg_z1.alloc(n));
     a.z1 = reinterpret_cast<VT*>(c->fcg_z1.p);
@@ -1569,6 +1579,8 @@ int cfd_create(cfd_ctx** out, int device) {
   if (const char* e = std::getenv("CFD_FCG_PERSIST")) c->fcg_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_HOST")) c->coarse_on_host = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_PDL")) c->pdl = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_FCG_UPDATE_BLOCKS")) c->upd_grid = std::max(0, std::atoi(e));
+  if (const char* e = std::getenv("CFD_HOST_PATTERNS")) c->host_patterns = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_L2_PERSIST")) c->l2_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_SPACING")) c->coarse_spacing = std::atof(e);
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;

@@ -360,22 +360,43 @@ __global__ void __launch_bounds__(kFcgThreads) k_fcg_update(FcgArgs<VT> a) {
   for (int j = 0; j < kFcgMaxM; j++) beta[j] = (VT)sc[kFcgBeta0 + j];
   const size_t n = (size_t)a.n;
   double v[1] = {0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-    VT pi = a.z[i], qi = a.w[i];
+  // UPD grid-stride elements per thread with all their loads issued before
+  // any store (the element order, and so the order of the (r, r) sum, is the
+  // grid-stride order)
+  constexpr int UPD = 4;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < a.n; i0 += UPD * stride) {
+    VT pi[UPD], qi[UPD], xo[UPD], ro[UPD];
 #pragma unroll
-    for (int j = 0; j < kFcgMaxM; j++) {
-      if (j < nd) {
-        pi -= beta[j] * a.p[j * n + i];
-        qi -= beta[j] * a.q[j * n + i];
+    for (int u = 0; u < UPD; u++) {
+      const int i = i0 + u * stride;
+      if (i < a.n) {
+        pi[u] = a.z[i];
+        qi[u] = a.w[i];
+        xo[u] = a.x[i];
+        ro[u] = a.r[i];
+#pragma unroll
+        for (int j = 0; j < kFcgMaxM; j++) {
+          if (j < nd) {
+            pi[u] -= beta[j] * a.p[j * n + i];
+            qi[u] -= beta[j] * a.q[j * n + i];
+          }
+        }
       }
     }
-    a.p[slot * n + i] = pi;
-    a.q[slot * n + i] = qi;
-    a.x[i] += alpha * pi;
-    const VT ri = a.r[i] - alpha * qi;
-    a.r[i] = ri;
-    if (a.z1) a.z1[i] = a.dinv[i] * ri;
-    v[0] += (double)ri * ri;
+#pragma unroll
+    for (int u = 0; u < UPD; u++) {
+      const int i = i0 + u * stride;
+      if (i < a.n) {
+        a.p[slot * n + i] = pi[u];
+        a.q[slot * n + i] = qi[u];
+        a.x[i] = xo[u] + alpha * pi[u];
+        const VT ri = ro[u] - alpha * qi[u];
+        a.r[i] = ri;
+        if (a.z1) a.z1[i] = a.dinv[i] * ri;
+        v[0] += (double)ri * ri;
+      }
+    }
   }
   block_sum<1>(v);
   if (!post_partials<1>(v, a.st.part, a.st.cnt)) return;
@@ -501,7 +522,9 @@ cudaError_t launch_fcg_combine(const FcgArgs<VT>& a, const CoarseArgs<VT>& ca, c
 
 template <class VT>
 cudaError_t launch_fcg_update(const FcgArgs<VT>& a, cudaStream_t s) {
-  return launch_k(a.pdl != 0, k_fcg_update<VT>, dim3(nblocks(a.n)), dim3(kFcgThreads), 0, s, a);
+  int grid = nblocks(a.n);
+  if (a.upd_grid > 0 && a.upd_grid < grid) grid = a.upd_grid;
+  return launch_k(a.pdl != 0, k_fcg_update<VT>, dim3(grid), dim3(kFcgThreads), 0, s, a);
 }
 
 template <class VT>

@@ -235,6 +235,7 @@ template <class VT> struct FcgArgs {
   VT* z1;
   const VT* dinv;
   int pdl;  // 1: the iteration kernels launch with programmatic dependent launch
+  int upd_grid;  // > 0: blocks of the update kernel (default: one thread per entry, at most kFcgMaxBlocks)
 };
 struct Int3 {
   int v[3];

@@ -62,3 +62,29 @@ def test_device_patterns_of_the_64_cavity_equal_host_patterns(tmp_path):
         assert np.array_equal(col_d, col_h), which
     s.close()
     h.close()
+
+
+def test_host_pattern_fallback_gives_the_same_run(decks):
+    """CFD_HOST_PATTERNS=1 takes the host build (the fallback when a row has
+    more candidates than the device build holds): the same operators and a
+    bit-identical run in deterministic mode."""
+    import os
+    import cfdfs
+    out = []
+    for host in (True, False):
+        os.environ["CFD_HOST_PATTERNS"] = "1" if host else "0"
+        try:
+            s = cfdfs.Solver(device=0, deterministic=1)
+        finally:
+            del os.environ["CFD_HOST_PATTERNS"]
+        s.load(decks["graded"])
+        s.step0()
+        mats = [s.matrix(w) for w in ("K", "G", "GT", "Z")]
+        s.run(3)
+        out.append((mats, *s.state()))
+        s.close()
+    (ma, Ua, Pa), (mb, Ub, Pb) = out
+    for a, b in zip(ma, mb):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    assert np.array_equal(Ua, Ub) and np.array_equal(Pa, Pb)
