@@ -283,8 +283,12 @@ def run_ours(args, rank, world, local_rank):
         return max_over_ranks(dist, x)
 
     def timed_solver(precision, precond, steps, warmup):
+        # the FP64 Jacobi-PCG comparison path always starts its solves from
+        # x0 = 0, as the reference does; --cg-warm starts the measured path's
+        # solves from the previous sub-iteration's pressure increment
+        warm = args.cg_warm if precision == cfdfs.MIXED else 0
         s = cfdfs.Solver(device=local_rank, precision=precision, cg_rtol=1e-8, cg_maxit=args.cg_maxit,
-                         precond=pc_of[precond], fcg_net_iters=args.net_iters)
+                         precond=pc_of[precond], fcg_net_iters=args.net_iters, cg_warm=warm)
         t0 = time.time()
         s.load(deck)
         t1 = time.time()
@@ -487,7 +491,7 @@ def run_ours(args, rank, world, local_rank):
                         "twolevel": "Jacobi + Galerkin coarse-space correction (17^3 lattice) in CG",
                         "jacobi": "jacobi"}[args.precond],
                        "weights": os.path.relpath(args.weights, ROOT) if learned else None,
-                       "ngp": 8, "cg_rtol": 1e-8, "cg_x0": "zero",
+                       "ngp": 8, "cg_rtol": 1e-8, "cg_x0": "previous increment" if args.cg_warm else "zero",
                        "timed_steps": f"steps {args.warmup + 1}..{args.warmup + args.steps} of the run from rest",
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush needed)",
                        "setup_s": round(r["setup_s"], 2), "setup_parts_s": r["setup_parts"]},
@@ -686,6 +690,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=1, help="0 skips the FP64 Jacobi-PCG comparison run")
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--cg-maxit", type=int, default=5000)
+    ap.add_argument("--cg-warm", type=int, default=0,
+                    help="1: the measured path's pressure solves start from the previous increment (default x0 = 0)")
     ap.add_argument("--cpu-budget", type=float, default=90.0,
                     help="seconds of timed reference steps before the reference arm stops")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
