@@ -282,11 +282,12 @@ def run_ours(args, rank, world, local_rank):
     def ranks_max(x: float) -> float:
         return max_over_ranks(dist, x)
 
-    def timed_solver(precision, precond, steps, warmup):
-        # the FP64 Jacobi-PCG comparison path always starts its solves from
-        # x0 = 0, as the reference does; --cg-warm starts the measured path's
-        # solves from the previous sub-iteration's pressure increment
-        warm = args.cg_warm if precision == cfdfs.MIXED else 0
+    def timed_solver(precision, precond, steps, warmup, warm=None):
+        # --cg-warm 1 (the default) starts the measured path's pressure solves
+        # from the previous sub-iteration's pressure increment; the FP64
+        # Jacobi-PCG comparison path starts them from x0 = 0, as the reference
+        # does (warm=0)
+        warm = args.cg_warm if warm is None else warm
         s = cfdfs.Solver(device=local_rank, precision=precision, cg_rtol=1e-8, cg_maxit=args.cg_maxit,
                          precond=pc_of[precond], fcg_net_iters=args.net_iters, cg_warm=warm)
         t0 = time.time()
@@ -348,10 +349,10 @@ def run_ours(args, rank, world, local_rank):
     # (denominator of the headline target, and the accuracy reference)
     fp64, acc = None, None
     if args.fp64_steps and not (precision == cfdfs.FP64 and args.precond == "jacobi"):
-        s64, r64 = timed_solver(cfdfs.FP64, "jacobi", args.steps, args.warmup)
+        s64, r64 = timed_solver(cfdfs.FP64, "jacobi", args.steps, args.warmup, warm=0)
         ms64 = ranks_max(r64["ms"])
         fp64 = dict(steps=args.steps, steps_per_s=round(replica_rate(world, args.steps, ms64), 4),
-                    ms_per_step=round(ms64 / args.steps, 3),
+                    ms_per_step=round(ms64 / args.steps, 3), cg_x0="zero",
                     cg_iters_per_step=round(r64["st"].cg_iters / max(1, r64["st"].steps), 1))
         U1, P1 = s.state()
         U0, P0 = s64.state()
@@ -690,8 +691,9 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=1, help="0 skips the FP64 Jacobi-PCG comparison run")
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--cg-maxit", type=int, default=5000)
-    ap.add_argument("--cg-warm", type=int, default=0,
-                    help="1: the measured path's pressure solves start from the previous increment (default x0 = 0)")
+    ap.add_argument("--cg-warm", type=int, default=1,
+                    help="1: the measured path's pressure solves start from the previous sub-iteration's "
+                         "increment; 0: from x0 = 0 (the reference's choice, always used by the FP64 comparison)")
     ap.add_argument("--cpu-budget", type=float, default=90.0,
                     help="seconds of timed reference steps before the reference arm stops")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
