@@ -289,7 +289,8 @@ def run_ours(args, rank, world, local_rank):
         # does (warm=0)
         warm = args.cg_warm if warm is None else warm
         s = cfdfs.Solver(device=local_rank, precision=precision, cg_rtol=1e-8, cg_maxit=args.cg_maxit,
-                         precond=pc_of[precond], fcg_net_iters=args.net_iters, cg_warm=warm)
+                         precond=pc_of[precond], fcg_net_iters=args.net_iters, cg_warm=warm,
+                         inner_rtol=args.inner_rtol)
         t0 = time.time()
         s.load(deck)
         t1 = time.time()
@@ -493,6 +494,7 @@ def run_ours(args, rank, world, local_rank):
                         "jacobi": "jacobi"}[args.precond],
                        "weights": os.path.relpath(args.weights, ROOT) if learned else None,
                        "ngp": 8, "cg_rtol": 1e-8, "cg_x0": "previous increment" if args.cg_warm else "zero",
+                       "inner_rtol": args.inner_rtol if precision == cfdfs.MIXED else None,
                        "timed_steps": f"steps {args.warmup + 1}..{args.warmup + args.steps} of the run from rest",
                        "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (no flush needed)",
                        "setup_s": round(r["setup_s"], 2), "setup_parts_s": r["setup_parts"]},
@@ -691,6 +693,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=1, help="0 skips the FP64 Jacobi-PCG comparison run")
     ap.add_argument("--profile-steps", type=int, default=2)
     ap.add_argument("--cg-maxit", type=int, default=5000)
+    ap.add_argument("--inner-rtol", type=float, default=1e-5,
+                    help="mixed precision: relative tolerance of each FP32 inner solve of the FP64 refinement")
     ap.add_argument("--cg-warm", type=int, default=1,
                     help="1: the measured path's pressure solves start from the previous sub-iteration's "
                          "increment; 0: from x0 = 0 (the reference's choice, always used by the FP64 comparison)")

@@ -98,7 +98,7 @@ def main():
         pass
     a = Args()
     a.steps, a.warmup, a.precision, a.n, a.precond, a.weights = 4, 3, "mixed", 4, "learned", bench.WEIGHTS
-    a.net_iters, a.fp64_steps, a.profile_steps, a.cg_maxit, a.cg_warm = 1, 1, 2, 5000, 0
+    a.net_iters, a.fp64_steps, a.profile_steps, a.cg_maxit, a.cg_warm, a.inner_rtol = 1, 1, 2, 5000, 0, 1e-4
     a.cpu_budget, a.cpu_baseline = 1.0, False
     print(json.dumps(bench.run_ours(a, 0, 1, 0)))
 
