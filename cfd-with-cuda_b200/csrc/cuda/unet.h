@@ -101,23 +101,34 @@ struct ConvTcParams {
   int act;
   const int* skip;
   int* err;  // set when a bounded wait gives up
+  // persistent form: shared-memory stages of the halo brick (1 or 2), TMEM
+  // columns allocated per CTA and accumulators in the ring; fold = 1: the
+  // three dx taps share one MMA (N = 3 nout columns, dx-major), nout output
+  // channels per slice
+  int astages, acc_cols, nacc, fold, nout;
 };
 struct ConvTcPlan {
   ConvTcParams p;
   int grid_x;
   size_t smem;
   int ready;
+  int pipe;  // 1: the persistent, pipelined kernel (grid_x CTAs, one dimension)
 };
 bool conv_tc_supported(const ConvDesc& d);
 int conv_tc_slice_width(int cin, int cout, int stride);
 long long conv_tc_pack_elems(int cin, int cout, int stride);
 // Rearranges [27][cin][cout] BF16 weights into per-tap canonical tensor-core
 // blocks (wpack holds conv_tc_pack_elems values).
+// fold = 1 packs the dx-folded layout of the persistent kernel (stride 1):
+// per slice, 9 (dy, dz) groups of N = 3 x slice-width columns, column
+// (dx + 1) x width + output channel.  The same number of values.
 cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
-                         cudaStream_t s);
+                         cudaStream_t s, int fold = 0);
 // Builds the launch plan (bricks, shared-memory layout) of a supported
-// convolution; 0 on success.
-int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan);
+// convolution; 0 on success.  pipe = 1 plans the persistent, pipelined
+// kernel instead of one CTA per brick, pipe = 2 that kernel with the dx
+// taps folded into N (stride 1 only; the weights packed with fold = 1).
+int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan, int pipe = 0);
 // Launches a planned convolution; out_f32 (FP32-output layers) and skip
 // replace the plan's pointers for this launch.
 cudaError_t conv3_forward_tc(const ConvTcPlan& plan, float* out_f32, const int* skip, int* err, cudaStream_t s);

@@ -104,6 +104,26 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// tcgen05.ld without its wait, for several loads in flight; tmem_wait_ld
+// then waits for all of them, and reg_pin16 (an empty statement that
+// "modifies" the registers, placed after the wait) keeps every use of the
+// loaded registers after the wait.
+__device__ __forceinline__ void tmem_ld16_async(unsigned taddr, unsigned (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void reg_pin16(unsigned (&r)[16]) {
+  asm volatile(""
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15]));
+}
+
 // One TMA tensor copy of a 4-D box (coordinates innermost first) into shared
 // memory, completing on the mbarrier (no multicast).
 __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -320,6 +340,330 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
   }
 }
 
+// ---- the persistent, pipelined form ----
+// CTA c serves output-channel slice c % nslices and loops over the bricks
+// c / nslices, c / nslices + gridDim.x / nslices, ...  Three roles run at
+// once:
+// - warp 4 kEpiGroups (lane 0) brings a brick's halo in by TMA into one of astages
+//   shared-memory stages (full[stage]);
+// - the next warp (lane 0) issues the MMAs of one 128-row tile at a time into one
+//   of nacc accumulators of N TMEM columns, commits each tile to
+//   mdone[acc], and after a brick's last tile commits bfree[stage] (the
+//   stage may be refilled once those MMAs have read it);
+// - warps 0 .. 4 kEpiGroups - 1, groups of four taking tiles in turn, read each
+//   finished accumulator back (warp w owns TMEM lanes 32 (w % 4) .. + 31,
+//   those of its sub-partition), write the outputs and free it (afree[acc],
+//   one arrival per warp of the group).  One group of four warps, one per
+//   sub-partition, leaves every latency of the epilogue exposed; several
+//   overlap.  Accumulator acc is read by group acc % kEpiGroups only.
+// So the epilogue of a tile overlaps the MMAs of the next ones, and with two
+// stages the copy of the next brick overlaps the MMAs of the current one.
+// The slice's weights are loaded once per CTA.
+//
+// FOLD (stride 1): the MMAs of a tile are 9 (dy, dz) groups of K = cin, each
+// against the three dx taps side by side (N = 3 nout columns, column
+// (dx + 1) nout + c), so a 16-channel layer issues 9 MMAs of N = 48 per tile
+// instead of 27 of N = 16.  The accumulator then holds D_dx[rho] =
+// sum over (dy, dz) of A[rho + HX dy + HX HY dz] W[dx, dy, dz], and output
+// row r is D_-1[r - 1] + D_0[r] + D_+1[r + 1]: the neighbouring rows come
+// from the neighbouring lanes (shuffles), and across the warps' 32-row
+// boundaries through shared memory.  A tile's 128 rows produce the 126
+// outputs between its first and last row, so tiles step by 126 rows.
+//
+// Every wait is bounded; a role whose wait gives up sets *err, stops, and
+// gives the copies or MMAs it has in flight one more bounded wait.
+constexpr int kEpiGroups = 3;  // groups of four epilogue warps, alternate tiles
+constexpr int kPipeThreads = 32 * (4 * kEpiGroups + 2);
+constexpr int kPipeAcc = 4;  // most accumulators in the ring
+static_assert(kPipeAcc >= kEpiGroups, "every epilogue group needs an accumulator");
+constexpr int kPipeBars = 5 + 2 * kPipeAcc + 2 * kEpiGroups;
+constexpr int kFoldChunks = 2;  // 16-channel chunks of a folded slice (nout <= 32)
+
+__device__ __forceinline__ void mbar_arrive_cta(unsigned long long* m) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(m)) : "memory");
+}
+// Bias, activation and store of 16 output channels of one voxel.
+__device__ __forceinline__ void store16(const ConvTcParams& p, long long v, int n0, int c, const float* sbias,
+                                        const float (&acc)[16]) {
+  if (p.out_f32) {
+    if (n0 + c == 0) p.out_f32[v] = acc[0] + sbias[0];
+    return;
+  }
+  __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    float y = acc[i] + sbias[c + i];
+    if (p.act && y < 0.f) y *= kLeaky;
+    o[i] = __float2bfloat16(y);
+  }
+  uint4* dst = (uint4*)(p.out + v * p.cout + n0 + c);
+  dst[0] = ((const uint4*)o)[0];
+  dst[1] = ((const uint4*)o)[1];
+}
+
+template <int CIN, int STRIDE, bool FOLD>
+__global__ void __launch_bounds__(kPipeThreads) k_conv_pipe(const __grid_constant__ ConvTcParams p) {
+  static_assert(!FOLD || STRIDE == 1, "the dx fold needs stride 1");
+  constexpr int NCH = CIN / 8, KSTEPS = CIN / 16, NPH = STRIDE == 2 ? 8 : 1;
+  constexpr int NG = FOLD ? 9 : 27;       // MMA groups per K step
+  constexpr int TSTEP = FOLD ? 126 : 128;  // output rows per tile
+  if (p.skip && *p.skip) return;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int nst = p.astages, nacc = p.nacc;
+  const size_t stage_bytes = (size_t)NPH * NCH * p.plane_bytes;
+  unsigned char* W = smem + (size_t)nst * stage_bytes;
+  const unsigned wbytes = 27u * CIN * p.nout * 2u;
+  // wbar, full[2], bfree[2], mdone[kPipeAcc], afree[kPipeAcc], xbar[kEpiGroups][2]
+  unsigned long long* bars = (unsigned long long*)(W + wbytes);  // wbytes is a multiple of 16
+  unsigned long long *wbar = bars, *full = bars + 1, *bfree = bars + 3, *mdone = bars + 5,
+                     *afree = bars + 5 + kPipeAcc, *xbar = bars + 5 + 2 * kPipeAcc;
+  unsigned* tmem_slot = (unsigned*)(bars + kPipeBars);
+  float* sbias = (float*)(tmem_slot + 2);  // nout floats
+  float* xs = sbias + p.nout;              // FOLD: [kEpiGroups][2][2][4][nout] edge rows
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int HX = p.halo[0], HY = p.halo[1];
+  const int slice = blockIdx.x % p.nslices;
+  const int cpos = blockIdx.x / p.nslices, cstride = gridDim.x / p.nslices;
+  const int nbricks = p.nb[0] * p.nb[1] * p.nb[2];
+  const int nunits = cpos < nbricks ? (nbricks - 1 - cpos) / cstride + 1 : 0;
+  auto brick_origin = [&](int u, int& x0, int& y0, int& z0) {
+    const int b = cpos + u * cstride;
+    x0 = (b % p.nb[0]) * p.brick[0];
+    y0 = ((b / p.nb[0]) % p.nb[1]) * p.brick[1];
+    z0 = (b / (p.nb[0] * p.nb[1])) * p.brick[2];
+  };
+
+  if (threadIdx.x == 0) {
+    mbar_init(wbar, 1);
+    for (int i = 0; i < 2; i++) {
+      mbar_init(full + i, 1);
+      mbar_init(bfree + i, 1);
+    }
+    for (int i = 0; i < kPipeAcc; i++) {
+      mbar_init(mdone + i, 1);
+      mbar_init(afree + i, 4);
+    }
+    for (int i = 0; i < 2 * kEpiGroups; i++) mbar_init(xbar + i, 4);
+    mbar_init_fence();
+  }
+  if (warp == 0) tmem_alloc(tmem_slot, (unsigned)p.acc_cols);
+  for (int i = threadIdx.x; i < p.nout; i += blockDim.x) {
+    const int co = slice * p.nout + i;
+    sbias[i] = co < p.cout ? p.bias[co] : 0.f;
+  }
+  {
+    // rows past the halo box that tap shifts of the last tiles read: zeros,
+    // in every stage, once (the copies never write them)
+    const int nbox = HX * HY * p.halo[2], slack = p.rows - nbox;
+    const int per_stage = NPH * NCH * slack;
+    for (int i = threadIdx.x; i < nst * per_stage; i += blockDim.x) {
+      const int st = i / per_stage, rem = i % per_stage;
+      const int pl = rem / slack, row = nbox + rem % slack;
+      *(uint4*)(smem + st * stage_bytes + (size_t)pl * p.plane_bytes + (size_t)row * 16) = make_uint4(0, 0, 0, 0);
+    }
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const unsigned tmem = *tmem_slot;
+  const unsigned abytes = (unsigned)NPH * NCH * 16u * (unsigned)(HX * HY * p.halo[2]);
+  const int ntiles = nunits * p.tiles;
+  bool ok = true;
+
+  if (warp == 4 * kEpiGroups) {
+    if (lane == 0) {
+      int issued = 0;
+      mbar_expect_tx(wbar, wbytes);
+      bulk_g2s(W, p.wpack + (size_t)slice * 27 * CIN * p.nout, wbytes, wbar);
+      for (int u = 0; u < nunits; u++) {
+        const int st = u % nst;
+        if (u >= nst && !mbar_wait_bounded(bfree + st, (unsigned)((u / nst - 1) & 1), kTcWaitNs)) {
+          ok = false;
+          break;
+        }
+        int x0, y0, z0;
+        brick_origin(u, x0, y0, z0);
+        mbar_expect_tx(full + st, abytes);
+        load_halo<NCH, STRIDE>(p, smem + st * stage_bytes, x0, y0, z0, full + st);
+        issued = u + 1;
+      }
+      if (!ok) {
+        if (p.err) atomicExch(p.err, 1);
+        mbar_wait_bounded(wbar, 0, kTcWaitNs);
+        for (int u = issued > nst ? issued - nst : 0; u < issued; u++)
+          mbar_wait_bounded(full + u % nst, (unsigned)((u / nst) & 1), kTcWaitNs);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 4 * kEpiGroups + 1) {
+    if (lane == 0) {
+      const unsigned idesc = umma_idesc(p.N);
+      const unsigned long long db0 = umma_desc(smem_u32(W), (unsigned)(p.N >> 3) * 128u, 128u);
+      const unsigned plane16 = (unsigned)p.plane_bytes >> 4;
+      const unsigned wg16 = (unsigned)(CIN * p.N * 2) >> 4, wk16 = (unsigned)(p.N >> 3) * 8u;
+      int toff[NG];
+#pragma unroll
+      for (int k = 0; k < NG; k++) {
+        int off, plane0 = 0;
+        if (FOLD) {
+          const int dy = k % 3 - 1, dz = k / 3 - 1;
+          off = HX * (dy + HY * dz);
+        } else {
+          const int dx = k % 3 - 1, dy = (k / 3) % 3 - 1, dz = k / 9 - 1;
+          if (STRIDE == 2) {
+            off = -(dx < 0) - HX * ((dy < 0) + HY * (dz < 0));
+            plane0 = ((dx != 0) + 2 * (dy != 0) + 4 * (dz != 0)) * NCH;
+          } else {
+            off = dx + HX * (dy + HY * dz);
+          }
+        }
+        toff[k] = plane0 * (int)plane16 + off;
+      }
+      int g = 0;  // tiles issued
+      ok = mbar_wait_bounded(wbar, 0, kTcWaitNs);
+      for (int u = 0; u < nunits && ok; u++) {
+        const int st = u % nst;
+        if (!mbar_wait_bounded(full + st, (unsigned)((u / nst) & 1), kTcWaitNs)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const unsigned long long da0 = umma_desc(smem_u32(smem + st * stage_bytes), (unsigned)p.plane_bytes, 128u);
+        for (int t = 0; t < p.tiles; t++, g++) {
+          const int r = g % nacc;
+          if (g >= nacc && !mbar_wait_bounded(afree + r, (unsigned)((g / nacc - 1) & 1), kTcWaitNs)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const unsigned d = tmem + (unsigned)(r * p.N);
+          const unsigned long long dat = da0 + (unsigned)(p.q0 - (FOLD ? 1 : 0) + TSTEP * t);
+#pragma unroll
+          for (int k = 0; k < NG; k++) {
+            const unsigned long long dak = dat + (unsigned long long)(long long)toff[k];
+            const unsigned long long dbk = db0 + (unsigned long long)k * wg16;
+#pragma unroll
+            for (int j = 0; j < KSTEPS; j++)
+              umma(d, dak + (unsigned long long)(2 * j) * plane16, dbk + (unsigned long long)(2 * j) * wk16, idesc,
+                   (k | j) != 0);
+          }
+          umma_commit(mdone + r);
+        }
+        if (ok) umma_commit(bfree + st);
+      }
+      if (!ok) {
+        if (p.err) atomicExch(p.err, 1);
+        if (g > 0) mbar_wait_bounded(mdone + (g - 1) % nacc, (unsigned)(((g - 1) / nacc) & 1), kTcWaitNs);
+      } else {
+        // the last arrivals on bfree land before the CTA ends
+        for (int u = nunits > nst ? nunits - nst : 0; u < nunits; u++)
+          mbar_wait_bounded(bfree + u % nst, (unsigned)((u / nst) & 1), kTcWaitNs);
+      }
+    }
+    __syncwarp();
+  } else {
+    // the epilogue: group eg takes tiles eg, eg + kEpiGroups, ...; its warp
+    // q owns rows 32q .. 32q + 31 (TMEM lanes of the warp's sub-partition)
+    const int n0 = slice * p.nout, eg = warp >> 2, q = warp & 3;
+    const unsigned lanebase = tmem + ((unsigned)(32 * q) << 16);
+    for (int g = eg; g < ntiles; g += kEpiGroups) {
+      const int u = g / p.tiles, t = g - u * p.tiles, r = g % nacc, k = g / kEpiGroups;
+      int x0, y0, z0;
+      brick_origin(u, x0, y0, z0);
+      // the MMA warp keeps going while the epilogue waits, so every lane
+      // takes the same branch on the wait's outcome
+      if (!__all_sync(0xffffffffu, mbar_wait_bounded(mdone + r, (unsigned)((g / nacc) & 1), kTcWaitNs))) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int row = 32 * q + lane;
+      const int prow = FOLD ? p.q0 - 1 + TSTEP * t + row : p.q0 + TSTEP * t + row;
+      const int hz = prow / (HX * HY), rem = prow - hz * HX * HY;
+      const int hy = rem / HX, hx = rem - hy * HX;
+      const int X = x0 + hx - 1, Y = y0 + hy - 1, Z = z0 + hz - 1;
+      const bool valid = (!FOLD || (row >= 1 && row <= 126)) && hx >= 1 && hx <= p.brick[0] && hy >= 1 &&
+                         hy <= p.brick[1] && hz >= 1 && hz <= p.brick[2] && X < p.dims[0] && Y < p.dims[1] &&
+                         Z < p.dims[2];
+      const long long v = X + (long long)p.dims[0] * (Y + (long long)p.dims[1] * Z);
+      const unsigned col0 = (unsigned)(r * p.N);
+      if constexpr (FOLD) {
+        // edge rows across the warps' boundaries: lane 31 posts D_-1 of its
+        // row for the next warp's lane 0, lane 0 posts D_+1 for the previous
+        // warp's lane 31.  The buffers and the mbarrier that publishes them
+        // (one arrival per warp, a bounded wait) are the group's own and
+        // alternate with its tiles (k counts them): a warp writes the buffers
+        // of its tile k + 2 only after every warp of the group has arrived
+        // for tile k + 1, that is after its reads of tile k.
+        // All of the tile's columns are read with one wait (kFoldChunks x 16
+        // output channels at most, checked by the plan).
+        const int nout = p.nout, nch = nout / 16;
+        float* xm = xs + (size_t)((eg * 2 + (k & 1)) * 2 + 0) * 4 * nout;
+        float* xp = xs + (size_t)((eg * 2 + (k & 1)) * 2 + 1) * 4 * nout;
+        unsigned raw[3][kFoldChunks][16];
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+          for (int h = 0; h < kFoldChunks; h++)
+            if (h < nch) tmem_ld16_async(lanebase + col0 + (unsigned)(b * nout + 16 * h), raw[b][h]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int b = 0; b < 3; b++)
+#pragma unroll
+          for (int h = 0; h < kFoldChunks; h++) reg_pin16(raw[b][h]);
+#pragma unroll
+        for (int h = 0; h < kFoldChunks; h++) {
+          if (h >= nch) break;
+          if (lane == 31)
+#pragma unroll
+            for (int i = 0; i < 16; i++) xm[q * nout + 16 * h + i] = __uint_as_float(raw[0][h][i]);
+          if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < 16; i++) xp[q * nout + 16 * h + i] = __uint_as_float(raw[2][h][i]);
+        }
+        __syncwarp();
+        unsigned long long* xb = xbar + 2 * eg + (k & 1);
+        if (lane == 0) mbar_arrive_cta(xb);
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(xb, (unsigned)((k >> 1) & 1), kTcWaitNs))) {
+          ok = false;
+          break;
+        }
+#pragma unroll
+        for (int h = 0; h < kFoldChunks; h++) {
+          if (h >= nch) break;
+          float acc[16];
+#pragma unroll
+          for (int i = 0; i < 16; i++) {
+            float left = __shfl_up_sync(0xffffffffu, __uint_as_float(raw[0][h][i]), 1);
+            float right = __shfl_down_sync(0xffffffffu, __uint_as_float(raw[2][h][i]), 1);
+            if (lane == 0) left = q > 0 ? xm[(q - 1) * nout + 16 * h + i] : 0.f;
+            if (lane == 31) right = q < 3 ? xp[(q + 1) * nout + 16 * h + i] : 0.f;
+            acc[i] = (left + __uint_as_float(raw[1][h][i])) + right;
+          }
+          if (valid) store16(p, v, n0, 16 * h, sbias, acc);
+        }
+      } else {
+        for (int c = 0; c < p.nout; c += 16) {
+          float acc[16];
+          tmem_ld16(lanebase + col0 + (unsigned)c, acc);
+          if (valid) store16(p, v, n0, c, sbias, acc);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cta(afree + r);
+    }
+    if (!ok && lane == 0 && p.err) atomicExch(p.err, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, (unsigned)p.acc_cols);
+  }
+}
+
 // wpack[slice][tap][kc][ng][n8][k8]: canonical K-major B blocks (8 output
 // channels x 8 input channels, 16-byte rows) per tap and output-channel slice.
 __global__ void k_pack_tc(const __nv_bfloat16* __restrict__ w, int cin, int cout, int N, int nslices,
@@ -335,6 +679,28 @@ __global__ void k_pack_tc(const __nv_bfloat16* __restrict__ w, int cin, int cout
     const int tap = (int)((r / ((N / 8) * (cin / 8))) % 27);
     const int slice = (int)(r / ((long long)(N / 8) * (cin / 8) * 27));
     const int ci = kc * 8 + k8, co = slice * N + ng * 8 + n8;
+    wp[i] = co < cout ? w[((size_t)tap * cin + ci) * cout + co] : __float2bfloat16(0.f);
+  }
+}
+
+// The dx-folded layout: wpack[slice][g][kc][ng][n8][k8] with g = (dy + 1) +
+// 3 (dz + 1) and column n = ng 8 + n8 = (dx + 1) W + c over N = 3 W columns
+// (W output channels per slice, channel slice W + c).
+__global__ void k_pack_fold(const __nv_bfloat16* __restrict__ w, int cin, int cout, int W, int nslices,
+                            __nv_bfloat16* wp) {
+  const int N = 3 * W;
+  const long long total = (long long)nslices * 9 * cin * N;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int k8 = (int)(i % 8);
+    const int n8 = (int)((i / 8) % 8);
+    const long long r = i / 64;
+    const int ng = (int)(r % (N / 8));
+    const int kc = (int)((r / (N / 8)) % (cin / 8));
+    const int g = (int)((r / ((N / 8) * (cin / 8))) % 9);
+    const int slice = (int)(r / ((long long)(N / 8) * (cin / 8) * 9));
+    const int n = ng * 8 + n8, dxi = n / W, co = slice * W + n % W;
+    const int tap = dxi + 3 * g, ci = kc * 8 + k8;
     wp[i] = co < cout ? w[((size_t)tap * cin + ci) * cout + co] : __float2bfloat16(0.f);
   }
 }
@@ -406,10 +772,15 @@ bool conv_tc_supported(const ConvDesc& d) {
 }
 
 cudaError_t conv_tc_pack(const __nv_bfloat16* w, int cin, int cout, int stride, __nv_bfloat16* wpack,
-                         cudaStream_t s) {
+                         cudaStream_t s, int fold) {
   const int N = conv_tc_slice_width(cin, cout, stride);
   const int ns = ceil_div(cout < 16 ? 16 : cout, N);
   const long long total = (long long)ns * 27 * cin * N;
+  if (fold) {
+    if (stride != 1) return cudaErrorInvalidValue;
+    k_pack_fold<<<(int)std::min<long long>((total + 255) / 256, 4096), 256, 0, s>>>(w, cin, cout, N, ns, wpack);
+    return cudaGetLastError();
+  }
   k_pack_tc<<<(int)std::min<long long>((total + 255) / 256, 4096), 256, 0, s>>>(w, cin, cout, N, ns, wpack);
   return cudaGetLastError();
 }
@@ -419,7 +790,94 @@ long long conv_tc_pack_elems(int cin, int cout, int stride) {
   return (long long)ceil_div(cout < 16 ? 16 : cout, N) * 27 * cin * N;
 }
 
-int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan) {
+namespace {
+
+// Halo-brick layout of the persistent form for bricks tz voxels deep: rows
+// per plane, tiles, shared memory per stage.  A tile computes rows
+// [first, first + 127] of the halo box and outputs 128 of them (126 with the
+// dx fold, whose first and last rows only feed their neighbours).
+int pipe_tstep(const ConvTcParams& p) { return p.fold ? 126 : 128; }
+void pipe_rows(const ConvTcParams& p, int& lo, int& hi) {
+  // lowest and highest shared-memory row that an MMA of the brick reads
+  const int HX = p.halo[0], HY = p.halo[1];
+  const int first = p.fold ? p.q0 - 1 : p.q0, last = first + pipe_tstep(p) * (p.tiles - 1) + 127;
+  const int down = p.fold ? HX + HX * HY : 1 + HX + HX * HY;
+  const int up = p.fold ? HX + HX * HY : (p.stride == 2 ? 0 : 1 + HX + HX * HY);
+  lo = first - down;
+  hi = last + up;
+}
+void pipe_layout(ConvTcParams& p, int tz, int hpad) {
+  const int HX = p.halo[0], HY = p.halo[1];
+  p.brick[2] = tz;
+  p.halo[2] = tz + hpad;
+  p.q0 = 1 + HX + HX * HY;
+  const int last = p.brick[0] + HX * (p.brick[1] + HY * p.brick[2]);
+  p.tiles = ceil_div(last - p.q0 + 1, pipe_tstep(p));
+  int lo, hi;
+  pipe_rows(p, lo, hi);
+  const int rows = std::max(HX * HY * p.halo[2], hi + 1);
+  p.rows = (rows + 7) & ~7;
+  p.plane_bytes = ((p.rows * 16) + 1023) & ~1023;
+}
+
+// The persistent form's bricks: the depth tz that minimises an estimate of
+// the CTA's time.  A brick's MMAs take tiles x (cycles of a tile's MMAs,
+// bound by the shared-memory reads of A and B at 128 bytes per clock), its
+// halo copy (16-byte rows) about bytes / 16 cycles; with two stages the
+// slower of the two sets the pace after the first copy, with one they add.
+// Returns false when no depth fits.
+bool plan_pipe(ConvTcParams& p, int num_sms, ConvTcPlan& plan) {
+  const int nchunk = p.cin / 8, nphase = p.stride == 2 ? 8 : 1, hpad = p.stride == 2 ? 1 : 2;
+  const long long wbytes = 27LL * p.cin * p.nout * 2;
+  const long long extra = 8LL * kPipeBars + 8 + 4LL * p.nout + (p.fold ? kEpiGroups * 16LL * 4 * p.nout : 0);
+  const long long cap = 227 * 1024;
+  const int cps = std::max(1, num_sms / p.nslices);
+  const double tile_cycles = (p.fold ? 9.0 : 27.0) * (p.cin / 16) * (32.0 + p.N / 4.0);
+  double best = -1;
+  int best_tz = 0, best_nst = 0;
+  for (int tz = 1; tz <= p.dims[2]; tz++) {
+    pipe_layout(p, tz, hpad);
+    const long long stage = (long long)nphase * nchunk * p.plane_bytes;
+    const int nbricks = p.nb[0] * p.nb[1] * ceil_div(p.dims[2], tz);
+    const int per_cta = ceil_div(nbricks, cps);
+    int nst = 0;
+    if (per_cta > 1 && 2 * stage + wbytes + extra <= cap)
+      nst = 2;
+    else if (stage + wbytes + extra <= cap)
+      nst = 1;
+    if (!nst) break;  // deeper bricks only grow
+    const double copy_cycles = (double)nphase * nchunk * 16.0 * p.halo[0] * p.halo[1] * p.halo[2] / 16.0;
+    const double mma_cycles = (double)p.tiles * tile_cycles;
+    const double cost = nst == 2 ? copy_cycles + per_cta * std::max(mma_cycles, copy_cycles)
+                                 : per_cta * (mma_cycles + copy_cycles);
+    if (best < 0 || cost <= best) {
+      best = cost;
+      best_tz = tz;
+      best_nst = nst;
+    }
+  }
+  if (!best_tz) return false;
+  pipe_layout(p, best_tz, hpad);
+  p.astages = best_nst;
+  // accumulator ring: a multiple of the epilogue groups, so that every
+  // accumulator is read by one group only (a group waits on each phase of
+  // its accumulators' mdone in turn; an mbarrier parity wait cannot look two
+  // phases ahead), within 256 TMEM columns where it can (two CTAs per SM)
+  const int per_group = std::max(1, std::min(256 / (kEpiGroups * p.N), kPipeAcc / kEpiGroups));
+  p.nacc = kEpiGroups * per_group;
+  int cols = 32;
+  while (cols < p.nacc * p.N) cols *= 2;
+  p.acc_cols = cols;
+  plan.smem = (size_t)best_nst * nphase * nchunk * p.plane_bytes + wbytes + extra;
+  const int nbricks = p.nb[0] * p.nb[1] * ceil_div(p.dims[2], best_tz);
+  plan.grid_x = p.nslices * std::min(nbricks, cps);
+  plan.pipe = 1;
+  return true;
+}
+
+}  // namespace
+
+int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, ConvTcPlan& plan, int pipe) {
   std::memset(&plan, 0, sizeof(plan));
   if (!conv_tc_supported(d)) return -1;
   ConvTcParams& p = plan.p;
@@ -433,6 +891,12 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
   p.cout = d.cout;
   p.N = conv_tc_slice_width(d.ca, d.cout, d.stride);
   p.nslices = ceil_div(d.cout < 16 ? 16 : d.cout, p.N);
+  p.nout = p.N;
+  if (pipe == 2) {
+    if (d.stride != 1) return -1;
+    p.fold = 1;
+    p.N = 3 * p.nout;
+  }
   const int nchunk = p.cin / 8, nphase = d.stride == 2 ? 8 : 1, hpad = d.stride == 2 ? 1 : 2;
   const long long wbytes = 27LL * p.cin * p.N * 2;
   for (int a = 0; a < 2; a++) {
@@ -440,9 +904,12 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
     p.brick[a] = ceil_div(p.dims[a], p.nb[a]);
     p.halo[a] = p.brick[a] + hpad;
   }
+  if (pipe) {
+    if (!plan_pipe(p, num_sms, plan)) return -3;
+  }
   // bricks along z: one wave of two CTAs per SM when two fit next to each
   // other in shared memory, else one wave of one CTA per SM with deeper bricks
-  for (int per_sm = 2; per_sm >= 1; per_sm--) {
+  for (int per_sm = 2; per_sm >= 1 && !pipe; per_sm--) {
     const long long budget = per_sm == 2 ? 113 * 1024 : 220 * 1024;
     const int target = std::max(1, per_sm * num_sms / (p.nb[0] * p.nb[1] * p.nslices));
     int tz = std::max(1, ceil_div(p.dims[2], target));
@@ -466,12 +933,18 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
   if (plan.smem > 227 * 1024) return -3;
   {
     // every shared-memory row the MMAs address lies inside its plane, the
-    // halo box stays small, and a group of tiles fits the TMEM columns
+    // halo box stays small, and a group of tiles (the persistent form: the
+    // accumulator ring) fits the TMEM columns
     const int HX = p.halo[0], HY = p.halo[1];
     const int off_min = 1 + HX + HX * HY, off_max = d.stride == 2 ? 0 : off_min;
-    if (p.q0 - off_min < 0 || p.q0 + 128 * p.tiles - 1 + off_max >= p.rows || p.rows * 16 > p.plane_bytes ||
-        p.halo[0] > 256 || p.halo[1] > 256 || p.halo[2] > 256 || p.tiles < 1 || p.N > kTmemCols ||
-        p.N % 16 != 0 || p.cin % 16 != 0)
+    int lo = p.q0 - off_min, hi = p.q0 + 128 * p.tiles - 1 + off_max;
+    if (pipe) pipe_rows(p, lo, hi);
+    if (lo < 0 || hi >= p.rows || p.rows * 16 > p.plane_bytes || p.halo[0] > 256 || p.halo[1] > 256 ||
+        p.halo[2] > 256 || p.tiles < 1 || p.N % 16 != 0 || p.N < 16 || p.cin % 16 != 0 || p.nout % 16 != 0 ||
+        (!pipe && p.N > kTmemCols) ||
+        (pipe && (p.N > 256 || p.nacc < 1 || p.nacc > kPipeAcc || p.nacc % kEpiGroups != 0 ||
+                  p.nacc * p.N > p.acc_cols || p.acc_cols > 512 ||
+                  plan.grid_x % p.nslices != 0 || (p.fold && p.nout > 16 * kFoldChunks))))
       return -5;
   }
   p.nb[2] = ceil_div(p.dims[2], p.brick[2]);
@@ -482,7 +955,7 @@ int conv_tc_plan(const ConvDesc& d, const __nv_bfloat16* wpack, int num_sms, Con
   p.out_f32 = d.out_f32;
   p.act = d.act;
   p.skip = d.skip;
-  plan.grid_x = p.nb[0] * p.nb[1] * p.nb[2];
+  if (!pipe) plan.grid_x = p.nb[0] * p.nb[1] * p.nb[2];
   plan.ready = 1;
   return 0;
 }
@@ -493,6 +966,24 @@ cudaError_t conv3_forward_tc(const ConvTcPlan& plan, float* out_f32, const int* 
   p.skip = skip;
   p.err = err;
   void (*k)(ConvTcParams) = nullptr;
+  if (plan.pipe) {
+    switch (p.cin * 8 + p.stride * 2 + p.fold) {
+      case 16 * 8 + 2: k = k_conv_pipe<16, 1, false>; break;
+      case 16 * 8 + 3: k = k_conv_pipe<16, 1, true>; break;
+      case 16 * 8 + 4: k = k_conv_pipe<16, 2, false>; break;
+      case 32 * 8 + 2: k = k_conv_pipe<32, 1, false>; break;
+      case 32 * 8 + 3: k = k_conv_pipe<32, 1, true>; break;
+      case 32 * 8 + 4: k = k_conv_pipe<32, 2, false>; break;
+      case 64 * 8 + 2: k = k_conv_pipe<64, 1, false>; break;
+      case 64 * 8 + 3: k = k_conv_pipe<64, 1, true>; break;
+      case 64 * 8 + 4: k = k_conv_pipe<64, 2, false>; break;
+      default: return cudaErrorInvalidValue;
+    }
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e != cudaSuccess) return e;
+    k<<<plan.grid_x, kPipeThreads, plan.smem, s>>>(p);
+    return cudaGetLastError();
+  }
   switch (p.cin * 4 + p.stride) {
     case 16 * 4 + 1: k = k_conv_tc<16, 1>; break;
     case 16 * 4 + 2: k = k_conv_tc<16, 2>; break;

@@ -89,6 +89,7 @@ int UnetNet::init(unsigned long long seed) {
     return -1;
   }
   if (const char* e = std::getenv("CFD_UNET_TC")) tc_enabled = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_CONV_PIPE")) conv_pipe = std::atoi(e);
   if (!own_stream && cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking) != cudaSuccess) return -1;
   const size_t b = (size_t)nparam * sizeof(float);
   if (cudaMalloc((void**)&P, b) || cudaMalloc((void**)&G, b) || cudaMalloc((void**)&M1, b) ||
@@ -210,7 +211,7 @@ cudaError_t UnetNet::prepare_tc(cudaStream_t s) {
       const int st = kUnetConv[l].stride;
       if (cin % 16) continue;
       cudaError_t e = grow(wpack[l], wpack_cap[l], conv_tc_pack_elems(cin, cout, st));
-      if (e == cudaSuccess) e = conv_tc_pack(Pb + unet_weight_offset(l), cin, cout, st, wpack[l], s);
+      if (e == cudaSuccess) e = conv_tc_pack(Pb + unet_weight_offset(l), cin, cout, st, wpack[l], s, pipe_mode(st) == 2);
       launches++;
       if (e != cudaSuccess) return e;
     }
@@ -221,7 +222,7 @@ cudaError_t UnetNet::prepare_tc(cudaStream_t s) {
       ConvDesc d = conv_desc(*this, l, out);
       plan_ok[l] = false;
       if (!wpack[l] || !conv_tc_supported(d)) continue;
-      plan_ok[l] = conv_tc_plan(d, wpack[l], num_sms, plans[l]) == 0;
+      plan_ok[l] = conv_tc_plan(d, wpack[l], num_sms, plans[l], pipe_mode(d.stride)) == 0;
     }
     plan_gen = gen;
     for (int a = 0; a < 3; a++) plan_dims[a] = dims[0][a];

@@ -80,6 +80,16 @@ struct UnetNet {
 
   // tensor-core path: packed weights and launch plans of the stride-1 layers
   bool tc_enabled = true;
+  // tensor-core kernel of each layer (CFD_CONV_PIPE): 0 one CTA per brick;
+  // 1 the persistent kernel; 2 the persistent kernel with the dx taps folded
+  // on the stride-1 layers, one CTA per brick on the stride-2 layers; 3 as 2
+  // with the persistent kernel on the stride-2 layers
+  int conv_pipe = 0;
+  // conv_tc_plan's pipe argument for a layer of this stride
+  int pipe_mode(int stride) const {
+    if (stride == 1) return conv_pipe == 1 ? 1 : (conv_pipe >= 2 ? 2 : 0);
+    return conv_pipe == 1 || conv_pipe == 3 ? 1 : 0;
+  }
   int num_sms = 148;
   __nv_bfloat16* wpack[kUnetConvs] = {};
   long long wpack_cap[kUnetConvs] = {};

@@ -52,13 +52,20 @@ def _gpu_tensors(net, dims):
     return [net.tensor(t, dims).astype(np.float64) for t in range(len(U.TENSORS))]
 
 
-@pytest.mark.parametrize("dims,tc", [(GRIDS[0], False), (GRIDS[1], False), (GRIDS[0], True), (GRIDS[1], True),
-                                     ((33, 17, 21), True), ((65, 65, 65), True)])
-def test_forward_layers_match_oracle(dims, tc):
+@pytest.mark.parametrize("dims,tc,pipe", [(GRIDS[0], False, 0), (GRIDS[1], False, 0), (GRIDS[0], True, 0),
+                                          (GRIDS[1], True, 0), ((33, 17, 21), True, 0), ((65, 65, 65), True, 0),
+                                          (GRIDS[0], True, 2), (GRIDS[1], True, 2), ((33, 17, 21), True, 2),
+                                          ((65, 65, 65), True, 2), ((65, 65, 65), True, 1),
+                                          ((33, 17, 21), True, 3)])
+def test_forward_layers_match_oracle(dims, tc, pipe, monkeypatch):
     """Each layer of the device forward pass (CUDA-core kernels, or the
-    tcgen05 tensor-core convolutions where the layer allows), recomputed by
-    the oracle from the device's own input tensor of that layer: BF16 outputs
-    agree except for rare rounding flips (FP32 vs FP64 accumulation)."""
+    tcgen05 tensor-core convolutions where the layer allows: one CTA per
+    brick; pipe = 1 the persistent, pipelined kernel; pipe = 2 that kernel
+    with the dx taps folded into N on the stride-1 layers; pipe = 3 both),
+    recomputed by the oracle from the device's own
+    input tensor of that layer: BF16 outputs agree except for rare rounding
+    flips (FP32 vs FP64 accumulation)."""
+    monkeypatch.setenv("CFD_CONV_PIPE", str(pipe))
     net, theta = _net(6)
     net.set_tensor_cores(tc)
     x, _ = _sample(dims, 3)
