@@ -179,6 +179,11 @@ struct cfd_ctx {
   // stream beside the SpMV); measured slower than the sequential form on the
   // 64^3 cavity (8.97 against 8.13 ms per step), so off by default
   bool fcg_split = false;
+  // mixed-precision convection on the tensor cores (k_convect_tc) where it
+  // applies; conv_err is its bounded-wait error word
+  bool convect_tc = false;
+  bool convect_tc_ran = false;
+  DevBuf<int> conv_err;
   // CFD_FCG_ANCHOR=0: with the network in the head iterations only, keep the
   // ring of the last fcg_m directions instead of anchoring the head's
   bool fcg_anchor = true;
@@ -1525,8 +1530,12 @@ int reduce_norms(cfd_ctx* c) {
   cudaStream_t s = c->stream;
   KL(CFD_K_OTHER, launch_reduce_norms(c->upart.p, c->nub, c->ppart.p, c->npb, c->norms.p, s));
   CU(cudaMemcpyAsync(c->h_small, c->norms.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  int* h_conv_err = reinterpret_cast<int*>(c->h_small + 8);
+  *h_conv_err = 0;
+  if (c->convect_tc_ran) CU(cudaMemcpyAsync(h_conv_err, c->conv_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   CU(cudaStreamSynchronize(s));
   for (int i = 0; i < 5; i++) c->last_norms[i] = c->h_small[i];
+  if (*h_conv_err) return fail(c, CFD_E_TIMEOUT, "device-side wait timed out in the tensor-core convection");
   return CFD_OK;
 }
 
@@ -1584,6 +1593,7 @@ int cfd_create(cfd_ctx** out, int device) {
   if (const char* e = std::getenv("CFD_L2_PERSIST")) c->l2_persist = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_COARSE_SPACING")) c->coarse_spacing = std::atof(e);
   if (const char* e = std::getenv("CFD_FCG_SPLIT")) c->fcg_split = std::atoi(e) != 0;
+  if (const char* e = std::getenv("CFD_CONVECT_TC")) c->convect_tc = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_FCG_ANCHOR")) c->fcg_anchor = std::atoi(e) != 0;
   if (const char* e = std::getenv("CFD_SPLIT_SPMV_PER_SM")) c->split_spmv_per_sm = std::atoi(e) == 1 ? 1 : 2;
   *out = c.release();
@@ -1813,6 +1823,19 @@ int cfd_convect(cfd_ctx* c) {
   if (mixed(c)) {
     ConvArgs<float> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un32, c->uphp32, c->r1conv};
     a.r1f = c->r1c32;
+    if (c->convect_tc && !c->opt.deterministic) {
+      a.e_begin = 0;
+      a.e_end = c->P.NE;
+      if (convect_tc_supported(a)) {
+        if (!c->conv_err.p) {
+          CU(c->conv_err.alloc(1));
+          CU(cudaMemsetAsync(c->conv_err.p, 0, sizeof(int), s));
+        }
+        c->convect_tc_ran = true;
+        KL(CFD_K_CONVECT, launch_convect_tc(a, c->conv_err.p, c->num_sms, s));
+        return CFD_OK;
+      }
+    }
     return run(a, [&](const ConvArgs<float>& x) { return launch_convect<float>(x, c->num_sms, s); });
   }
   ConvArgs<double> a{c->P.NE, c->P.NGP, c->ltog.p, c->coord.p, c->basis.p, c->un, c->unphalf_prev, c->r1conv};

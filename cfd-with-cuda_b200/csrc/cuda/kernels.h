@@ -98,6 +98,12 @@ struct ConvArgs {
 };
 template <class T>
 cudaError_t launch_convect(const ConvArgs<T>& a, int num_sms, cudaStream_t s);
+// The same term with the per-element contractions on the tensor cores
+// (tcgen05, TF32 split into hi + lo parts; convect_tc.cu): FP32 copies (r1f
+// set), NGP = 8, no colouring.  *err (device, zeroed by the caller) is set
+// when a bounded wait of the kernel gives up.
+bool convect_tc_supported(const ConvArgs<float>& a);
+cudaError_t launch_convect_tc(const ConvArgs<float>& a, int* err, int num_sms, cudaStream_t s);
 
 template <class VT>
 struct Step1Args {

@@ -36,6 +36,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 #include "unet.h"
 
 namespace cfd {
@@ -50,17 +51,6 @@ struct Dims6 {
   int c[3], f[3];
 };
 
-__device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
-  // SWIZZLE_NONE, K-major canonical layout: 8-row core matrices of 16-byte
-  // rows; lbo = byte distance between the two K halves, sbo = between 8-row
-  // groups; version field (bits 46-47) = 1.
-  unsigned long long d = (unsigned long long)((saddr >> 4) & 0x3FFFu);
-  d |= (unsigned long long)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (unsigned long long)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= 1ULL << 46;
-  return d;
-}
-
 // BF16 x BF16 -> FP32, both operands K-major, M = 128.
 __host__ __device__ constexpr unsigned umma_idesc(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(n >> 3) << 17) | ((128u >> 4) << 24);
@@ -72,36 +62,6 @@ __device__ __forceinline__ void umma(unsigned tmem_d, unsigned long long a, unsi
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_alloc(unsigned* slot, unsigned ncols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
-               "r"(ncols)
-               : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
-  unsigned r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
 // tcgen05.ld without its wait, for several loads in flight; tmem_wait_ld
