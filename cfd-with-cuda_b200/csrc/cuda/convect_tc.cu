@@ -51,8 +51,12 @@ constexpr unsigned oA1h = 0, oA1l = oA1h + kA1, oB1h = oA1l + kA1, oB1l = oB1h +
 constexpr unsigned oA2h = oB1l + kB1, oA2l = oA2h + kA2, oB2h = oA2l + kA2, oB2l = oB2h + kB2;
 constexpr int kSld = 33;                                    // row stride (floats) of the TMEM staging
 constexpr unsigned oS = oB2l + kB2;                         // float[128][33]
-constexpr unsigned oU = oS + 128 * kSld * 4;                // float4[16][27] (Un), then float4[16][27] (uprev)
-constexpr unsigned oLt = oU + 2 * kCtElems * 27 * 16;       // int[16][27]
+// the gathered nodal values, float4[16][27] of Un then of uprev, share the
+// staging area: they are dead once operand (1) is written, and the staging
+// is first written after MMA (1) completes
+constexpr unsigned oU = oS;
+static_assert(2 * kCtElems * 27 * 16 <= 128 * kSld * 4, "nodal staging must fit in the TMEM staging");
+constexpr unsigned oLt = oS + 128 * kSld * 4;               // int[16][27]
 constexpr unsigned oX = oLt + kCtElems * 27 * 4;            // float[16][24] corner coordinates
 constexpr unsigned oDsp = oX + kCtElems * 24 * 4;           // float[3][8][8]
 constexpr unsigned oW = oDsp + 3 * 8 * 8 * 4;               // float[8]
@@ -326,12 +330,19 @@ bool convect_tc_supported(const ConvArgs<float>& a) {
 cudaError_t launch_convect_tc(const ConvArgs<float>& a, int* err, int num_sms, cudaStream_t s) {
   if (!convect_tc_supported(a) || !err) return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(k_convect_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCtSmem);
+  // all of the unified L1 as shared memory: three 72 KB blocks per SM
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_convect_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
-  int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_convect_tc, kCtThreads, kCtSmem);
+  // blocks per SM from the shared memory (the occupancy query answered one
+  // block per SM for this kernel, where three fit)
+  int dev = 0, smem_sm = 0;
+  e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
   if (e != cudaSuccess) return e;
+  int per_sm = smem_sm / (int)(kCtSmem + 1024);  // 1 KB reserved per block
+  per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
   const int ntiles = (a.e_end - a.e_begin + kCtElems - 1) / kCtElems;
-  int grid = num_sms * (per_sm > 0 ? per_sm : 1);
+  int grid = num_sms * per_sm;
   if (grid > ntiles) grid = ntiles;
   k_convect_tc<<<grid, kCtThreads, kCtSmem, s>>>(a, err);
   return cudaGetLastError();
