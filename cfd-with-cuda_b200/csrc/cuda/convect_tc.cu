@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kCtThreads) k_convect_tc(ConvArgs<float> a, in
   float* sw = reinterpret_cast<float*>(smem + oW);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem + oBar);
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(smem + oSlot);
-  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int t = threadIdx.x, warp = t >> 5;
 
   // operand tiles start at zero (padding rows and K columns stay zero); the
   // constant basis tiles, split into hi and lo
