@@ -104,6 +104,35 @@ def test_out_of_range_values_rejected(tmp_path, decks):
             HostMesh(str(p))
 
 
+def test_number_forms_read_as_strtod(tmp_path):
+    """The deck reader takes numbers in the forms the reference's istream
+    extraction (strtol / strtod) accepts: the same corner coordinates written
+    with a leading '+', an exponent, a hexadecimal mantissa, no integer or no
+    fraction digits, and node numbers with a leading '+', give bit-identical
+    coordinates and the same mesh."""
+    from cfdfs import HostMesh, meshgen
+    path = meshgen.write_cavity(str(tmp_path / "c2.inp"), meshgen.CavitySpec(2, re=100, dt=0.01, steps=2, ngp=8))
+    text = open(path).read()
+    forms = {0.0: ["+0.0", "0e5", "0x0p0", ".0", "0."], 0.5: ["+0.5", "5e-1", "0x1p-1", ".5", "+.5E0"],
+             1.0: ["1.", "+1", "1e0", "0X1P0", "10e-1"]}
+    lines = text.split("\n")
+    first = next(k for k, l in enumerate(lines) if l.startswith("Corner Node No")) + 1
+    for k in range(27):
+        f = lines[first + k].split()
+        out = ["+" + f[0] if k % 2 else f[0]]
+        for c, v in enumerate(f[1:]):
+            alts = forms[float(v)]
+            out.append(alts[(k + c) % len(alts)])
+        lines[first + k] = "   ".join(out)
+    alt = tmp_path / "c2_forms.inp"
+    alt.write_text("\n".join(lines))
+    a, b = HostMesh(path), HostMesh(str(alt))
+    assert a.coord().tobytes() == b.coord().tobytes()
+    assert np.array_equal(a.ltog(), b.ltog()) and np.array_equal(a.bcnodes(), b.bcnodes())
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("key", ["c1", "graded", "perturbed", "duct_small"])
 def test_element_colouring_conflict_free(decks, key):
     """The deterministic mode's colouring (one colour per launch, plain adds):
