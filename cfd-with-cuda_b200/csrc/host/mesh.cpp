@@ -24,7 +24,6 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
-#include <parallel/algorithm>
 #include <sstream>
 #include <utility>
 
@@ -304,37 +303,37 @@ struct Key2 {
 };
 
 // Numbers the distinct keys in order of first appearance (appearance index =
-// position in keys[]) starting at base; out[i] = number of keys[i].  The
-// (key, index) pairs are sorted in parallel; since the indices differ, the
-// order is total and each group of equal keys starts at its first
-// appearance.
+// position in keys[]) starting at base; out[i] = number of keys[i].  Every
+// key starts with its smallest corner id (the high word of a), which buckets
+// it: a CSR over the ncorner corner nodes, sized by counting, holds the keys
+// met so far per corner, and one pass in index order looks each key up among
+// its corner's few distinct keys (an edge or face of a hex mesh has at most
+// a dozen per corner), numbering it when it is new.
+inline uint32_t first_corner(uint64_t k) { return (uint32_t)(k >> 32); }
+inline uint32_t first_corner(const Key2& k) { return (uint32_t)(k.a >> 32); }
 template <class K>
-int number_by_first_appearance(const std::vector<K>& keys, int base, std::vector<int>& out) {
+int number_by_first_appearance(const std::vector<K>& keys, int ncorner, int base, std::vector<int>& out) {
   const size_t n = keys.size();
-  std::vector<std::pair<K, uint32_t>> kv(n);
-#pragma omp parallel for schedule(static)
-  for (size_t i = 0; i < n; i++) kv[i] = {keys[i], (uint32_t)i};
-  __gnu_parallel::sort(kv.begin(), kv.end(), [](const std::pair<K, uint32_t>& x, const std::pair<K, uint32_t>& y) {
-    return x.first < y.first || (x.first == y.first && x.second < y.second);
-  });
-  // group leader = first appearance (smallest index, first in its group)
-  std::vector<uint32_t> leader(n);
-  std::vector<char> first(n, 0);
-  for (size_t s = 0; s < n;) {
-    size_t t = s;
-    while (t < n && kv[t].first == kv[s].first) t++;
-    for (size_t u = s; u < t; u++) leader[kv[u].second] = kv[s].second;
-    first[kv[s].second] = 1;
-    s = t;
-  }
-  // leaders numbered in index order
-  std::vector<int> number(n, -1);
-  int count = 0;
-  for (size_t i = 0; i < n; i++)
-    if (first[i]) number[i] = base + count++;
+  std::vector<int> off((size_t)ncorner + 1, 0);
+  for (size_t i = 0; i < n; i++) off[first_corner(keys[i]) + 1]++;
+  for (int c = 0; c < ncorner; c++) off[c + 1] += off[c];
+  std::vector<K> bkey(n);
+  std::vector<int> bnum(n), fill((size_t)ncorner, 0);
   out.resize(n);
-#pragma omp parallel for schedule(static)
-  for (size_t i = 0; i < n; i++) out[i] = number[leader[i]];
+  int count = 0;
+  for (size_t i = 0; i < n; i++) {
+    const K& k = keys[i];
+    const uint32_t c = first_corner(k);
+    const int s = off[c], f = fill[c];
+    int t = 0;
+    while (t < f && !(bkey[s + t] == k)) t++;
+    if (t == f) {
+      bkey[s + f] = k;
+      bnum[s + f] = base + count++;
+      fill[c] = f + 1;
+    }
+    out[i] = bnum[s + t];
+  }
   return count;
 }
 
@@ -403,7 +402,7 @@ int preprocess(HostProblem& P, std::string& err, bool patterns) {
       ekeys[(size_t)e * 12 + ed] = ((uint64_t)a << 32) | b;
     }
   std::vector<int> enum_;
-  int nEdge = number_by_first_appearance(ekeys, NCN, enum_);
+  int nEdge = number_by_first_appearance(ekeys, NCN, NCN, enum_);
   std::vector<uint64_t>().swap(ekeys);
   // ---- mid-face nodes ----
   std::vector<Key2> fkeys((size_t)NE * 6);
@@ -415,7 +414,7 @@ int preprocess(HostProblem& P, std::string& err, bool patterns) {
       fkeys[(size_t)e * 6 + f] = Key2{((uint64_t)c[0] << 32) | c[1], ((uint64_t)c[2] << 32) | c[3]};
     }
   std::vector<int> fnum;
-  int nFace = number_by_first_appearance(fkeys, NCN + nEdge, fnum);
+  int nFace = number_by_first_appearance(fkeys, NCN, NCN + nEdge, fnum);
   std::vector<Key2>().swap(fkeys);
   P.NN = NCN + nEdge + nFace + NE;
   std::vector<double> coord((size_t)P.NN * 3, 0.0);
