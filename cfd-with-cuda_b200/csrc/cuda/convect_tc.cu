@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kCtThreads) k_convect_tc(ConvArgs<float> a, in
   const int re = r >> 3, rq = r & 7;  // its element slot and quantity / Gauss point / component
   const int ntiles = (a.e_end - a.e_begin + kCtElems - 1) / kCtElems;
   bool ok = true;
-  int it = 0;
+  int it = 0, pending = 0;  // the barrier whose wait gave up
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, it++) {
     const int p0 = a.e_begin + tile * kCtElems;
     const int cnt = min(kCtElems, a.e_end - p0);
@@ -210,7 +210,10 @@ __global__ void __launch_bounds__(kCtThreads) k_convect_tc(ConvArgs<float> a, in
     __syncwarp();
     ok = __syncthreads_and(mbar_wait_bounded(&bar[0], (unsigned)(it & 1), kCtWaitNs));
     tc_fence_after();
-    if (!ok) break;
+    if (!ok) {
+      pending = 0;
+      break;
+    }
     {
       float v[16];
       tmem_ld16(trow, v);
@@ -286,7 +289,10 @@ __global__ void __launch_bounds__(kCtThreads) k_convect_tc(ConvArgs<float> a, in
     __syncwarp();
     ok = __syncthreads_and(mbar_wait_bounded(&bar[1], (unsigned)(it & 1), kCtWaitNs));
     tc_fence_after();
-    if (!ok) break;
+    if (!ok) {
+      pending = 1;
+      break;
+    }
     {
       // row (e, d): R1e_i^d over the nodes i
       float v[16];
@@ -311,8 +317,7 @@ __global__ void __launch_bounds__(kCtThreads) k_convect_tc(ConvArgs<float> a, in
     // more bounded wait, then release the accumulator columns
     if (t == 0) {
       atomicExch(err, 1);
-      mbar_wait_bounded(&bar[0], (unsigned)(it & 1), kCtWaitNs);
-      mbar_wait_bounded(&bar[1], (unsigned)(it & 1), kCtWaitNs);
+      mbar_wait_bounded(&bar[pending], (unsigned)(it & 1), kCtWaitNs);
     }
     tc_fence_before();
     __syncthreads();
